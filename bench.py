@@ -1,0 +1,293 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 ForceAtlas2 engine on the plain Barnes-Hut workload.
+
+Workload (one "step" = one ForceAtlas2 iteration of the whole graph):
+  R-MAT scale 20, 16,777,216 edge draws, a=.57 b=.19 c=.19 (seed 0), self-loops
+  and repeated undirected edges removed (N = 646,043 nodes, E = 15,701,711
+  edges); positions uniform in [-1e4, 1e4]^2 (srandom(1234) + the reference's
+  randomizePositions); strong gravity, scale 10, gravity 1, theta 1.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value` is device-timed iterations/s with the graph resident in HBM (CUDA
+events on the engine's stream around K iterations, max over ranks, summed
+over ranks: with N > 1 every rank lays out its own replica of the graph, the
+single-graph path does not shard).  `e2e` is the same metric through the
+public C ABI with host buffers: per step, the positions are copied in from
+pinned host memory, one iteration runs and the positions are copied back.
+`--impl reference` times the reference's own CPU ForceAtlas2
+(CPUForceAtlas2::doStep, built from its sources into oracle/_ref) on the same
+graph and positions, one iteration per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FA2 iters/s on R-MAT 1M/16M: plain BH vs learned-correction at equal force RMSE"
+UNIT = "iters/s"
+SCALE, DRAWS = 20, 16_777_216
+K_R, K_G, STRONG = 10.0, 1.0, True
+WIDTH = 2.0e4
+KERNELS_PER_ITER = 17  # attract, bbox, keys, 8 sort passes, runs, count, emit, summarize, traverse, displace
+
+
+def clocks_sampler(device: int, path: str):
+    try:
+        return subprocess.Popen(
+            ["nvidia-smi", f"--id={device}",
+             "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+             "--format=csv,noheader,nounits", "-lms", "200"],
+            stdout=open(path, "w"), stderr=subprocess.DEVNULL)
+    except Exception:
+        return None
+
+
+def clocks_summary(path: str):
+    sm, mx, reasons = [], [], set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    try:
+        for line in open(path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+    except OSError:
+        pass
+    if not sm:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons)}
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def barrier_max(world, value: float) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ------------------------------------------------------------------ reference --
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/libref_cpu.so is not built (needs the "
+                                         "reference sources at build time)"}))
+        return
+    from gpugraphlayout_b200 import synth
+    s, t = synth.rmat_edges(SCALE, DRAWS, seed=0)
+    og = O.Graph(s, t)
+    rg = O.RefGraph(graph=og)
+    ref = O.RefCPUFA2(rg, WIDTH, WIDTH, 1234, True, STRONG, K_G, K_R)
+    for _ in range(args.warmup):
+        ref.step(1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ref.step(1)
+    dt = time.perf_counter() - t0
+    v = args.steps / dt
+    sample = (f"{args.warmup}+{args.steps} full iterations of CPUForceAtlas2::doStep "
+              f"(Barnes-Hut, 1 thread) on the whole workload graph")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": workload_config(og.n, og.m),
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def workload_config(n, m):
+    return {"workload": f"R-MAT scale {SCALE} ({DRAWS:,} draws, a=.57 b=.19 c=.19, seed 0), "
+                        f"N={n:,} E={m:,}; positions U[-1e4,1e4]^2; strong gravity, scale 10, "
+                        f"gravity 1, theta 1; plain Barnes-Hut",
+            "nodes": n, "edges": m, "l2": "per-iteration working set larger than L2 "
+                                          "(padded CSR alone exceeds 126 MB)",
+            "parallelism": "replicas (one graph per GPU)"}
+
+
+def cpu_baseline_sample(og, xy):
+    """The reference CPU ForceAtlas2 on the workload graph: 3 iterations after
+    one untimed one (~10-30 s of single-thread CPU work at scale 20)."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        return None
+    rg = O.RefGraph(graph=og)
+    ref = O.RefCPUFA2(rg, WIDTH, WIDTH, 1234, True, STRONG, K_G, K_R)
+    ref.set_positions(xy)
+    ref.step(1)
+    it = 3
+    t0 = time.perf_counter()
+    ref.step(it)
+    dt = time.perf_counter() - t0
+    return {"value": it / dt, "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"{it} iterations of CPUForceAtlas2::doStep (Barnes-Hut, 1 thread) on "
+                      f"the full workload graph after 1 untimed iteration"}
+
+
+# ----------------------------------------------------------------------- ours --
+
+def run_ours(args, world, rank, local):
+    from gpugraphlayout_b200 import Engine, UGraph, kernel_names, random_positions, synth
+    s_raw, t_raw = synth.rmat_edges(SCALE, DRAWS, seed=0)
+    g = UGraph.from_pairs(s_raw, t_raw)
+    n, m = g.num_nodes(), g.num_edges()
+    s, t = g.edges()
+    xy0 = random_positions(n, WIDTH, WIDTH, 1234)
+    eng = Engine(n, s, t, strong_gravity=STRONG, gravity=K_G, scale=K_R, device=local)
+    eng.set_positions(xy0)
+
+    import torch
+    torch.cuda.set_device(local)
+    eng.step(max(args.warmup, 3))
+    clk_path = os.path.join(tempfile.gettempdir(), f"fa2_clocks_{rank}.csv")
+    sampler = clocks_sampler(local, clk_path)
+    time.sleep(0.3)
+    barrier(world)
+    torch.cuda.synchronize()
+    ms, kms = eng.step_timed(args.steps)
+    torch.cuda.synchronize()
+    barrier(world)
+    if sampler:
+        sampler.terminate()
+        sampler.wait()
+    st = eng.stats()
+    ms_max = barrier_max(world, ms)
+    value = world * args.steps / (ms_max / 1000.0)
+
+    # end to end through the C ABI with pinned host buffers
+    host = torch.empty((n, 2), dtype=torch.float32, pin_memory=True)
+    host.numpy()[:] = eng.get_positions()
+    ptr = host.data_ptr()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        eng.set_positions_ptr(ptr)
+        eng.step(1)
+        eng.get_positions_ptr(ptr)
+    e2e_s = barrier_max(world, time.perf_counter() - t0)
+    e2e = world * args.steps / e2e_s
+
+    if rank != 0:
+        return
+    names = kernel_names()
+    pk, pk_kind = peaks()
+    hbm = float(pk["hbm_gbs"])
+    # algorithmic bytes per launch
+    nnz = st["nnz_padded"]
+    attract_bytes = 4 * nnz + 4 * (n + 1) + 8 * n + 4 * n + 8 * n
+    disp_bytes = 40 * n
+    trav_ms = kms.get("traverse", 0.0)
+    kernels = {}
+    for nm in names:
+        kernels[nm] = {"ms": kms.get(nm, 0.0)}
+    kernels["attract"].update(bytes=attract_bytes,
+                              gbs=attract_bytes / (kms["attract"] * 1e6) if kms["attract"] else None)
+    kernels["displace"].update(bytes=disp_bytes,
+                               gbs=disp_bytes / (kms["displace"] * 1e6) if kms["displace"] else None)
+    inter = st["interactions"]
+    kernels["traverse"].update(interactions=inter, visits=st["visits"],
+                               interactions_per_s=inter / (trav_ms * 1e-3) if trav_ms else None)
+    dom = max(names, key=lambda k: kms.get(k, 0.0))
+    att_gbs = kernels["attract"]["gbs"] or 0.0
+    roofline = {"kernel": "attract", "bound": "hbm", "achieved": att_gbs, "peak": hbm,
+                "unit": "GB/s", "frac": att_gbs / hbm, "traffic": None,
+                "note": f"peak = {pk_kind} HBM copy bandwidth; dominant kernel by time is "
+                        f"'{dom}' ({kms.get(dom, 0.0):.3f} ms/launch)"}
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": workload_config(n, m),
+        "clocks": clocks_summary(clk_path),
+        "gpu_launches": KERNELS_PER_ITER * args.steps,
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * n,
+                "d2h_bytes_per_step": 8 * n},
+        "roofline": roofline,
+        "kernels": kernels,
+        "tree": {"nodes": st["tree_nodes"], "cells": st["tree_cells"],
+                 "max_level": st["max_level"]},
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        out["cpu_baseline"] = cpu_baseline_sample(O.Graph(s_raw, t_raw), xy0)
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup(args.gpus)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

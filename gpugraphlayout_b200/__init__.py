@@ -1,0 +1,283 @@
+"""B200-native ForceAtlas2 layout engine (drop-in for the GPU path of
+govertb/GPUGraphLayout).
+
+The engine is libfa2b200.so (C ABI in include/fa2b200.h, sm_100a kernels).
+This module mirrors the reference's C++ interface for Python callers:
+
+* ``UGraph(path)`` / ``UGraph.from_pairs(s, t)`` -- RPGraph::UGraph
+* ``GraphLayout(graph, width=10000, height=10000)`` -- RPGraph::GraphLayout
+* ``CUDAForceAtlas2(layout, use_barneshut, strong_gravity, gravity, scale)``
+  -- RPGraph::CUDAForceAtlas2 (doStep, doSteps, sync_layout, setScale,
+  setGravity, mass)
+* ``Engine`` -- the C ABI context itself, with the test and measurement hooks
+  (forces, body sort order, per-kernel timing).
+
+Errors raise ``Fa2Error`` carrying the C status code; a missing library
+raises at first use (there is no CPU fallback).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._native import Fa2Error, GraphDesc, Params, Stats, check, lib
+
+__all__ = ["Engine", "UGraph", "GraphLayout", "CUDAForceAtlas2", "Fa2Error", "kernel_names",
+           "random_positions"]
+
+
+def _ptr(a: np.ndarray):
+    return C.c_void_p(a.ctypes.data) if a is not None and a.size else None
+
+
+def kernel_names() -> list[str]:
+    out, i = [], 0
+    while True:
+        s = lib().fa2_kernel_name(i)
+        if s is None:
+            return out
+        out.append(s.decode())
+        i += 1
+
+
+def random_positions(n: int, width: float, height: float, seed: int = 1234) -> np.ndarray:
+    """srandom(seed) + GraphLayout::randomizePositions: (n, 2) float32."""
+    xy = np.zeros((max(n, 1), 2), np.float32)
+    lib().fa2_random_positions(n, width, height, seed, _ptr(xy))
+    return xy[:n].copy()
+
+
+class Engine:
+    """One fa2_ctx: a graph on the GPU with its ForceAtlas2 state.
+
+    ``sources``/``targets`` list each undirected edge once over node ids
+    0..num_nodes-1 (as UGraph.edges() returns them)."""
+
+    def __init__(self, num_nodes: int, sources, targets, *, strong_gravity: bool = False,
+                 gravity: float = 1.0, scale: float = 1.0, theta: float = 1.0,
+                 epssq: float = 0.05 * 0.05, device: int = 0, use_barneshut: bool = True):
+        L = lib()
+        self._src = np.ascontiguousarray(sources, np.uint32)
+        self._dst = np.ascontiguousarray(targets, np.uint32)
+        g = GraphDesc(num_nodes, len(self._src), _ptr(self._src), _ptr(self._dst))
+        p = Params()
+        L.fa2_default_params(C.byref(p))
+        p.use_barneshut = int(use_barneshut)
+        p.strong_gravity = int(strong_gravity)
+        p.gravity, p.scale, p.theta, p.epssq, p.device = gravity, scale, theta, epssq, device
+        st = C.c_int(0)
+        self._ctx = L.fa2_create(C.byref(g), C.byref(p), C.byref(st))
+        check(st.value, "fa2_create")
+        self.n = num_nodes
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            lib().fa2_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- positions ---------------------------------------------------------
+    def set_positions(self, xy) -> None:
+        a = np.ascontiguousarray(xy, np.float32).reshape(self.n, 2)
+        check(lib().fa2_set_positions(self._ctx, _ptr(a)), "fa2_set_positions")
+
+    def get_positions(self, out: np.ndarray | None = None) -> np.ndarray:
+        a = out if out is not None else np.zeros((self.n, 2), np.float32)
+        check(lib().fa2_get_positions(self._ctx, _ptr(a)), "fa2_get_positions")
+        return a
+
+    def set_positions_ptr(self, host_ptr: int) -> None:
+        """Upload from a raw host pointer (e.g. pinned memory)."""
+        check(lib().fa2_set_positions(self._ctx, C.c_void_p(host_ptr)), "fa2_set_positions")
+
+    def get_positions_ptr(self, host_ptr: int) -> None:
+        check(lib().fa2_get_positions(self._ctx, C.c_void_p(host_ptr)), "fa2_get_positions")
+
+    # -- stepping ----------------------------------------------------------
+    def step(self, iters: int = 1) -> None:
+        check(lib().fa2_step(self._ctx, iters), "fa2_step")
+
+    def step_timed(self, iters: int):
+        """Runs iters steps; returns (device ms of the call, {kernel: mean ms per launch})."""
+        names = kernel_names()
+        ms = C.c_float(0.0)
+        km = (C.c_float * len(names))()
+        check(lib().fa2_step_timed(self._ctx, iters, C.byref(ms), km, len(names)),
+              "fa2_step_timed")
+        return ms.value, {nm: km[i] for i, nm in enumerate(names)}
+
+    def set_force_params(self, scale: float, gravity: float) -> None:
+        check(lib().fa2_set_force_params(self._ctx, scale, gravity), "fa2_set_force_params")
+
+    # -- inspection ----------------------------------------------------------
+    def forces(self):
+        """(total, gravity + attraction) of the last step, each (n, 2)."""
+        tot = np.zeros((self.n, 2), np.float32)
+        ga = np.zeros((self.n, 2), np.float32)
+        check(lib().fa2_get_forces(self._ctx, _ptr(tot), _ptr(ga)), "fa2_get_forces")
+        return tot, ga
+
+    def sort_order(self) -> np.ndarray:
+        out = np.zeros(self.n, np.uint32)
+        check(lib().fa2_get_sort_order(self._ctx, _ptr(out)), "fa2_get_sort_order")
+        return out
+
+    def stats(self) -> dict:
+        s = Stats()
+        check(lib().fa2_get_stats(self._ctx, C.byref(s)), "fa2_get_stats")
+        return {f: getattr(s, f) for f, _ in Stats._fields_}
+
+    def speed_state(self):
+        gs, se = C.c_float(), C.c_float()
+        fp = np.zeros((self.n, 2), np.float32)
+        check(lib().fa2_get_speed_state(self._ctx, C.byref(gs), C.byref(se), _ptr(fp)),
+              "fa2_get_speed_state")
+        return gs.value, se.value, fp
+
+    def set_speed_state(self, global_speed: float, speed_efficiency: float, f_prev=None):
+        fp = None if f_prev is None else np.ascontiguousarray(f_prev, np.float32).reshape(self.n, 2)
+        check(lib().fa2_set_speed_state(self._ctx, global_speed, speed_efficiency, _ptr(fp)),
+              "fa2_set_speed_state")
+
+
+class UGraph:
+    """RPGraph::UGraph: ids by first appearance, self-loops and repeated
+    undirected edges dropped."""
+
+    def __init__(self, edgelist_path: str | None = None, *, _handle=None):
+        if _handle is None:
+            st = C.c_int(0)
+            _handle = lib().fa2_ugraph_load(str(edgelist_path).encode(), C.byref(st))
+            check(st.value, f"UGraph({edgelist_path!r})")
+        self._h = _handle
+        self._deg = None
+
+    @classmethod
+    def from_pairs(cls, sources, targets) -> "UGraph":
+        s = np.ascontiguousarray(sources, np.uint32)
+        t = np.ascontiguousarray(targets, np.uint32)
+        st = C.c_int(0)
+        h = lib().fa2_ugraph_from_pairs(_ptr(s), _ptr(t), len(s), C.byref(st))
+        check(st.value, "UGraph.from_pairs")
+        return cls(_handle=h)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().fa2_ugraph_free(self._h)
+            self._h = None
+
+    def num_nodes(self) -> int:
+        return int(lib().fa2_ugraph_num_nodes(self._h))
+
+    def num_edges(self) -> int:
+        return int(lib().fa2_ugraph_num_edges(self._h))
+
+    def degrees(self) -> np.ndarray:
+        if self._deg is None:
+            out = np.zeros(max(1, self.num_nodes()), np.uint32)
+            check(lib().fa2_ugraph_degrees(self._h, _ptr(out)))
+            self._deg = out[: self.num_nodes()]
+        return self._deg
+
+    def degree(self, nid: int) -> int:
+        return int(self.degrees()[nid]) if nid < self.num_nodes() else 0
+
+    in_degree = out_degree = degree
+
+    @property
+    def node_map_r(self) -> np.ndarray:
+        out = np.zeros(max(1, self.num_nodes()), np.uint32)
+        check(lib().fa2_ugraph_node_map_r(self._h, _ptr(out)))
+        return out[: self.num_nodes()]
+
+    def edges(self):
+        m = self.num_edges()
+        s = np.zeros(max(1, m), np.uint32)
+        t = np.zeros(max(1, m), np.uint32)
+        check(lib().fa2_ugraph_edges(self._h, _ptr(s), _ptr(t)))
+        return s[:m], t[:m]
+
+    def neighbors_with_geq_id(self, nid: int) -> list[int]:
+        s, t = self.edges()
+        return t[s == nid].tolist()
+
+
+class GraphLayout:
+    """RPGraph::GraphLayout: positions of a UGraph's nodes."""
+
+    def __init__(self, graph: UGraph, width: float = 10000, height: float = 10000):
+        self.graph = graph
+        self.width, self.height = width, height
+        self.xy = np.zeros((graph.num_nodes(), 2), np.float32)
+
+    def randomizePositions(self, seed: int = 1234) -> None:
+        """srandom(seed) as graph_viewer does at start-up, then the reference's draw."""
+        self.xy[:] = random_positions(self.graph.num_nodes(), self.width, self.height, seed)
+
+    def getX(self, n):
+        return float(self.xy[n, 0])
+
+    def getY(self, n):
+        return float(self.xy[n, 1])
+
+    def setX(self, n, v):
+        self.xy[n, 0] = v
+
+    def setY(self, n, v):
+        self.xy[n, 1] = v
+
+    def _write(self, path: str, binary: int):
+        check(lib().fa2_write_layout(self.graph._h, _ptr(np.ascontiguousarray(self.xy)),
+                                     str(path).encode(), binary), f"write {path}")
+
+    def writeToCSV(self, path: str):
+        self._write(path, 0)
+
+    def writeToBin(self, path: str):
+        self._write(path, 1)
+
+
+class CUDAForceAtlas2:
+    """RPGraph::CUDAForceAtlas2: the constructor randomizes the layout (as the
+    reference's ForceAtlas2 constructor does) and uploads graph and positions."""
+
+    def __init__(self, layout: GraphLayout, use_barneshut: bool, strong_gravity: bool,
+                 gravity: float, scale: float, *, seed: int = 1234, device: int = 0):
+        self.layout = layout
+        self.k_r, self.k_g = scale, gravity
+        self.strong_gravity = strong_gravity
+        layout.randomizePositions(seed)
+        s, t = layout.graph.edges()
+        self.engine = Engine(layout.graph.num_nodes(), s, t, strong_gravity=strong_gravity,
+                             gravity=gravity, scale=scale, device=device)
+        self.engine.set_positions(layout.xy)
+        self.iteration = 0
+
+    def setScale(self, s: float):
+        self.k_r = s
+
+    def setGravity(self, g: float):
+        self.k_g = g
+
+    def mass(self, n: int) -> float:
+        return self.layout.graph.degree(n) + 1.0
+
+    def doStep(self):
+        self.doSteps(1)
+
+    def doSteps(self, n: int):
+        self.engine.set_force_params(self.k_r, self.k_g)
+        self.engine.step(n)
+        self.iteration += n
+
+    def sync_layout(self):
+        self.engine.get_positions(self.layout.xy)

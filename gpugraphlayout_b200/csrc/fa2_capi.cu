@@ -1,0 +1,662 @@
+// fa2_capi.cu -- the C ABI of include/fa2b200.h: context set-up, the CUDA
+// graph of one iteration, and the host side of the rare replay path.
+//
+// One iteration is captured once into a CUDA graph on two streams (attraction
+// overlaps the tree build) and replayed per step.  When the tree build finds
+// bodies at exactly the same position it flags the iteration ("poison") and
+// every later kernel of the launch skips its work; the host then applies the
+// reference's .99 scaling (src/RPBHKernels.cu:271-278) and re-runs that
+// iteration from the key stage, before continuing with the rest.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <numeric>
+#include <vector>
+
+#include "../../include/fa2b200.h"
+#include "fa2_internal.cuh"
+
+using namespace fa2;
+
+namespace {
+
+constexpr int kNumSlots = 10;
+const char *const kSlotNames[kNumSlots] = {"attract", "bbox",       "keys", "sort",     "runs",
+                                           "tree_count", "emit",   "summarize", "traverse",
+                                           "displace"};
+enum Slot { S_ATTRACT, S_BBOX, S_KEYS, S_SORT, S_RUNS, S_COUNT, S_EMIT, S_SUMM, S_TRAV, S_DISP };
+
+constexpr int kMaxReplayRounds = 64;
+
+}  // namespace
+
+struct fa2_ctx {
+    int device = 0;
+    int nsm = 148;
+    uint32_t n = 0;
+    uint64_t m = 0;
+    fa2_params prm{};
+    Params kp{};
+    std::vector<uint32_t> ref_of;  // internal -> reference id
+    uint64_t nnz_pad = 0;
+    AttractPlan plan{};
+    Buffers b{};
+    // allocations
+    std::vector<void *> allocs;
+    void *scratch = nullptr;
+    size_t scratch_bytes = 0;
+    float2 *stage_xy = nullptr;    // n, reference order
+    uint32_t *stage_ids = nullptr; // n
+    int bbox_blocks = 0, trav_blocks = 0;
+    cudaStream_t sA = nullptr, sB = nullptr;
+    cudaEvent_t evFork = nullptr, evJoin = nullptr;
+    // graphs
+    cudaGraphExec_t exec = nullptr;
+    cudaGraphExec_t exec_timed = nullptr;
+    cudaGraph_t graph_timed = nullptr;         // kept: its nodes address exec_timed
+    std::vector<cudaGraphNode_t> timed_nodes;  // event-record nodes, [slot*2 + start/end]
+    std::vector<cudaEvent_t> slot_events;      // events captured into the timed graph
+    std::vector<cudaEvent_t> event_pool;       // per (iteration, slot, start/end)
+    int last_perturb_rounds = 0;
+};
+
+namespace {
+
+int cuda_status(cudaError_t e) {
+    if (e == cudaSuccess) return FA2_OK;
+    if (e == cudaErrorMemoryAllocation) return FA2_ERR_OUT_OF_MEMORY;
+    return FA2_ERR_CUDA;
+}
+
+#define CK(call)                                   \
+    do {                                           \
+        cudaError_t e_ = (call);                   \
+        if (e_ != cudaSuccess) return cuda_status(e_); \
+    } while (0)
+
+template <typename T>
+int dalloc(fa2_ctx *c, T **p, size_t count) {
+    void *q = nullptr;
+    size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    CK(cudaMalloc(&q, bytes));
+    c->allocs.push_back(q);
+    *p = (T *)q;
+    return FA2_OK;
+}
+
+void free_all(fa2_ctx *c) {
+    if (c->exec) cudaGraphExecDestroy(c->exec);
+    if (c->exec_timed) cudaGraphExecDestroy(c->exec_timed);
+    if (c->graph_timed) cudaGraphDestroy(c->graph_timed);
+    for (cudaEvent_t e : c->slot_events) cudaEventDestroy(e);
+    for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
+    for (void *p : c->allocs) cudaFree(p);
+    c->allocs.clear();
+    if (c->evFork) cudaEventDestroy(c->evFork);
+    if (c->evJoin) cudaEventDestroy(c->evJoin);
+    if (c->sA) cudaStreamDestroy(c->sA);
+    if (c->sB) cudaStreamDestroy(c->sB);
+}
+
+// Nodes in degree-descending order (ties by reference id), a symmetric CSR
+// over that order with each row sorted and padded with its own id to a
+// multiple of four, and the attraction buckets over it.
+void build_graph(fa2_ctx *c, const fa2_graph_desc *g, std::vector<uint32_t> &off,
+                 std::vector<int32_t> &col, std::vector<float> &mass) {
+    const uint32_t n = c->n;
+    std::vector<uint32_t> deg(n, 0);
+    for (uint64_t e = 0; e < g->num_edges; ++e) {
+        deg[g->sources[e]]++;
+        deg[g->targets[e]]++;
+    }
+    c->ref_of.resize(n);
+    std::iota(c->ref_of.begin(), c->ref_of.end(), 0u);
+    std::stable_sort(c->ref_of.begin(), c->ref_of.end(),
+                     [&](uint32_t a, uint32_t b) { return deg[a] > deg[b]; });
+    std::vector<uint32_t> int_of(n);
+    for (uint32_t i = 0; i < n; ++i) int_of[c->ref_of[i]] = i;
+    off.assign((size_t)n + 1, 0);
+    mass.resize(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        uint32_t d = deg[c->ref_of[i]];
+        off[i + 1] = off[i] + ((d + 3u) & ~3u);
+        mass[i] = (float)d + 1.0f;  // ForceAtlas2::mass (src/RPForceAtlas2.cpp:74-77)
+    }
+    c->nnz_pad = off[n];
+    col.assign(std::max<uint64_t>(c->nnz_pad, 4), 0);
+    std::vector<uint32_t> fill(off.begin(), off.end() - 1);
+    for (uint64_t e = 0; e < g->num_edges; ++e) {
+        uint32_t a = int_of[g->sources[e]], b = int_of[g->targets[e]];
+        col[fill[a]++] = (int32_t)b;
+        col[fill[b]++] = (int32_t)a;
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        std::sort(col.begin() + off[i], col.begin() + fill[i]);
+        for (uint32_t q = fill[i]; q < off[i + 1]; ++q) col[q] = (int32_t)i;
+    }
+    // buckets: lanes per row from the number of 16-byte loads per row
+    auto lanes_for = [](uint32_t q) -> int {
+        if (q >= 512) return 256;
+        if (q > 16) return 32;
+        int l = 1;
+        while (l < (int)q) l <<= 1;
+        return l;
+    };
+    AttractPlan &P = c->plan;
+    memset(&P, 0, sizeof(P));
+    uint32_t r = 0;
+    int blocks = 0;
+    while (r < n && P.nbuckets < kMaxBuckets) {
+        int lanes = lanes_for((off[r + 1] - off[r]) / 4);
+        uint32_t r1 = r;
+        while (r1 < n && lanes_for((off[r1 + 1] - off[r1]) / 4) == lanes) ++r1;
+        AttractBucket &bk = P.b[P.nbuckets++];
+        bk.row_begin = (int)r;
+        bk.row_end = (int)r1;
+        bk.lanes = lanes;
+        bk.block_begin = blocks;
+        int rows_per_block = lanes == 256 ? 1 : (256 / 32) * (32 / lanes);
+        blocks += (int)((r1 - r + rows_per_block - 1) / rows_per_block);
+        r = r1;
+    }
+    P.nblocks = blocks;
+}
+
+// Enqueues one iteration.  full = false is the replay of a poisoned
+// iteration: gravity, attraction and the bounding box were computed from the
+// positions before the .99 scaling, as in the reference, and are kept.
+void enqueue_iteration(fa2_ctx *c, bool full, bool perturb_first, bool timed) {
+    const Buffers &b = c->b;
+    cudaStream_t A = c->sA, B = c->sB;
+    auto mark = [&](int slot, int end, cudaStream_t s) {
+        if (timed)
+            cudaEventRecordWithFlags(c->slot_events[slot * 2 + end], s, cudaEventRecordExternal);
+    };
+    cudaMemsetAsync(c->scratch, 0, c->scratch_bytes, A);
+    if (full) {
+        cudaEventRecord(c->evFork, A);
+        cudaStreamWaitEvent(B, c->evFork, 0);
+        mark(S_ATTRACT, 0, B);
+        launch_attract(b, c->kp, c->plan, B);
+        mark(S_ATTRACT, 1, B);
+        cudaEventRecord(c->evJoin, B);
+        mark(S_BBOX, 0, A);
+        launch_bbox(b, c->bbox_blocks, A);
+        mark(S_BBOX, 1, A);
+    }
+    if (perturb_first) launch_runs(b, 1, c->nsm, A);
+    mark(S_KEYS, 0, A);
+    launch_keys(b, c->nsm, A);
+    mark(S_KEYS, 1, A);
+    mark(S_SORT, 0, A);
+    launch_sort(b, A);
+    mark(S_SORT, 1, A);
+    mark(S_RUNS, 0, A);
+    launch_runs(b, 0, c->nsm, A);
+    mark(S_RUNS, 1, A);
+    mark(S_COUNT, 0, A);
+    launch_tree_count(b, A);
+    mark(S_COUNT, 1, A);
+    mark(S_EMIT, 0, A);
+    launch_emit(b, c->nsm, A);
+    mark(S_EMIT, 1, A);
+    mark(S_SUMM, 0, A);
+    launch_summarize(b, c->nsm, A);
+    mark(S_SUMM, 1, A);
+    if (full) cudaStreamWaitEvent(A, c->evJoin, 0);
+    mark(S_TRAV, 0, A);
+    launch_traverse(b, c->kp, c->trav_blocks, A);
+    mark(S_TRAV, 1, A);
+    mark(S_DISP, 0, A);
+    launch_displace(b, c->nsm, A);
+    mark(S_DISP, 1, A);
+}
+
+int capture(fa2_ctx *c, bool timed, cudaGraphExec_t *out) {
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(c->sA, cudaStreamCaptureModeThreadLocal));
+    enqueue_iteration(c, true, false, timed);
+    cudaError_t e = cudaStreamEndCapture(c->sA, &graph);
+    if (e != cudaSuccess) return cuda_status(e);
+    e = cudaGraphInstantiate(out, graph, 0);
+    if (e == cudaSuccess && timed) {
+        size_t nn = 0;
+        cudaGraphGetNodes(graph, nullptr, &nn);
+        std::vector<cudaGraphNode_t> nodes(nn);
+        cudaGraphGetNodes(graph, nodes.data(), &nn);
+        c->timed_nodes.assign(kNumSlots * 2, nullptr);
+        for (cudaGraphNode_t nd : nodes) {
+            cudaGraphNodeType t;
+            cudaGraphNodeGetType(nd, &t);
+            if (t != cudaGraphNodeTypeEventRecord) continue;
+            cudaEvent_t ev;
+            cudaGraphEventRecordNodeGetEvent(nd, &ev);
+            for (int s = 0; s < kNumSlots * 2; ++s)
+                if (c->slot_events[s] == ev) c->timed_nodes[s] = nd;
+        }
+    }
+    if (timed)
+        c->graph_timed = graph;
+    else
+        cudaGraphDestroy(graph);
+    return cuda_status(e);
+}
+
+int read_state(fa2_ctx *c, DevState *st) {
+    CK(cudaMemcpyAsync(st, c->b.st, sizeof(DevState), cudaMemcpyDeviceToHost, c->sA));
+    CK(cudaStreamSynchronize(c->sA));
+    return FA2_OK;
+}
+
+// Replays a poisoned iteration until no coincident bodies remain.
+int resolve_poison(fa2_ctx *c, DevState *st) {
+    int rounds = 0;
+    while (st->poison) {
+        if (++rounds > kMaxReplayRounds) return FA2_ERR_DEVICE_LIMIT;
+        CK(cudaMemsetAsync(&c->b.st->poison, 0, sizeof(int), c->sA));
+        enqueue_iteration(c, false, true, false);
+        CK(cudaGetLastError());
+        int s = read_state(c, st);
+        if (s) return s;
+        if (st->err) return FA2_ERR_DEVICE_LIMIT;
+    }
+    c->last_perturb_rounds = rounds;
+    return FA2_OK;
+}
+
+// Runs n iterations; with `timed`, kernel_sum accumulates per-slot device ms.
+int run_steps(fa2_ctx *c, int32_t n_iters, bool timed, std::vector<double> *kernel_sum,
+              std::vector<int> *kernel_cnt) {
+    if (n_iters <= 0 || c->n == 0) return FA2_OK;
+    cudaGraphExec_t *exec = timed ? &c->exec_timed : &c->exec;
+    if (!*exec) {
+        int s = capture(c, timed, exec);
+        if (s) return s;
+    }
+    DevState st;
+    int s = read_state(c, &st);
+    if (s) return s;
+    int done = 0;
+    c->last_perturb_rounds = 0;
+    while (done < n_iters) {
+        const int before = st.iters_done;
+        const int chunk = n_iters - done;
+        if (timed) {
+            size_t need = (size_t)chunk * kNumSlots * 2;
+            while (c->event_pool.size() < need) {
+                cudaEvent_t e;
+                CK(cudaEventCreate(&e));
+                c->event_pool.push_back(e);
+            }
+        }
+        for (int it = 0; it < chunk; ++it) {
+            if (timed)
+                for (int q = 0; q < kNumSlots * 2; ++q)
+                    if (c->timed_nodes[q])
+                        CK(cudaGraphExecEventRecordNodeSetEvent(
+                            *exec, c->timed_nodes[q], c->event_pool[(size_t)it * kNumSlots * 2 + q]));
+            CK(cudaGraphLaunch(*exec, c->sA));
+        }
+        s = read_state(c, &st);
+        if (s) return s;
+        if (st.err) return FA2_ERR_DEVICE_LIMIT;
+        int completed = st.iters_done - before;
+        if (timed && kernel_sum) {
+            for (int it = 0; it < completed; ++it)
+                for (int q = 0; q < kNumSlots; ++q) {
+                    if (!c->timed_nodes[2 * q] || !c->timed_nodes[2 * q + 1]) continue;
+                    float ms = 0.0f;
+                    size_t base = (size_t)it * kNumSlots * 2;
+                    if (cudaEventElapsedTime(&ms, c->event_pool[base + 2 * q],
+                                             c->event_pool[base + 2 * q + 1]) == cudaSuccess) {
+                        (*kernel_sum)[q] += ms;
+                        (*kernel_cnt)[q] += 1;
+                    }
+                }
+        }
+        done += completed;
+        if (st.poison) {
+            s = resolve_poison(c, &st);
+            if (s) return s;
+            done += 1;  // the replayed iteration completed
+        }
+    }
+    return FA2_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void fa2_default_params(fa2_params *p) {
+    if (!p) return;
+    p->use_barneshut = 1;
+    p->strong_gravity = 0;
+    p->gravity = 1.0f;
+    p->scale = 1.0f;
+    p->theta = 1.0f;
+    p->epssq = 0.05 * 0.05;
+    p->jitter_tolerance = 1.0f;
+    p->k_s_max = 10.0f;
+    p->device = 0;
+}
+
+fa2_ctx *fa2_create(const fa2_graph_desc *g, const fa2_params *prm, int *status) {
+    int dummy;
+    if (!status) status = &dummy;
+    *status = FA2_ERR_INVALID_ARGUMENT;
+    if (!g || !prm) return nullptr;
+    if (g->num_edges && (!g->sources || !g->targets)) return nullptr;
+    if (!prm->use_barneshut) {
+        *status = FA2_ERR_UNSUPPORTED;
+        return nullptr;
+    }
+    if (!(prm->theta > 0.0f)) return nullptr;
+    for (uint64_t e = 0; e < g->num_edges; ++e)
+        if (g->sources[e] >= g->num_nodes || g->targets[e] >= g->num_nodes ||
+            g->sources[e] == g->targets[e])
+            return nullptr;
+    if ((uint64_t)g->num_nodes * 2 + 2 * g->num_edges + 3ull * g->num_nodes >= (1ull << 32) ||
+        g->num_nodes >= (1u << 25)) {
+        *status = FA2_ERR_TOO_LARGE;
+        return nullptr;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= prm->device || prm->device < 0) {
+        *status = FA2_ERR_NO_DEVICE;
+        return nullptr;
+    }
+    cudaDeviceProp dp;
+    if (cudaGetDeviceProperties(&dp, prm->device) != cudaSuccess || dp.major < 10) {
+        *status = FA2_ERR_NO_DEVICE;
+        return nullptr;
+    }
+    if (cudaSetDevice(prm->device) != cudaSuccess) {
+        *status = FA2_ERR_CUDA;
+        return nullptr;
+    }
+    fa2_ctx *c = new fa2_ctx();
+    c->device = prm->device;
+    c->nsm = dp.multiProcessorCount;
+    c->n = g->num_nodes;
+    c->m = g->num_edges;
+    c->prm = *prm;
+    c->kp.k_r = prm->scale;
+    c->kp.k_g = prm->gravity;
+    c->kp.itolsq = 1.0f / (prm->theta * prm->theta);  // src/RPForceAtlas2.cpp:47
+    c->kp.epssq = prm->epssq;
+    c->kp.strong_gravity = prm->strong_gravity;
+
+    std::vector<uint32_t> off;
+    std::vector<int32_t> col;
+    std::vector<float> mass;
+    build_graph(c, g, off, col, mass);
+
+    auto fail = [&](int s) {
+        *status = s;
+        free_all(c);
+        delete c;
+        return (fa2_ctx *)nullptr;
+    };
+    const uint32_t n = c->n;
+    Buffers &b = c->b;
+    b.n = (int)n;
+    uint64_t cap = std::min<uint64_t>(33ull * n + 64, kMaxTreeNodes);
+    b.capacity = (uint32_t)cap;
+    uint32_t *d_off = nullptr, *d_ref = nullptr;
+    int4 *d_col = nullptr;
+    int s = FA2_OK;
+    if ((s = dalloc(c, &b.pos, n)) || (s = dalloc(c, &b.fprev, n)) || (s = dalloc(c, &b.f, n)) ||
+        (s = dalloc(c, &b.fag, n)) || (s = dalloc(c, &b.mass, n)) ||
+        (s = dalloc(c, &d_off, (size_t)n + 1)) || (s = dalloc(c, &d_col, col.size() / 4)) ||
+        (s = dalloc(c, &d_ref, n)) || (s = dalloc(c, &b.keys[0], n)) ||
+        (s = dalloc(c, &b.keys[1], n)) || (s = dalloc(c, &b.vals[0], n)) ||
+        (s = dalloc(c, &b.vals[1], n)) || (s = dalloc(c, &b.lcp, n)) ||
+        (s = dalloc(c, &b.group, n)) || (s = dalloc(c, &b.body_node, n)) ||
+        (s = dalloc(c, &b.nodes, cap)) || (s = dalloc(c, &b.parent, cap)) ||
+        (s = dalloc(c, &b.cnt, cap)) || (s = dalloc(c, &b.warp_partial, (n + 31) / 32)) ||
+        (s = dalloc(c, &b.st, 1)) || (s = dalloc(c, &c->stage_xy, n)) ||
+        (s = dalloc(c, &c->stage_ids, n)))
+        return fail(s);
+    c->bbox_blocks = c->nsm * 2;
+    if ((s = dalloc(c, &b.bbox_partial, c->bbox_blocks))) return fail(s);
+    b.csr_off = d_off;
+    b.csr_col4 = d_col;
+    b.ref_of = d_ref;
+    // one memset clears counters, histograms and look-back flags
+    const size_t sort_status = (size_t)8 * sort_tiles((int)n) * 256;
+    const size_t count_status = (size_t)count_tiles((int)n);
+    c->scratch_bytes = sizeof(IterCounters) + 4 * (sort_status + count_status);
+    char *scr = nullptr;
+    if ((s = dalloc(c, &scr, c->scratch_bytes))) return fail(s);
+    c->scratch = scr;
+    b.ctr = (IterCounters *)scr;
+    b.sort_status = (uint32_t *)(scr + sizeof(IterCounters));
+    b.count_status = b.sort_status + sort_status;
+
+    if (cudaStreamCreateWithFlags(&c->sA, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->sB, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->evFork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->evJoin, cudaEventDisableTiming) != cudaSuccess)
+        return fail(FA2_ERR_CUDA);
+    c->slot_events.resize(kNumSlots * 2);
+    for (auto &e : c->slot_events)
+        if (cudaEventCreate(&e) != cudaSuccess) return fail(FA2_ERR_CUDA);
+    sort_set_smem_attr();
+    c->trav_blocks = c->nsm * traverse_blocks_per_sm();
+
+    cudaStream_t A = c->sA;
+    if (cudaMemcpyAsync(d_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice, A) ||
+        cudaMemcpyAsync(d_col, col.data(), col.size() * 4, cudaMemcpyHostToDevice, A) ||
+        cudaMemcpyAsync(d_ref, c->ref_of.data(), (size_t)n * 4, cudaMemcpyHostToDevice, A) ||
+        cudaMemcpyAsync(b.mass, mass.data(), (size_t)n * 4, cudaMemcpyHostToDevice, A) ||
+        cudaMemsetAsync(b.pos, 0, (size_t)n * 8, A) || cudaMemsetAsync(b.fprev, 0, (size_t)n * 8, A) ||
+        cudaMemsetAsync(b.f, 0, (size_t)n * 8, A) || cudaMemsetAsync(b.fag, 0, (size_t)n * 8, A) ||
+        cudaMemsetAsync(b.st, 0, sizeof(DevState), A))
+        return fail(FA2_ERR_CUDA);
+    DevState st0;
+    memset(&st0, 0, sizeof(st0));
+    st0.global_speed = 1.0f;      // src/RPFA2Kernels.cu:30
+    st0.speed_efficiency = 1.0f;  // :31
+    st0.jitter_tolerance = prm->jitter_tolerance;
+    st0.k_s_max = prm->k_s_max;
+    if (cudaMemcpyAsync(b.st, &st0, sizeof(st0), cudaMemcpyHostToDevice, A) ||
+        cudaStreamSynchronize(A))
+        return fail(FA2_ERR_CUDA);
+    *status = FA2_OK;
+    return c;
+}
+
+void fa2_destroy(fa2_ctx *c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->sA) cudaStreamSynchronize(c->sA);
+    if (c->sB) cudaStreamSynchronize(c->sB);
+    free_all(c);
+    delete c;
+}
+
+int fa2_set_positions(fa2_ctx *c, const float *xy) {
+    if (!c || (!xy && c->n)) return FA2_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(c->device));
+    if (c->n == 0) return FA2_OK;
+    const size_t bytes = (size_t)c->n * 8;
+    CK(cudaMemcpyAsync(c->stage_xy, xy, bytes, cudaMemcpyHostToDevice, c->sA));
+    launch_scatter_xy((int)c->n, c->b.ref_of, c->stage_xy, c->b.pos, c->sA);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->sA));
+    return FA2_OK;
+}
+
+int fa2_get_positions(fa2_ctx *c, float *xy) {
+    if (!c || (!xy && c->n)) return FA2_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(c->device));
+    if (c->n == 0) return FA2_OK;
+    launch_gather_xy((int)c->n, c->b.ref_of, c->b.pos, c->stage_xy, c->sA);
+    CK(cudaMemcpyAsync(xy, c->stage_xy, (size_t)c->n * 8, cudaMemcpyDeviceToHost, c->sA));
+    CK(cudaStreamSynchronize(c->sA));
+    return FA2_OK;
+}
+
+int fa2_step(fa2_ctx *c, int32_t n_iters) {
+    if (!c || n_iters < 0) return FA2_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(c->device));
+    return run_steps(c, n_iters, false, nullptr, nullptr);
+}
+
+int fa2_step_timed(fa2_ctx *c, int32_t n_iters, float *ms_total, float *kernel_ms,
+                   int32_t n_kernels) {
+    if (!c || n_iters < 0 || !ms_total) return FA2_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(c->device));
+    cudaEvent_t t0, t1;
+    CK(cudaEventCreate(&t0));
+    CK(cudaEventCreate(&t1));
+    std::vector<double> sum(kNumSlots, 0.0);
+    std::vector<int> cnt(kNumSlots, 0);
+    cudaEventRecord(t0, c->sA);
+    int s = run_steps(c, n_iters, true, &sum, &cnt);
+    cudaEventRecord(t1, c->sA);
+    cudaEventSynchronize(t1);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, t0, t1);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    *ms_total = ms;
+    if (kernel_ms)
+        for (int q = 0; q < n_kernels && q < kNumSlots; ++q)
+            kernel_ms[q] = cnt[q] ? (float)(sum[q] / cnt[q]) : 0.0f;
+    return s;
+}
+
+const char *fa2_kernel_name(int32_t i) { return (i >= 0 && i < kNumSlots) ? kSlotNames[i] : nullptr; }
+
+int fa2_get_stats(fa2_ctx *c, fa2_stats *out) {
+    if (!c || !out) return FA2_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(c->device));
+    DevState st;
+    memset(&st, 0, sizeof(st));
+    if (c->n) {
+        int s = read_state(c, &st);
+        if (s) return s;
+    }
+    memset(out, 0, sizeof(*out));
+    out->num_bodies = c->n;
+    out->tree_nodes = st.tree_nodes;
+    out->tree_cells = st.tree_nodes >= c->n ? st.tree_nodes - c->n : 0;
+    out->max_level = st.max_level;
+    out->perturb_rounds = c->last_perturb_rounds;
+    out->device_error = st.err;
+    out->nnz_padded = c->nnz_pad;
+    out->global_speed = st.global_speed;
+    out->speed_efficiency = st.speed_efficiency;
+    out->radius = st.radius;
+    out->root_x = st.rootx;
+    out->root_y = st.rooty;
+    out->interactions = st.interactions;
+    out->visits = st.visits;
+    return FA2_OK;
+}
+
+int fa2_get_forces(fa2_ctx *c, float *f_total, float *f_attr_grav) {
+    if (!c) return FA2_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(c->device));
+    if (c->n == 0) return FA2_OK;
+    float *outs[2] = {f_total, f_attr_grav};
+    float2 *srcs[2] = {c->b.f, c->b.fag};
+    for (int q = 0; q < 2; ++q) {
+        if (!outs[q]) continue;
+        launch_gather_xy((int)c->n, c->b.ref_of, srcs[q], c->stage_xy, c->sA);
+        CK(cudaMemcpyAsync(outs[q], c->stage_xy, (size_t)c->n * 8, cudaMemcpyDeviceToHost, c->sA));
+        CK(cudaStreamSynchronize(c->sA));
+    }
+    return FA2_OK;
+}
+
+int fa2_get_sort_order(fa2_ctx *c, uint32_t *order) {
+    if (!c || (!order && c->n)) return FA2_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(c->device));
+    if (c->n == 0) return FA2_OK;
+    launch_sorted_ref_ids((int)c->n, c->b.ref_of, c->b.vals[0], c->stage_ids, c->sA);
+    CK(cudaMemcpyAsync(order, c->stage_ids, (size_t)c->n * 4, cudaMemcpyDeviceToHost, c->sA));
+    CK(cudaStreamSynchronize(c->sA));
+    return FA2_OK;
+}
+
+int fa2_set_speed_state(fa2_ctx *c, float global_speed, float speed_efficiency,
+                        const float *f_prev) {
+    if (!c) return FA2_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(c->device));
+    DevState st;
+    int s = read_state(c, &st);
+    if (s) return s;
+    st.global_speed = global_speed;
+    st.speed_efficiency = speed_efficiency;
+    CK(cudaMemcpyAsync(c->b.st, &st, sizeof(st), cudaMemcpyHostToDevice, c->sA));
+    if (c->n) {
+        if (f_prev) {
+            CK(cudaMemcpyAsync(c->stage_xy, f_prev, (size_t)c->n * 8, cudaMemcpyHostToDevice, c->sA));
+            launch_scatter_xy((int)c->n, c->b.ref_of, c->stage_xy, c->b.fprev, c->sA);
+        } else {
+            CK(cudaMemsetAsync(c->b.fprev, 0, (size_t)c->n * 8, c->sA));
+        }
+    }
+    CK(cudaStreamSynchronize(c->sA));
+    return FA2_OK;
+}
+
+int fa2_get_speed_state(fa2_ctx *c, float *global_speed, float *speed_efficiency,
+                        float *f_prev) {
+    if (!c) return FA2_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(c->device));
+    DevState st;
+    int s = read_state(c, &st);
+    if (s) return s;
+    if (global_speed) *global_speed = st.global_speed;
+    if (speed_efficiency) *speed_efficiency = st.speed_efficiency;
+    if (f_prev && c->n) {
+        launch_gather_xy((int)c->n, c->b.ref_of, c->b.fprev, c->stage_xy, c->sA);
+        CK(cudaMemcpyAsync(f_prev, c->stage_xy, (size_t)c->n * 8, cudaMemcpyDeviceToHost, c->sA));
+        CK(cudaStreamSynchronize(c->sA));
+    }
+    return FA2_OK;
+}
+
+int fa2_set_force_params(fa2_ctx *c, float scale, float gravity) {
+    if (!c) return FA2_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(c->device));
+    if (c->kp.k_r == scale && c->kp.k_g == gravity) return FA2_OK;
+    CK(cudaStreamSynchronize(c->sA));
+    c->kp.k_r = scale;
+    c->kp.k_g = gravity;
+    c->prm.scale = scale;
+    c->prm.gravity = gravity;
+    // the captured graphs hold the old values as kernel arguments
+    if (c->exec) cudaGraphExecDestroy(c->exec);
+    if (c->exec_timed) cudaGraphExecDestroy(c->exec_timed);
+    if (c->graph_timed) cudaGraphDestroy(c->graph_timed);
+    c->exec = c->exec_timed = nullptr;
+    c->graph_timed = nullptr;
+    return FA2_OK;
+}
+
+const char *fa2_status_string(int s) {
+    switch (s) {
+        case FA2_OK: return "ok";
+        case FA2_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case FA2_ERR_NO_DEVICE: return "no usable CUDA device (sm_100 required)";
+        case FA2_ERR_CUDA: return "CUDA runtime error";
+        case FA2_ERR_OUT_OF_MEMORY: return "out of device memory";
+        case FA2_ERR_DEVICE_LIMIT: return "device-side limit reached";
+        case FA2_ERR_TOO_LARGE: return "graph too large for this engine";
+        case FA2_ERR_UNSUPPORTED: return "unsupported option";
+        case FA2_ERR_IO: return "file could not be read or written";
+        default: return "unknown status";
+    }
+}
+
+const char *fa2_version(void) { return "fa2b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

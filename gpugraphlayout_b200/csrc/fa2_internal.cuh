@@ -1,0 +1,143 @@
+// fa2_internal.cuh -- device data layout and kernel entry points of the B200
+// ForceAtlas2 engine.  Host code in fa2_capi.cu enqueues one iteration as
+//
+//   stream A: bbox -> keys -> sort (8 passes) -> runs -> tree_count -> emit
+//             -> summarize -> [join B] -> traverse (+ speed) -> displace
+//   stream B: attract (gravity + attraction)
+//
+// which replaces the eleven launches of CUDAForceAtlas2::doStep
+// (src/RPGPUForceAtlas2.cu:206-248 of the reference).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fa2 {
+
+constexpr int kWarp = 32;
+constexpr int kLevels = 32;        // quadrant digits in a 64-bit Morton key
+constexpr int kBodyLevel = 63;     // level code of a body (leaf) node
+constexpr int kMetaShift = 6;      // node meta = next_index << 6 | level code
+constexpr uint32_t kMaxTreeNodes = 1u << 26;
+constexpr int kMaxRun = 1024;      // longest run of equal 64-bit keys handled
+constexpr int kDeepLevels = 64;    // levels past 32 used to order such a run
+
+// Device error bits (DevState::err).  Any of them stops the iteration.
+enum : int {
+    kErrSortWait = 1,      // a sort tile waited too long on its predecessor
+    kErrScanWait = 2,      // a tree-count tile waited too long
+    kErrRunTooLong = 4,    // more than kMaxRun bodies share a 64-bit key
+    kErrTreeTooLarge = 8,  // the quadtree needs more nodes than allocated
+};
+
+// Scalars that live on the device for the whole run.
+struct DevState {
+    float minx, maxx, miny, maxy;        // bounding box of the positions
+    float radius, rootx, rooty;          // root cell (src/RPBHKernels.cu:140-148)
+    float global_speed, speed_efficiency; // src/RPFA2Kernels.cu:29-33, per context here
+    float jitter_tolerance, k_s_max;
+    int poison;          // coincident bodies seen: this iteration is replayed
+    int err;             // kErr* bits
+    int iters_done;      // completed iterations
+    uint32_t tree_nodes; // nodes of the last quadtree
+    int max_level;
+    float swg_sum, etra_sum;
+    unsigned long long interactions;  // body-node force terms of the last traversal
+    unsigned long long visits;        // body-node acceptance tests of the last traversal
+};
+
+// Per-iteration scratch, cleared by one memset at the start of an iteration.
+struct IterCounters {
+    unsigned bbox_done;
+    unsigned sort_ticket[8];
+    unsigned count_ticket;
+    unsigned trav_ticket;
+    unsigned trav_done;
+    unsigned pad[4];
+    unsigned hist[8][256];  // per-pass digit histograms of the sort keys
+};
+
+// Sort geometry (one tile per block).
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / kWarp;
+constexpr int kSortRounds = 16;
+constexpr int kSortTile = kSortThreads * kSortRounds;  // 4096 keys
+constexpr int kCountThreads = 256;
+constexpr int kCountItems = 4;
+constexpr int kCountTile = kCountThreads * kCountItems;  // 1024 bodies
+
+inline int sort_tiles(int n) { return (n + kSortTile - 1) / kSortTile; }
+inline int count_tiles(int n) { return (n + kCountTile - 1) / kCountTile; }
+
+// Attraction work split: rows (nodes in degree-descending order) with the
+// same number of lanes per row form one contiguous bucket.
+struct AttractBucket {
+    int row_begin, row_end;  // rows [row_begin, row_end)
+    int lanes;               // lanes per row: 256 (one block), 32, 16, ..., 1
+    int block_begin;         // first block index of this bucket
+};
+constexpr int kMaxBuckets = 8;
+struct AttractPlan {
+    AttractBucket b[kMaxBuckets];
+    int nbuckets;
+    int nblocks;
+};
+
+struct Buffers {
+    int n;
+    // per node, internal (degree-descending) order
+    float2 *pos, *fprev, *f, *fag;
+    float *mass;
+    const uint32_t *csr_off;  // n + 1, padded-row offsets (multiples of 4)
+    const int4 *csr_col4;     // neighbour ids in fours
+    const uint32_t *ref_of;   // internal id -> reference id
+    // sort
+    uint64_t *keys[2];
+    uint32_t *vals[2];
+    // tree
+    int8_t *lcp;              // n
+    uint32_t *group;          // n: first preorder node of body k's group
+    uint32_t *body_node;      // n: preorder node of sorted body k
+    float4 *nodes;            // capacity: x, y, mass, meta
+    int32_t *parent;          // capacity
+    int32_t *cnt;             // capacity: child counters
+    uint32_t capacity;
+    // reductions
+    float4 *bbox_partial;     // bbox blocks
+    float2 *warp_partial;     // one per 32 sorted bodies
+    DevState *st;
+    IterCounters *ctr;
+    uint32_t *sort_status;    // [8][sort tiles][256]
+    uint32_t *count_status;   // [count tiles]
+};
+
+struct Params {
+    float k_r, k_g, itolsq, epssq;
+    int strong_gravity;
+};
+
+constexpr int kBBoxThreads = 512;
+constexpr int kTravThreads = 256;
+constexpr int kDispThreads = 512;
+
+// ---------------------------------------------------------------- kernels --
+void launch_bbox(const Buffers &b, int nblocks, cudaStream_t s);
+void launch_keys(const Buffers &b, int nsm, cudaStream_t s);
+void launch_sort(const Buffers &b, cudaStream_t s);
+void launch_runs(const Buffers &b, int perturb, int nsm, cudaStream_t s);
+void launch_tree_count(const Buffers &b, cudaStream_t s);
+void launch_emit(const Buffers &b, int nsm, cudaStream_t s);
+void launch_summarize(const Buffers &b, int nsm, cudaStream_t s);
+void launch_traverse(const Buffers &b, const Params &p, int nblocks, cudaStream_t s);
+void launch_displace(const Buffers &b, int nsm, cudaStream_t s);
+void launch_attract(const Buffers &b, const Params &p, const AttractPlan &plan, cudaStream_t s);
+void launch_scatter_xy(int n, const uint32_t *ref_of, const float2 *src_ref, float2 *dst_int,
+                       cudaStream_t s);
+void launch_gather_xy(int n, const uint32_t *ref_of, const float2 *src_int, float2 *dst_ref,
+                      cudaStream_t s);
+void launch_sorted_ref_ids(int n, const uint32_t *ref_of, const uint32_t *vals, uint32_t *out,
+                           cudaStream_t s);
+void sort_set_smem_attr();
+int traverse_blocks_per_sm();
+
+}  // namespace fa2

@@ -1,0 +1,871 @@
+// fa2_kernels.cu -- the per-iteration kernels of the B200 ForceAtlas2 engine
+// except the radix sort (fa2_sort.cu).
+//
+// Quadtree.  The reference builds its quadtree by concurrent lock-based
+// insertion (src/RPBHKernels.cu:184-329); the shape of that tree does not
+// depend on insertion order: its cells are exactly the quadrant prefixes that
+// hold at least two bodies.  Here the same tree is built without locks:
+//   keys        each body's 32 quadrant digits, computed with the reference's
+//               float cell-centre arithmetic and tie rule (:217-241), form a
+//               64-bit Morton key;
+//   sort        keys ascending = the reference's in-order body order (sortd);
+//   runs        equal keys (only possible past depth 32) are ordered by
+//               deeper digits; exactly coincident bodies are flagged;
+//   tree_count  LCP of neighbouring keys (in quadrant digits) gives, per
+//               body k, the cells that start at k: levels L[k-1]+1 .. L[k];
+//               a scan gives every node its preorder index;
+//   emit        writes each node once: position/mass of bodies, level and
+//               subtree end of cells, parent links;
+//   summarize   bottom-up mass and centre of mass, children in quadrant order
+//               (SummarizationKernel :357-506), with the last child to finish
+//               computing its parent instead of spin-waiting.
+// The tree is stored in preorder with each node's "next" index (the node
+// after its subtree), so the traversal needs no stack.
+#include <float.h>
+#include <stdint.h>
+
+#include "fa2_internal.cuh"
+
+namespace fa2 {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ int lcp_digits(uint64_t a, uint64_t b) {
+    uint64_t x = a ^ b;
+    return x == 0 ? kLevels : (__clzll(x) >> 1);
+}
+
+__device__ __forceinline__ int meta_level(int meta) { return meta & 63; }
+__device__ __forceinline__ uint32_t meta_next(int meta) { return (uint32_t)meta >> kMetaShift; }
+__device__ __forceinline__ float make_meta(uint32_t next, int level) {
+    return __int_as_float((int)((next << kMetaShift) | (uint32_t)level));
+}
+
+// Quadrant digits of (px, py) under the root cell, computed the way
+// TreeBuildingKernel walks down (src/RPBHKernels.cu:217-241): the child
+// centre is the parent centre +/- r, r halving per level; a coordinate
+// equal to the centre goes to the low side.
+__device__ __forceinline__ uint64_t morton_key(float px, float py, float x, float y, float r) {
+    uint64_t key = 0;
+#pragma unroll 8
+    for (int lvl = 0; lvl < kLevels; ++lvl) {
+        r *= 0.5f;
+        int j = 0;
+        float dx = -r, dy = -r;
+        if (x < px) {
+            j = 1;
+            dx = r;
+        }
+        if (y < py) {
+            j |= 2;
+            dy = r;
+        }
+        x = __fadd_rn(x, dx);
+        y = __fadd_rn(y, dy);
+        key = (key << 2) | (uint64_t)j;
+    }
+    return key;
+}
+
+// ------------------------------------------------------------------- bbox --
+
+__global__ void __launch_bounds__(kBBoxThreads) k_bbox(int n, const float2 *__restrict pos,
+                                                       float4 *__restrict partial,
+                                                       DevState *st, IterCounters *ctr) {
+    __shared__ float4 s_w[kBBoxThreads / kWarp];
+    __shared__ bool s_last;
+    if (st->err || st->poison) return;
+    float mnx = FLT_MAX, mxx = -FLT_MAX, mny = FLT_MAX, mxy = -FLT_MAX;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float2 p = pos[i];
+        mnx = fminf(mnx, p.x);
+        mxx = fmaxf(mxx, p.x);
+        mny = fminf(mny, p.y);
+        mxy = fmaxf(mxy, p.y);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mnx = fminf(mnx, __shfl_xor_sync(kFull, mnx, o));
+        mxx = fmaxf(mxx, __shfl_xor_sync(kFull, mxx, o));
+        mny = fminf(mny, __shfl_xor_sync(kFull, mny, o));
+        mxy = fmaxf(mxy, __shfl_xor_sync(kFull, mxy, o));
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) s_w[wid] = make_float4(mnx, mxx, mny, mxy);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float4 a = s_w[0];
+        for (int w = 1; w < kBBoxThreads / kWarp; ++w) {
+            float4 b = s_w[w];
+            a = make_float4(fminf(a.x, b.x), fmaxf(a.y, b.y), fminf(a.z, b.z), fmaxf(a.w, b.w));
+        }
+        partial[blockIdx.x] = a;
+        __threadfence();
+        s_last = atomicAdd(&ctr->bbox_done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (s_last && threadIdx.x == 0) {
+        __threadfence();
+        float4 a = __ldcg(&partial[0]);
+        for (int b = 1; b < (int)gridDim.x; ++b) {
+            float4 c = __ldcg(&partial[b]);
+            a = make_float4(fminf(a.x, c.x), fmaxf(a.y, c.y), fminf(a.z, c.z), fmaxf(a.w, c.w));
+        }
+        st->minx = a.x;
+        st->maxx = a.y;
+        st->miny = a.z;
+        st->maxy = a.w;
+        // src/RPBHKernels.cu:140-148
+        st->radius = fmaxf(a.y - a.x, a.w - a.z) * 0.5f;
+        st->rootx = (a.x + a.y) * 0.5f;
+        st->rooty = (a.z + a.w) * 0.5f;
+    }
+}
+
+// ------------------------------------------------------------------- keys --
+
+__global__ void __launch_bounds__(256) k_keys(int n, const float2 *__restrict pos,
+                                              const DevState *__restrict st,
+                                              uint64_t *__restrict keys, uint32_t *__restrict vals,
+                                              IterCounters *ctr) {
+    __shared__ unsigned s_hist[8][256];
+    if (st->err || st->poison) return;
+    for (int j = threadIdx.x; j < 8 * 256; j += blockDim.x) (&s_hist[0][0])[j] = 0;
+    __syncthreads();
+    const float rx = st->rootx, ry = st->rooty, rr = st->radius;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float2 p = pos[i];
+        uint64_t key = morton_key(p.x, p.y, rx, ry, rr);
+        keys[i] = key;
+        vals[i] = (uint32_t)i;
+#pragma unroll
+        for (int ps = 0; ps < 8; ++ps) atomicAdd(&s_hist[ps][(key >> (8 * ps)) & 255], 1u);
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < 8 * 256; j += blockDim.x) {
+        unsigned c = (&s_hist[0][0])[j];
+        if (c) atomicAdd(&(&ctr->hist[0][0])[j], c);
+    }
+}
+
+// ------------------------------------------------------------------- runs --
+
+// Replays the cell centre of a 32-digit key path.
+__device__ __forceinline__ void key_centre(uint64_t key, float rx, float ry, float rr, float &x,
+                                           float &y, float &r) {
+    x = rx;
+    y = ry;
+    r = rr;
+    for (int lvl = 0; lvl < kLevels; ++lvl) {
+        r *= 0.5f;
+        int j = (int)(key >> (2 * (kLevels - 1 - lvl))) & 3;
+        x = __fadd_rn(x, (j & 1) ? r : -r);
+        y = __fadd_rn(y, (j & 2) ? r : -r);
+    }
+}
+
+// Orders two bodies that share all 32 digits by the digits below level 32
+// (the reference keeps splitting: src/RPBHKernels.cu:282-313), then by
+// reference id.  Returns true if a goes first.
+__device__ bool deep_less(float2 pa, float2 pb, uint32_t ida, uint32_t idb, float x, float y,
+                          float r) {
+    for (int lvl = 0; lvl < kDeepLevels; ++lvl) {
+        r *= 0.5f;
+        int ja = (x < pa.x ? 1 : 0) | (y < pa.y ? 2 : 0);
+        int jb = (x < pb.x ? 1 : 0) | (y < pb.y ? 2 : 0);
+        if (ja != jb) return ja < jb;
+        x = __fadd_rn(x, (ja & 1) ? r : -r);
+        y = __fadd_rn(y, (ja & 2) ? r : -r);
+    }
+    return ida < idb;
+}
+
+// One thread per run of equal keys: order the run, then either flag exactly
+// coincident bodies (perturb == 0) or scale every body that sits on an
+// earlier one (lower reference id) by .99, as the reference's insertion does
+// for the later-inserted body (src/RPBHKernels.cu:271-278).
+__global__ void __launch_bounds__(256) k_runs(int n, const uint64_t *__restrict keys,
+                                              uint32_t *__restrict vals, float2 *__restrict pos,
+                                              const uint32_t *__restrict ref_of, DevState *st,
+                                              int perturb) {
+    if (st->err || st->poison) return;
+    const float rx = st->rootx, ry = st->rooty, rr = st->radius;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k + 1 < n; k += gridDim.x * blockDim.x) {
+        uint64_t key = keys[k];
+        if (keys[k + 1] != key || (k > 0 && keys[k - 1] == key)) continue;
+        int len = 2;
+        while (k + len < n && keys[k + len] == key && len <= kMaxRun) ++len;
+        if (len > kMaxRun) {
+            atomicOr(&st->err, kErrRunTooLong);
+            continue;
+        }
+        float cx, cy, cr;
+        key_centre(key, rx, ry, rr, cx, cy, cr);
+        uint32_t *v = vals + k;
+        for (int a = 1; a < len; ++a) {  // insertion sort, stable
+            uint32_t va = v[a];
+            float2 pa = pos[va];
+            int b = a - 1;
+            while (b >= 0) {
+                uint32_t vb = v[b];
+                if (!deep_less(pa, pos[vb], ref_of[va], ref_of[vb], cx, cy, cr)) break;
+                v[b + 1] = vb;
+                --b;
+            }
+            v[b + 1] = va;
+        }
+        // coincident neighbours (equal positions are adjacent after ordering)
+        bool any = false;
+        float2 prev = pos[v[0]];
+        for (int a = 1; a < len; ++a) {
+            float2 p = pos[v[a]];
+            bool same = p.x == prev.x && p.y == prev.y;
+            prev = p;
+            if (!same) continue;
+            any = true;
+            if (perturb) pos[v[a]] = make_float2((float)((double)p.x * .99), (float)((double)p.y * .99));
+        }
+        if (any && !perturb) atomicAdd(&st->poison, 1);
+    }
+}
+
+// ------------------------------------------------------------- tree count --
+
+__device__ __forceinline__ int lcp_at(const uint64_t *__restrict keys, int n, int k) {
+    return (k < 0 || k >= n - 1) ? -1 : lcp_digits(keys[k], keys[k + 1]);
+}
+
+// cells that start at sorted body k
+__device__ __forceinline__ int cells_at(int k, int Lk, int Lkm1) {
+    return k == 0 ? max(Lk, 0) + 1 : max(0, Lk - Lkm1);
+}
+
+__global__ void __launch_bounds__(kCountThreads) k_tree_count(
+    int n, const uint64_t *__restrict keys, int8_t *__restrict lcp, uint32_t *__restrict group,
+    int32_t *__restrict cnt, uint32_t capacity, DevState *st, IterCounters *ctr,
+    uint32_t *status) {
+    __shared__ int s_tile;
+    __shared__ uint32_t s_warp[kCountThreads / kWarp];
+    __shared__ uint32_t s_prefix;
+    if (st->err || st->poison) return;
+    if (threadIdx.x == 0) s_tile = atomicAdd(&ctr->count_ticket, 1u);
+    __syncthreads();
+    const int tile = s_tile;
+    const int base = tile * kCountTile + threadIdx.x * kCountItems;
+    int g[kCountItems];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int e = 0; e < kCountItems; ++e) {
+        int k = base + e;
+        g[e] = 0;
+        if (k < n) {
+            int Lk = lcp_at(keys, n, k);
+            int Lkm1 = lcp_at(keys, n, k - 1);
+            lcp[k] = (int8_t)Lk;
+            g[e] = cells_at(k, Lk, Lkm1) + 1;
+        }
+        sum += (uint32_t)g[e];
+    }
+    // block exclusive scan of per-thread sums
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t inc = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(kFull, inc, o);
+        if (lane >= o) inc += t;
+    }
+    if (lane == 31) s_warp[wid] = inc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (int w = 0; w < kCountThreads / kWarp; ++w) {
+            uint32_t t = s_warp[w];
+            s_warp[w] = run;
+            run += t;
+        }
+        // decoupled look-back over tiles: flag in bit 31, value below
+        const uint32_t kAgg = 1u << 30, kPre = 2u << 30, kMask = (1u << 30) - 1;
+        uint32_t prefix = 0;
+        if (tile == 0) {
+            atomicExch(&status[0], kPre | run);
+        } else {
+            atomicExch(&status[tile], kAgg | run);
+            int t = tile - 1;
+            long spins = 0;
+            while (t >= 0) {
+                uint32_t s = *((volatile uint32_t *)&status[t]);
+                if ((s >> 30) == 0) {
+                    if (++spins > (1L << 22)) {
+                        atomicOr(&st->err, kErrScanWait);
+                        break;
+                    }
+                    continue;
+                }
+                prefix += s & kMask;
+                if ((s >> 30) == 2) break;
+                --t;
+            }
+            atomicExch(&status[tile], kPre | (prefix + run));
+        }
+        s_prefix = prefix;
+    }
+    __syncthreads();
+    uint32_t off = s_prefix + s_warp[wid] + inc - sum;
+#pragma unroll
+    for (int e = 0; e < kCountItems; ++e) {
+        int k = base + e;
+        if (k < n) {
+            group[k] = off;
+            for (int q = 0; q < g[e]; ++q)
+                if (off + q < capacity) cnt[off + q] = 0;
+            if (k == n - 1) {
+                uint32_t total = off + (uint32_t)g[e];
+                st->tree_nodes = total;
+                st->max_level = 0;  // raised by k_emit
+                st->interactions = 0;  // counted by k_traverse
+                st->visits = 0;
+                if (total > capacity) atomicOr(&st->err, kErrTreeTooLarge);
+            }
+        }
+        off += (uint32_t)g[e];
+    }
+}
+
+// ------------------------------------------------------------------- emit --
+
+__device__ __forceinline__ int load_lcp(const int8_t *__restrict lcp, int n, int k) {
+    return (k < 0 || k >= n - 1) ? -1 : (int)lcp[k];
+}
+
+// preorder index of sorted body b
+__device__ __forceinline__ uint32_t body_index(const int8_t *__restrict lcp,
+                                               const uint32_t *__restrict group, int n, int b) {
+    int Lb = load_lcp(lcp, n, b), Lbm1 = load_lcp(lcp, n, b - 1);
+    return group[b] + (uint32_t)cells_at(b, Lb, Lbm1);
+}
+
+// Index of the cell at level lam that contains sorted body k, given that it
+// starts before k: its first body a is the smallest j with LCP(K_j, K_k) >= lam.
+__device__ uint32_t find_cell(const uint64_t *__restrict keys, const int8_t *__restrict lcp,
+                              const uint32_t *__restrict group, int n, int k, int lam) {
+    const uint64_t kk = keys[k];
+    int ok = k - 1;  // known to satisfy
+    int step = 1, bad = -1;
+    for (;;) {
+        int j = ok - step;
+        if (j < 0) {
+            bad = -1;
+            break;
+        }
+        if (lcp_digits(keys[j], kk) >= lam) {
+            ok = j;
+            step <<= 1;
+        } else {
+            bad = j;
+            break;
+        }
+    }
+    // smallest satisfying index in (bad, ok]
+    int lo = bad + 1, hi = ok;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (lcp_digits(keys[mid], kk) >= lam)
+            hi = mid;
+        else
+            lo = mid + 1;
+    }
+    const int a = lo;
+    const int lo_level = a == 0 ? 0 : load_lcp(lcp, n, a - 1) + 1;
+    return group[a] + (uint32_t)(lam - lo_level);
+}
+
+// Largest j >= k with LCP(K_k, K_j) >= lvl (the last body of the cell at
+// level lvl that starts at k).
+__device__ int find_end(const uint64_t *__restrict keys, int n, int k, int lvl) {
+    const uint64_t kk = keys[k];
+    int ok = k, step = 1, bad = n;
+    for (;;) {
+        int j = ok + step;
+        if (j >= n) {
+            bad = n;
+            break;
+        }
+        if (lcp_digits(keys[j], kk) >= lvl) {
+            ok = j;
+            step <<= 1;
+        } else {
+            bad = j;
+            break;
+        }
+    }
+    int lo = ok, hi = bad - 1;  // largest satisfying in [ok, bad)
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (lcp_digits(keys[mid], kk) >= lvl)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(256) k_emit(int n, const uint64_t *__restrict keys,
+                                              const uint32_t *__restrict vals,
+                                              const int8_t *__restrict lcp,
+                                              const uint32_t *__restrict group,
+                                              const float2 *__restrict pos,
+                                              const float *__restrict mass, float4 *__restrict nodes,
+                                              int32_t *__restrict parent, int32_t *__restrict cnt,
+                                              uint32_t *__restrict body_node, DevState *st) {
+    if (st->err || st->poison) return;
+    int local_max = 0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int Lk = load_lcp(lcp, n, k), Lkm1 = load_lcp(lcp, n, k - 1);
+        const int c = cells_at(k, Lk, Lkm1);
+        const uint32_t Gk = group[k];
+        const uint32_t bnode = Gk + (uint32_t)c;
+        const int lo_level = k == 0 ? 0 : Lkm1 + 1;
+        // the body
+        const uint32_t i = vals[k];
+        const float2 p = pos[i];
+        nodes[bnode] = make_float4(p.x, p.y, mass[i], make_meta(bnode + 1, kBodyLevel));
+        body_node[k] = bnode;
+        const int lam = max(max(Lk, Lkm1), 0);
+        const uint32_t pb = c > 0 ? bnode - 1 : find_cell(keys, lcp, group, n, k, lam);
+        parent[bnode] = (int32_t)pb;
+        atomicAdd(&cnt[pb], 1);
+        // the cells that start here, outermost first
+        for (int q = 0; q < c; ++q) {
+            const int lvl = lo_level + q;
+            const uint32_t node = Gk + (uint32_t)q;
+            const int b = lvl == 0 ? n - 1 : find_end(keys, n, k, lvl);
+            const uint32_t next = body_index(lcp, group, n, b) + 1;
+            nodes[node] = make_float4(0.0f, 0.0f, 0.0f, make_meta(next, lvl));
+            int32_t par = -1;
+            if (q > 0)
+                par = (int32_t)node - 1;
+            else if (lvl > 0)
+                par = (int32_t)find_cell(keys, lcp, group, n, k, lvl - 1);
+            parent[node] = par;
+            if (par >= 0) atomicAdd(&cnt[par], 1);
+            local_max = max(local_max, lvl);
+        }
+    }
+    local_max = __reduce_max_sync(kFull, local_max);
+    if ((threadIdx.x & 31) == 0 && local_max > 0) atomicMax(&st->max_level, local_max);
+}
+
+// -------------------------------------------------------------- summarize --
+
+// Bottom-up cell mass and centre of mass.  Every node decrements its
+// parent's child counter; the child that brings it to zero computes the
+// parent from all its children, in quadrant order, as SummarizationKernel
+// does (src/RPBHKernels.cu:461-494), and continues upwards.
+__global__ void __launch_bounds__(256) k_summarize(int n, const uint32_t *__restrict body_node,
+                                                   const int32_t *__restrict parent,
+                                                   int32_t *cnt, float4 *nodes, DevState *st) {
+    if (st->err || st->poison) return;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        int32_t p = parent[body_node[k]];
+        while (p >= 0) {
+            __threadfence();
+            if (atomicSub(&cnt[p], 1) != 1) break;
+            __threadfence();
+            const float4 prec = __ldcg(&nodes[p]);
+            const uint32_t end = meta_next(__float_as_int(prec.w));
+            float cm = 0.0f, px = 0.0f, py = 0.0f;
+            for (uint32_t c = (uint32_t)p + 1; c < end;) {
+                const float4 r = __ldcg(&nodes[c]);
+                const float m = r.z;
+                px += r.x * m;
+                py += r.y * m;
+                cm += m;
+                c = meta_next(__float_as_int(r.w));
+            }
+            const float inv = 1.0f / cm;
+            __stcg(&nodes[p], make_float4(px * inv, py * inv, cm, prec.w));
+            p = __ldcg(&parent[p]);
+        }
+    }
+}
+
+// --------------------------------------------------------------- traverse --
+
+// Repulsion by a warp-cooperative preorder walk.  The 32 lanes of a warp
+// hold 32 consecutive bodies of the sorted order, as the reference's
+// ForceCalculationKernel does (src/RPBHKernels.cu:609-685); a cell is used as
+// a whole only if every lane passes d^2 + eps >= dq[level] (:661), else the
+// warp descends into it.  Bodies always interact.  The walk visits nodes in
+// the reference's order, so each lane adds the same terms in the same order.
+// The tail adds gravity + attraction, forms the swing and traction sums
+// (SpeedKernel, src/RPFA2Kernels.cu:111-202) and, in the last block to
+// finish, updates the adaptive speed (:204-219).
+__global__ void __launch_bounds__(kTravThreads) k_traverse(
+    int n, const float4 *__restrict nodes, const uint32_t *__restrict body_node,
+    const uint32_t *__restrict vals, const float2 *__restrict fag,
+    const float2 *__restrict fprev, float2 *__restrict f, float2 *__restrict warp_partial,
+    DevState *st, IterCounters *ctr, Params prm) {
+    __shared__ float s_dq[64];
+    __shared__ bool s_last;
+    __shared__ float s_red[2][kTravThreads / kWarp];
+    if (st->err || st->poison) return;
+    if (threadIdx.x == 0) {
+        // src/RPBHKernels.cu:579-592: dq for the children of the root is
+        // (2 radius)^2 / theta^2 + eps, quartering per level.
+        float tmp = st->radius * 2;
+        float dq = tmp * tmp * prm.itolsq;
+        s_dq[0] = 0.0f;
+        for (int l = 1; l <= kLevels; ++l) {
+            s_dq[l] = dq + prm.epssq;
+            dq = dq * 0.25f;
+        }
+        for (int l = kLevels + 1; l < 64; ++l) s_dq[l] = 0.0f;
+    }
+    __syncthreads();
+    const uint32_t end = st->tree_nodes;
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (n + 31) >> 5;
+    for (;;) {
+        int w = 0;
+        if (lane == 0) w = (int)atomicAdd(&ctr->trav_ticket, 1u);
+        w = __shfl_sync(kFull, w, 0);
+        if (w >= nwarps) break;
+        const int k = w * 32 + lane;
+        const bool active = k < n;
+        const float4 me = nodes[body_node[active ? k : n - 1]];
+        const float px = me.x, py = me.y, kmi = prm.k_r * me.z;
+        float ax = 0.0f, ay = 0.0f;
+        uint32_t node = 1, n_acc = 0, n_vis = 0;
+        while (node < end) {
+            const float4 r = __ldg(&nodes[node]);
+            const float dx = px - r.x, dy = py - r.y;
+            const float d2 = dx * dx + dy * dy + prm.epssq;
+            const int meta = __float_as_int(r.w);
+            const bool ok = !active || d2 >= s_dq[meta_level(meta)];
+            ++n_vis;
+            if (__all_sync(kFull, ok)) {
+                const float c = kmi * r.z / d2;
+                ax = fmaf(dx, c, ax);
+                ay = fmaf(dy, c, ay);
+                node = meta_next(meta);
+                ++n_acc;
+            } else {
+                ++node;
+            }
+        }
+        if (lane == 0) {
+            const unsigned lanes = (unsigned)min(32, n - w * 32);
+            atomicAdd(&st->interactions, (unsigned long long)n_acc * lanes);
+            atomicAdd(&st->visits, (unsigned long long)n_vis * lanes);
+        }
+        float sw = 0.0f, tr = 0.0f;
+        if (active) {
+            const uint32_t i = vals[k];
+            const float2 g = fag[i], fp = fprev[i];
+            const float fx = g.x + ax, fy = g.y + ay;
+            f[i] = make_float2(fx, fy);
+            float dx = fx - fp.x, dy = fy - fp.y;
+            sw = me.z * sqrtf(dx * dx + dy * dy);
+            dx = fx + fp.x;
+            dy = fy + fp.y;
+            tr = me.z * (float)(sqrtf(dx * dx + dy * dy) / 2.0);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            sw += __shfl_xor_sync(kFull, sw, o);
+            tr += __shfl_xor_sync(kFull, tr, o);
+        }
+        if (lane == 0) warp_partial[w] = make_float2(sw, tr);
+    }
+    // last block: fixed-order sum of the per-warp partials, then the speed rule
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(&ctr->trav_done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    float sw = 0.0f, tr = 0.0f;
+    for (int w = threadIdx.x; w < nwarps; w += blockDim.x) {
+        float2 v = __ldcg(&warp_partial[w]);
+        sw += v.x;
+        tr += v.y;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        sw += __shfl_xor_sync(kFull, sw, o);
+        tr += __shfl_xor_sync(kFull, tr, o);
+    }
+    if (lane == 0) {
+        s_red[0][threadIdx.x >> 5] = sw;
+        s_red[1][threadIdx.x >> 5] = tr;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float swg = 0.0f, etra = 0.0f;
+        for (int w = 0; w < kTravThreads / kWarp; ++w) {
+            swg += s_red[0][w];
+            etra += s_red[1][w];
+        }
+        st->swg_sum = swg;
+        st->etra_sum = etra;
+        // src/RPFA2Kernels.cu:243-275
+        float estimated_optimal_jitter_tollerance = 0.05 * sqrtf((float)n);
+        float minJT = sqrtf(estimated_optimal_jitter_tollerance);
+        float jt = st->jitter_tolerance *
+                   fmaxf(minJT, fminf(st->k_s_max, estimated_optimal_jitter_tollerance * etra /
+                                                       powf((float)n, 2.0f)));
+        float min_speed_efficiency = 0.05f;
+        float se = st->speed_efficiency, gs = st->global_speed;
+        if (swg / etra > 2.0) {
+            if (se > min_speed_efficiency) se *= 0.5;
+            jt = fmaxf(jt, st->jitter_tolerance);
+        }
+        float targetSpeed = jt * se * etra / swg;
+        if (swg > jt * etra) {
+            if (se > min_speed_efficiency) se *= 0.7;
+        } else if (gs < 1000) {
+            se *= 1.3;
+        }
+        float max_rise = 0.5f;
+        gs += fminf(targetSpeed - gs, max_rise * gs);
+        st->speed_efficiency = se;
+        st->global_speed = gs;
+    }
+}
+
+// --------------------------------------------------------------- displace --
+
+// DisplacementKernel (src/RPFA2Kernels.cu:223-251).
+__global__ void __launch_bounds__(kDispThreads) k_displace(int n, float2 *__restrict pos,
+                                                           const float2 *__restrict f,
+                                                           float2 *__restrict fprev, DevState *st) {
+    if (st->err || st->poison) return;
+    const float global_speed = st->global_speed;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float2 fi = f[i], fp = fprev[i];
+        const float dx = fi.x - fp.x, dy = fi.y - fp.y;
+        const float swg = sqrtf(dx * dx + dy * dy);
+        const float factor = global_speed / (1.0 + sqrtf(global_speed * swg));
+        float2 p = pos[i];
+        p.x += fi.x * factor;
+        p.y += fi.y * factor;
+        pos[i] = p;
+        fprev[i] = fi;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->iters_done += 1;
+}
+
+// ---------------------------------------------------------------- attract --
+
+// Gravity (GravityKernel, src/RPFA2Kernels.cu:35-73) plus attraction summed
+// per node over its symmetric CSR row (AttractiveForceKernel :75-109 without
+// atomics).  Rows hold neighbour ids padded with the row's own id to a
+// multiple of four (a padding entry adds p_i - p_i = 0), so a lane loads four
+// ids with one 16-byte load.  `lanes` lanes share a row and reduce with
+// shuffles; heavy rows take a whole block.
+template <int LANES>
+__device__ __forceinline__ void attract_group(int row, bool valid, const float2 *__restrict pos,
+                                              const float *__restrict mass,
+                                              const uint32_t *__restrict off,
+                                              const int4 *__restrict col4, float2 *__restrict fag,
+                                              const Params &prm, int sl) {
+    float ax = 0.0f, ay = 0.0f;
+    float2 p = make_float2(0.0f, 0.0f);
+    if (valid) {
+        p = pos[row];
+        const uint32_t b = off[row] >> 2, e = off[row + 1] >> 2;
+        for (uint32_t q = b + sl; q < e; q += LANES) {
+            const int4 c = __ldcs(&col4[q]);
+            const float2 q0 = __ldg(&pos[c.x]), q1 = __ldg(&pos[c.y]);
+            const float2 q2 = __ldg(&pos[c.z]), q3 = __ldg(&pos[c.w]);
+            ax += (q0.x - p.x) + (q1.x - p.x) + ((q2.x - p.x) + (q3.x - p.x));
+            ay += (q0.y - p.y) + (q1.y - p.y) + ((q2.y - p.y) + (q3.y - p.y));
+        }
+    }
+    if (LANES > 1) {
+#pragma unroll
+        for (int o = LANES / 2; o > 0; o >>= 1) {
+            ax += __shfl_xor_sync(kFull, ax, o);
+            ay += __shfl_xor_sync(kFull, ay, o);
+        }
+    }
+    if (valid && sl == 0) {
+        const float m = mass[row];
+        float f_g;
+        if (prm.strong_gravity)
+            f_g = prm.k_g * m;
+        else if (p.x != 0.0f || p.y != 0.0f)
+            f_g = prm.k_g * m * rsqrtf(p.x * p.x + p.y * p.y);
+        else
+            f_g = 0.0f;
+        fag[row] = make_float2(-p.x * f_g + ax, -p.y * f_g + ay);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_attract(AttractPlan plan, const float2 *__restrict pos,
+                                                 const float *__restrict mass,
+                                                 const uint32_t *__restrict off,
+                                                 const int4 *__restrict col4,
+                                                 float2 *__restrict fag, Params prm) {
+    __shared__ float2 s_red[256 / kWarp];
+    int bi = 0;
+#pragma unroll 1
+    for (int q = 1; q < plan.nbuckets; ++q)
+        if ((int)blockIdx.x >= plan.b[q].block_begin) bi = q;
+    const AttractBucket bk = plan.b[bi];
+    const int blk = blockIdx.x - bk.block_begin;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (bk.lanes == 256) {
+        // one row per block
+        const int row = bk.row_begin + blk;
+        const float2 p = pos[row];
+        const uint32_t b = off[row] >> 2, e = off[row + 1] >> 2;
+        float ax = 0.0f, ay = 0.0f;
+        for (uint32_t q = b + threadIdx.x; q < e; q += 256) {
+            const int4 c = __ldcs(&col4[q]);
+            const float2 q0 = __ldg(&pos[c.x]), q1 = __ldg(&pos[c.y]);
+            const float2 q2 = __ldg(&pos[c.z]), q3 = __ldg(&pos[c.w]);
+            ax += (q0.x - p.x) + (q1.x - p.x) + ((q2.x - p.x) + (q3.x - p.x));
+            ay += (q0.y - p.y) + (q1.y - p.y) + ((q2.y - p.y) + (q3.y - p.y));
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            ax += __shfl_xor_sync(kFull, ax, o);
+            ay += __shfl_xor_sync(kFull, ay, o);
+        }
+        if (lane == 0) s_red[wid] = make_float2(ax, ay);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            ax = 0.0f;
+            ay = 0.0f;
+            for (int w = 0; w < 256 / kWarp; ++w) {
+                ax += s_red[w].x;
+                ay += s_red[w].y;
+            }
+            const float m = mass[row];
+            float f_g;
+            if (prm.strong_gravity)
+                f_g = prm.k_g * m;
+            else if (p.x != 0.0f || p.y != 0.0f)
+                f_g = prm.k_g * m * rsqrtf(p.x * p.x + p.y * p.y);
+            else
+                f_g = 0.0f;
+            fag[row] = make_float2(-p.x * f_g + ax, -p.y * f_g + ay);
+        }
+        return;
+    }
+    const int rows_per_warp = 32 / bk.lanes;
+    const int sub = lane / bk.lanes, sl = lane % bk.lanes;
+    const int row = bk.row_begin + (blk * (256 / kWarp) + wid) * rows_per_warp + sub;
+    const bool valid = row < bk.row_end;
+    switch (bk.lanes) {
+        case 32: attract_group<32>(row, valid, pos, mass, off, col4, fag, prm, sl); break;
+        case 16: attract_group<16>(row, valid, pos, mass, off, col4, fag, prm, sl); break;
+        case 8: attract_group<8>(row, valid, pos, mass, off, col4, fag, prm, sl); break;
+        case 4: attract_group<4>(row, valid, pos, mass, off, col4, fag, prm, sl); break;
+        case 2: attract_group<2>(row, valid, pos, mass, off, col4, fag, prm, sl); break;
+        default: attract_group<1>(row, valid, pos, mass, off, col4, fag, prm, sl); break;
+    }
+}
+
+// ----------------------------------------------------------- permutations --
+
+__global__ void k_scatter_xy(int n, const uint32_t *__restrict ref_of,
+                             const float2 *__restrict src_ref, float2 *__restrict dst_int) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        dst_int[i] = src_ref[ref_of[i]];
+}
+
+__global__ void k_gather_xy(int n, const uint32_t *__restrict ref_of,
+                            const float2 *__restrict src_int, float2 *__restrict dst_ref) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        dst_ref[ref_of[i]] = src_int[i];
+}
+
+__global__ void k_sorted_ref_ids(int n, const uint32_t *__restrict ref_of,
+                                 const uint32_t *__restrict vals, uint32_t *__restrict out) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        out[k] = ref_of[vals[k]];
+}
+
+inline int grid_for(int n, int threads, int cap) {
+    int g = (n + threads - 1) / threads;
+    return g < 1 ? 1 : (g > cap ? cap : g);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- launchers --
+
+void launch_bbox(const Buffers &b, int nblocks, cudaStream_t s) {
+    k_bbox<<<nblocks, kBBoxThreads, 0, s>>>(b.n, b.pos, b.bbox_partial, b.st, b.ctr);
+}
+
+void launch_keys(const Buffers &b, int nsm, cudaStream_t s) {
+    k_keys<<<grid_for(b.n, 256, nsm * 8), 256, 0, s>>>(b.n, b.pos, b.st, b.keys[0], b.vals[0],
+                                                       b.ctr);
+}
+
+void launch_runs(const Buffers &b, int perturb, int nsm, cudaStream_t s) {
+    k_runs<<<grid_for(b.n, 256, nsm * 8), 256, 0, s>>>(b.n, b.keys[0], b.vals[0], b.pos, b.ref_of,
+                                                       b.st, perturb);
+}
+
+void launch_tree_count(const Buffers &b, cudaStream_t s) {
+    k_tree_count<<<count_tiles(b.n), kCountThreads, 0, s>>>(b.n, b.keys[0], b.lcp, b.group, b.cnt,
+                                                            b.capacity, b.st, b.ctr,
+                                                            b.count_status);
+}
+
+void launch_emit(const Buffers &b, int nsm, cudaStream_t s) {
+    k_emit<<<grid_for(b.n, 256, nsm * 8), 256, 0, s>>>(b.n, b.keys[0], b.vals[0], b.lcp, b.group,
+                                                       b.pos, b.mass, b.nodes, b.parent, b.cnt,
+                                                       b.body_node, b.st);
+}
+
+void launch_summarize(const Buffers &b, int nsm, cudaStream_t s) {
+    k_summarize<<<grid_for(b.n, 256, nsm * 8), 256, 0, s>>>(b.n, b.body_node, b.parent, b.cnt,
+                                                            b.nodes, b.st);
+}
+
+void launch_traverse(const Buffers &b, const Params &p, int nblocks, cudaStream_t s) {
+    k_traverse<<<nblocks, kTravThreads, 0, s>>>(b.n, b.nodes, b.body_node, b.vals[0], b.fag,
+                                                b.fprev, b.f, b.warp_partial, b.st, b.ctr, p);
+}
+
+void launch_displace(const Buffers &b, int nsm, cudaStream_t s) {
+    k_displace<<<grid_for(b.n, kDispThreads, nsm * 4), kDispThreads, 0, s>>>(b.n, b.pos, b.f,
+                                                                            b.fprev, b.st);
+}
+
+void launch_attract(const Buffers &b, const Params &p, const AttractPlan &plan, cudaStream_t s) {
+    if (plan.nblocks == 0) return;
+    k_attract<<<plan.nblocks, 256, 0, s>>>(plan, b.pos, b.mass, b.csr_off, b.csr_col4, b.fag, p);
+}
+
+void launch_scatter_xy(int n, const uint32_t *ref_of, const float2 *src_ref, float2 *dst_int,
+                       cudaStream_t s) {
+    k_scatter_xy<<<grid_for(n, 256, 4096), 256, 0, s>>>(n, ref_of, src_ref, dst_int);
+}
+
+void launch_gather_xy(int n, const uint32_t *ref_of, const float2 *src_int, float2 *dst_ref,
+                      cudaStream_t s) {
+    k_gather_xy<<<grid_for(n, 256, 4096), 256, 0, s>>>(n, ref_of, src_int, dst_ref);
+}
+
+void launch_sorted_ref_ids(int n, const uint32_t *ref_of, const uint32_t *vals, uint32_t *out,
+                           cudaStream_t s) {
+    k_sorted_ref_ids<<<grid_for(n, 256, 4096), 256, 0, s>>>(n, ref_of, vals, out);
+}
+
+int traverse_blocks_per_sm() {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_traverse, kTravThreads, 0);
+    return nb < 1 ? 1 : nb;
+}
+
+}  // namespace fa2

@@ -1,0 +1,192 @@
+/*
+ * fa2b200.h -- C ABI of the B200 ForceAtlas2 engine (libfa2b200.so).
+ *
+ * This is the boundary under the reference's C++ interface: the drop-in
+ * RPGraph::CUDAForceAtlas2 (include/RPGPUForceAtlas2.hpp) is a thin shim over
+ * these calls, and any FFI (ctypes, cgo, JNI) can bind them directly.  Plain
+ * C types only: no CUDA or torch types cross this boundary.
+ *
+ * Conventions
+ *  - Node ids are the reference's: 0..num_nodes-1 as UGraph assigns them
+ *    (first appearance in the edge list).  Position and force arrays are
+ *    interleaved x,y pairs in that id order.
+ *  - Every call returns a status (FA2_OK = 0) instead of exiting, which is
+ *    what the reference does on a CUDA error (src/RPCommon.hpp:33-41); the
+ *    C++ shim turns a nonzero status back into that print-and-exit.
+ *  - All state lives in the context; any number of contexts may coexist
+ *    (the reference keeps its speed and tree state in device statics,
+ *    src/RPFA2Kernels.cu:29-33 and src/RPBHKernels.cu:58-62, so it allows one).
+ *  - Calls on one context are not thread-safe; use one host thread per context.
+ */
+#ifndef FA2B200_H
+#define FA2B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum fa2_status {
+    FA2_OK = 0,
+    FA2_ERR_INVALID_ARGUMENT = 1, /* bad pointer, size, id, or a self-loop */
+    FA2_ERR_NO_DEVICE = 2,        /* no CUDA device, or not an sm_100 part */
+    FA2_ERR_CUDA = 3,             /* a CUDA runtime call failed */
+    FA2_ERR_OUT_OF_MEMORY = 4,
+    FA2_ERR_DEVICE_LIMIT = 5,     /* a device-side bound was hit (see fa2_get_stats) */
+    FA2_ERR_TOO_LARGE = 6,        /* graph beyond the engine's index ranges */
+    FA2_ERR_UNSUPPORTED = 7,      /* e.g. exact (non-Barnes-Hut) repulsion */
+    FA2_ERR_IO = 8                /* a file could not be read or written */
+};
+
+typedef struct fa2_ctx fa2_ctx;
+
+/* An undirected graph: each edge once, no self-loops, ids < num_nodes.
+ * Replaces the graph half of the CUDAForceAtlas2 constructor
+ * (src/RPGPUForceAtlas2.cu:51-84), which reads UGraph::neighbors_with_geq_id. */
+typedef struct {
+    uint32_t num_nodes;
+    uint64_t num_edges;
+    const uint32_t *sources;
+    const uint32_t *targets;
+} fa2_graph_desc;
+
+/* The ForceAtlas2 parameters of src/RPForceAtlas2.cpp:28-55. */
+typedef struct {
+    int32_t use_barneshut;    /* must be 1: the GPU path is Barnes-Hut only
+                                 (src/graph_viewer.cpp:93-97) */
+    int32_t strong_gravity;   /* 1: f_g = k_g m; 0: f_g = k_g m / |p| */
+    float gravity;            /* k_g (setGravity) */
+    float scale;              /* k_r (setScale) */
+    float theta;              /* Barnes-Hut accuracy, 1.0 (:45) */
+    float epssq;              /* softening, 0.05^2 (:46) */
+    float jitter_tolerance;   /* 1.0 (:40) */
+    float k_s_max;            /* 10.0 (:43) */
+    int32_t device;           /* CUDA device ordinal */
+} fa2_params;
+
+/* Fills the reference defaults (weak gravity, gravity 1, scale 1). */
+void fa2_default_params(fa2_params *p);
+
+/* Replaces the CUDAForceAtlas2 constructor (src/RPGPUForceAtlas2.cu:37-162):
+ * builds the device graph and all per-iteration buffers.  Positions start at
+ * zero; call fa2_set_positions.  Returns NULL and sets *status on failure. */
+fa2_ctx *fa2_create(const fa2_graph_desc *graph, const fa2_params *params, int *status);
+
+/* Replaces ~CUDAForceAtlas2 (src/RPGPUForceAtlas2.cu:192-204). */
+void fa2_destroy(fa2_ctx *ctx);
+
+/* Replaces sendLayoutToGPU (src/RPGPUForceAtlas2.cu:256-260): xy holds
+ * 2*num_nodes floats (host memory; pinned memory makes the copy faster).
+ * Like the reference it copies positions only; previous forces and the
+ * adaptive speed are kept (fa2_set_speed_state resets them). */
+int fa2_set_positions(fa2_ctx *ctx, const float *xy);
+
+/* Replaces retrieveLayoutFromGPU (src/RPGPUForceAtlas2.cu:250-254), the data
+ * half of sync_layout (:270-278). */
+int fa2_get_positions(fa2_ctx *ctx, float *xy);
+
+/* Replaces CUDAForceAtlas2::doStep (src/RPGPUForceAtlas2.cu:206-248), run
+ * n_iters times; returns when the device has finished, like doStep's
+ * cudaDeviceSynchronize (:246). */
+int fa2_step(fa2_ctx *ctx, int32_t n_iters);
+
+/* fa2_step with device timing: *ms_total receives the CUDA-event time of
+ * the whole call on the engine's stream; kernel_ms (may be NULL) receives,
+ * for each kernel listed by fa2_kernel_name, its mean duration per launch in
+ * ms over the call.  n_kernels is the size of kernel_ms.  No reference
+ * counterpart: it serves measurement. */
+int fa2_step_timed(fa2_ctx *ctx, int32_t n_iters, float *ms_total, float *kernel_ms,
+                   int32_t n_kernels);
+
+/* Name of timed kernel slot i, or NULL past the last one. */
+const char *fa2_kernel_name(int32_t i);
+
+/* Diagnostics of the last step; test and measurement hooks with no
+ * reference counterpart. */
+typedef struct {
+    uint32_t num_bodies;
+    uint32_t tree_nodes;        /* cells + bodies of the last quadtree */
+    uint32_t tree_cells;
+    int32_t max_level;          /* deepest cell level (root 0) */
+    int32_t perturb_rounds;     /* .99 re-insertion rounds in the last step */
+    int32_t device_error;       /* bit set of device-side limit hits, 0 = none */
+    uint64_t nnz_padded;        /* CSR entries incl. padding */
+    float global_speed;         /* adaptive speed after the last step */
+    float speed_efficiency;
+    float radius, root_x, root_y;
+    uint64_t interactions;      /* body-node force terms of the last traversal */
+    uint64_t visits;            /* body-node acceptance tests of the last traversal */
+} fa2_stats;
+
+int fa2_get_stats(fa2_ctx *ctx, fa2_stats *out);
+
+/* Last step's forces before displacement (test hook): f_total is the full
+ * FA2 force, f_attr_grav the gravity + attraction part; either may be NULL.
+ * The reference keeps these in fxl/fyl (src/RPGPUForceAtlas2.cu:136-139). */
+int fa2_get_forces(fa2_ctx *ctx, float *f_total, float *f_attr_grav);
+
+/* Last step's body order of the quadtree, as node ids: the reference's sortd
+ * (src/RPBHKernels.cu:513-559). */
+int fa2_get_sort_order(fa2_ctx *ctx, uint32_t *order);
+
+/* Overwrites the adaptive speed state (global_speed, speed_efficiency) and the
+ * previous forces (2*num_nodes floats, or NULL for zero).  Checkpoint/restore
+ * hook: the reference never saves these (src/RPGraphLayout.cpp:228-250). */
+int fa2_set_speed_state(fa2_ctx *ctx, float global_speed, float speed_efficiency,
+                        const float *f_prev);
+int fa2_get_speed_state(fa2_ctx *ctx, float *global_speed, float *speed_efficiency,
+                        float *f_prev);
+
+/* Changes k_r and k_g between steps: ForceAtlas2::setScale / setGravity
+ * (src/RPForceAtlas2.cpp:64-72), which the reference passes to every launch. */
+int fa2_set_force_params(fa2_ctx *ctx, float scale, float gravity);
+
+/* ------------------------------------------------------------------------
+ * Host graph layer: RPGraph::UGraph and GraphLayout behind plain C, for
+ * callers that bind the C ABI instead of the C++ classes.
+ * ---------------------------------------------------------------------- */
+
+typedef struct fa2_ugraph fa2_ugraph;
+
+/* RPGraph::UGraph::UGraph(path) (src/RPGraph.cpp:35-56): ids by first
+ * appearance, self-loops and repeated undirected edges dropped.  NULL with
+ * FA2_ERR_IO when the file cannot be opened. */
+fa2_ugraph *fa2_ugraph_load(const char *path, int *status);
+
+/* The same from n_pairs (s, t) pairs already in memory, in file order. */
+fa2_ugraph *fa2_ugraph_from_pairs(const uint32_t *s, const uint32_t *t, uint64_t n_pairs,
+                                  int *status);
+void fa2_ugraph_free(fa2_ugraph *g);
+uint32_t fa2_ugraph_num_nodes(const fa2_ugraph *g);
+uint64_t fa2_ugraph_num_edges(const fa2_ugraph *g);
+
+/* node_map_r: UGraph id -> edge-list id (num_nodes entries). */
+int fa2_ugraph_node_map_r(const fa2_ugraph *g, uint32_t *out);
+
+/* UGraph::degree of every node (num_nodes entries). */
+int fa2_ugraph_degrees(const fa2_ugraph *g, uint32_t *out);
+
+/* All edges as CUDAForceAtlas2 lists them (src/RPGPUForceAtlas2.cu:77-84):
+ * sources ascending, each source's neighbors_with_geq_id in order. */
+int fa2_ugraph_edges(const fa2_ugraph *g, uint32_t *sources, uint32_t *targets);
+
+/* srandom(seed), then GraphLayout(graph, width, height).randomizePositions()
+ * (src/RPGraphLayout.cpp:45-52): 2*n floats, x then y per node. */
+void fa2_random_positions(uint32_t n, float width, float height, uint32_t seed, float *xy);
+
+/* GraphLayout::writeToCSV / writeToBin (src/RPGraphLayout.cpp:209-250) of
+ * positions xy for graph g.  Refuses (FA2_ERR_IO) an existing file. */
+int fa2_write_layout(const fa2_ugraph *g, const float *xy, const char *path, int binary);
+
+/* Human-readable text of a status code. */
+const char *fa2_status_string(int status);
+
+/* Library version string. */
+const char *fa2_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
