@@ -25,6 +25,11 @@ _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 _lib = None
 
 
+class _SpeedState(C.Structure):
+    _fields_ = [("global_speed", C.c_float), ("speed_efficiency", C.c_float),
+                ("jitter_tolerance", C.c_float), ("k_s_max", C.c_float)]
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -60,6 +65,7 @@ def lib():
                                               C.c_int32, _i32p, _f64p, _f64p]
         L.orc_fa2_step.restype = C.c_int32
         L.orc_fa2_step.argtypes = [C.c_void_p]
+        L.orc_speed_update.argtypes = [C.c_int32, C.c_float, C.c_float, C.POINTER(_SpeedState)]
         _lib = L
     return _lib
 
