@@ -23,11 +23,10 @@ using namespace fa2;
 
 namespace {
 
-constexpr int kNumSlots = 10;
-const char *const kSlotNames[kNumSlots] = {"attract", "bbox",       "keys", "sort",     "runs",
-                                           "tree_count", "emit",   "summarize", "traverse",
-                                           "displace"};
-enum Slot { S_ATTRACT, S_BBOX, S_KEYS, S_SORT, S_RUNS, S_COUNT, S_EMIT, S_SUMM, S_TRAV, S_DISP };
+constexpr int kNumSlots = 9;
+const char *const kSlotNames[kNumSlots] = {"attract", "keys",      "sort",     "runs",    "tree_count",
+                                           "emit",    "summarize", "traverse", "displace"};
+enum Slot { S_ATTRACT, S_KEYS, S_SORT, S_RUNS, S_COUNT, S_EMIT, S_SUMM, S_TRAV, S_DISP };
 
 constexpr int kMaxReplayRounds = 64;
 
@@ -183,9 +182,6 @@ void enqueue_iteration(fa2_ctx *c, bool full, bool perturb_first, bool timed) {
         launch_attract(b, c->kp, c->plan, B);
         mark(S_ATTRACT, 1, B);
         cudaEventRecord(c->evJoin, B);
-        mark(S_BBOX, 0, A);
-        launch_bbox(b, c->bbox_blocks, A);
-        mark(S_BBOX, 1, A);
     }
     if (perturb_first) launch_runs(b, 1, c->nsm, A);
     mark(S_KEYS, 0, A);
@@ -417,12 +413,14 @@ fa2_ctx *fa2_create(const fa2_graph_desc *g, const fa2_params *prm, int *status)
         (s = dalloc(c, &b.vals[1], n)) || (s = dalloc(c, &b.lcp, n)) ||
         (s = dalloc(c, &b.group, n)) || (s = dalloc(c, &b.body_node, n)) ||
         (s = dalloc(c, &b.nodes, cap)) || (s = dalloc(c, &b.parent, cap)) ||
-        (s = dalloc(c, &b.cnt, cap)) || (s = dalloc(c, &b.warp_partial, (n + 31) / 32)) ||
+        (s = dalloc(c, &b.cnt, cap)) || (s = dalloc(c, &b.kids, cap)) || (s = dalloc(c, &b.warp_partial, (n + 31) / 32)) ||
         (s = dalloc(c, &b.st, 1)) || (s = dalloc(c, &c->stage_xy, n)) ||
         (s = dalloc(c, &c->stage_ids, n)))
         return fail(s);
     c->bbox_blocks = c->nsm * 2;
-    if ((s = dalloc(c, &b.bbox_partial, c->bbox_blocks))) return fail(s);
+    // partial boxes of k_bbox (bbox_blocks) and of k_displace (up to 4 per SM)
+    if ((s = dalloc(c, &b.bbox_partial, (size_t)c->nsm * 4))) return fail(s);
+    c->kp.nsm = c->nsm;
     b.csr_off = d_off;
     b.csr_col4 = d_col;
     b.ref_of = d_ref;
@@ -486,6 +484,9 @@ int fa2_set_positions(fa2_ctx *c, const float *xy) {
     const size_t bytes = (size_t)c->n * 8;
     CK(cudaMemcpyAsync(c->stage_xy, xy, bytes, cudaMemcpyHostToDevice, c->sA));
     launch_scatter_xy((int)c->n, c->b.ref_of, c->stage_xy, c->b.pos, c->sA);
+    // the root cell of the next tree comes from these positions
+    CK(cudaMemsetAsync(c->scratch, 0, c->scratch_bytes, c->sA));
+    launch_bbox(c->b, c->bbox_blocks, c->sA);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(c->sA));
     return FA2_OK;

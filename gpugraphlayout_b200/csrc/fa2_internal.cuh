@@ -53,7 +53,8 @@ struct IterCounters {
     unsigned count_ticket;
     unsigned trav_ticket;
     unsigned trav_done;
-    unsigned pad[4];
+    unsigned disp_done;
+    unsigned pad[3];
     unsigned hist[8][256];  // per-pass digit histograms of the sort keys
 };
 
@@ -101,6 +102,7 @@ struct Buffers {
     float4 *nodes;            // capacity: x, y, mass, meta
     int32_t *parent;          // capacity
     int32_t *cnt;             // capacity: child counters
+    int4 *kids;               // capacity: first four children of each cell
     uint32_t capacity;
     // reductions
     float4 *bbox_partial;     // bbox blocks
@@ -114,10 +116,11 @@ struct Buffers {
 struct Params {
     float k_r, k_g, itolsq, epssq;
     int strong_gravity;
+    int nsm;
 };
 
 constexpr int kBBoxThreads = 512;
-constexpr int kTravThreads = 256;
+constexpr int kTravThreads = 512;
 constexpr int kDispThreads = 512;
 
 // ---------------------------------------------------------------- kernels --

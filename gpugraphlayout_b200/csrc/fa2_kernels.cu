@@ -24,6 +24,8 @@
 #include <float.h>
 #include <stdint.h>
 
+#include <cuda/atomic>
+
 #include "fa2_internal.cuh"
 
 namespace fa2 {
@@ -71,57 +73,74 @@ __device__ __forceinline__ uint64_t morton_key(float px, float py, float x, floa
 
 // ------------------------------------------------------------------- bbox --
 
-__global__ void __launch_bounds__(kBBoxThreads) k_bbox(int n, const float2 *__restrict pos,
-                                                       float4 *__restrict partial,
-                                                       DevState *st, IterCounters *ctr) {
-    __shared__ float4 s_w[kBBoxThreads / kWarp];
-    __shared__ bool s_last;
-    if (st->err || st->poison) return;
-    float mnx = FLT_MAX, mxx = -FLT_MAX, mny = FLT_MAX, mxy = -FLT_MAX;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        float2 p = pos[i];
-        mnx = fminf(mnx, p.x);
-        mxx = fmaxf(mxx, p.x);
-        mny = fminf(mny, p.y);
-        mxy = fmaxf(mxy, p.y);
-    }
+__device__ __forceinline__ float4 bbox_merge(float4 a, float4 b) {
+    return make_float4(fminf(a.x, b.x), fmaxf(a.y, b.y), fminf(a.z, b.z), fmaxf(a.w, b.w));
+}
+
+__device__ __forceinline__ float4 warp_bbox(float4 a) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        mnx = fminf(mnx, __shfl_xor_sync(kFull, mnx, o));
-        mxx = fmaxf(mxx, __shfl_xor_sync(kFull, mxx, o));
-        mny = fminf(mny, __shfl_xor_sync(kFull, mny, o));
-        mxy = fmaxf(mxy, __shfl_xor_sync(kFull, mxy, o));
+        float4 b;
+        b.x = __shfl_xor_sync(kFull, a.x, o);
+        b.y = __shfl_xor_sync(kFull, a.y, o);
+        b.z = __shfl_xor_sync(kFull, a.z, o);
+        b.w = __shfl_xor_sync(kFull, a.w, o);
+        a = bbox_merge(a, b);
     }
+    return a;
+}
+
+// Block bounding box (minx, maxx, miny, maxy) of the thread values; the
+// last block to finish merges all block results and sets the root cell the
+// way BoundingBoxKernel does (src/RPBHKernels.cu:128-148).  Every thread of
+// the block must call it.
+template <int THREADS>
+__device__ void bbox_finish(float4 a, float4 *__restrict partial, unsigned *done, DevState *st) {
+    __shared__ float4 s_w[THREADS / kWarp];
+    __shared__ bool s_last;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (lane == 0) s_w[wid] = make_float4(mnx, mxx, mny, mxy);
+    a = warp_bbox(a);
+    if (lane == 0) s_w[wid] = a;
     __syncthreads();
     if (threadIdx.x == 0) {
-        float4 a = s_w[0];
-        for (int w = 1; w < kBBoxThreads / kWarp; ++w) {
-            float4 b = s_w[w];
-            a = make_float4(fminf(a.x, b.x), fmaxf(a.y, b.y), fminf(a.z, b.z), fmaxf(a.w, b.w));
-        }
-        partial[blockIdx.x] = a;
+        float4 b = s_w[0];
+        for (int w = 1; w < THREADS / kWarp; ++w) b = bbox_merge(b, s_w[w]);
+        partial[blockIdx.x] = b;
         __threadfence();
-        s_last = atomicAdd(&ctr->bbox_done, 1u) == gridDim.x - 1;
+        s_last = atomicAdd(done, 1u) == gridDim.x - 1;
     }
     __syncthreads();
-    if (s_last && threadIdx.x == 0) {
-        __threadfence();
-        float4 a = __ldcg(&partial[0]);
-        for (int b = 1; b < (int)gridDim.x; ++b) {
-            float4 c = __ldcg(&partial[b]);
-            a = make_float4(fminf(a.x, c.x), fmaxf(a.y, c.y), fminf(a.z, c.z), fmaxf(a.w, c.w));
-        }
+    if (!s_last) return;
+    __threadfence();
+    a = make_float4(FLT_MAX, -FLT_MAX, FLT_MAX, -FLT_MAX);
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += THREADS) a = bbox_merge(a, __ldcg(&partial[b]));
+    a = warp_bbox(a);
+    __syncthreads();
+    if (lane == 0) s_w[wid] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < THREADS / kWarp; ++w) a = bbox_merge(a, s_w[w]);
         st->minx = a.x;
         st->maxx = a.y;
         st->miny = a.z;
         st->maxy = a.w;
-        // src/RPBHKernels.cu:140-148
         st->radius = fmaxf(a.y - a.x, a.w - a.z) * 0.5f;
         st->rootx = (a.x + a.y) * 0.5f;
         st->rooty = (a.z + a.w) * 0.5f;
     }
+}
+
+// Bounding box of the current positions (run after positions are set from
+// the host; during stepping the displacement pass computes it).
+__global__ void __launch_bounds__(kBBoxThreads) k_bbox(int n, const float2 *__restrict pos,
+                                                       float4 *__restrict partial,
+                                                       DevState *st, IterCounters *ctr) {
+    float4 a = make_float4(FLT_MAX, -FLT_MAX, FLT_MAX, -FLT_MAX);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float2 p = pos[i];
+        a = bbox_merge(a, make_float4(p.x, p.x, p.y, p.y));
+    }
+    bbox_finish<kBBoxThreads>(a, partial, &ctr->bbox_done, st);
 }
 
 // ------------------------------------------------------------------- keys --
@@ -244,7 +263,7 @@ __device__ __forceinline__ int cells_at(int k, int Lk, int Lkm1) {
 
 __global__ void __launch_bounds__(kCountThreads) k_tree_count(
     int n, const uint64_t *__restrict keys, int8_t *__restrict lcp, uint32_t *__restrict group,
-    int32_t *__restrict cnt, uint32_t capacity, DevState *st, IterCounters *ctr,
+    int32_t *__restrict cnt, int4 *__restrict kids, uint32_t capacity, DevState *st, IterCounters *ctr,
     uint32_t *status) {
     __shared__ int s_tile;
     __shared__ uint32_t s_warp[kCountThreads / kWarp];
@@ -319,7 +338,10 @@ __global__ void __launch_bounds__(kCountThreads) k_tree_count(
         if (k < n) {
             group[k] = off;
             for (int q = 0; q < g[e]; ++q)
-                if (off + q < capacity) cnt[off + q] = 0;
+                if (off + q < capacity) {
+                    cnt[off + q] = 0;
+                    kids[off + q] = make_int4(-1, -1, -1, -1);
+                }
             if (k == n - 1) {
                 uint32_t total = off + (uint32_t)g[e];
                 st->tree_nodes = total;
@@ -418,6 +440,7 @@ __global__ void __launch_bounds__(256) k_emit(int n, const uint64_t *__restrict 
                                               const float2 *__restrict pos,
                                               const float *__restrict mass, float4 *__restrict nodes,
                                               int32_t *__restrict parent, int32_t *__restrict cnt,
+                                              int4 *__restrict kids,
                                               uint32_t *__restrict body_node, DevState *st) {
     if (st->err || st->poison) return;
     int local_max = 0;
@@ -435,7 +458,10 @@ __global__ void __launch_bounds__(256) k_emit(int n, const uint64_t *__restrict 
         const int lam = max(max(Lk, Lkm1), 0);
         const uint32_t pb = c > 0 ? bnode - 1 : find_cell(keys, lcp, group, n, k, lam);
         parent[bnode] = (int32_t)pb;
-        atomicAdd(&cnt[pb], 1);
+        {
+            const int slot = atomicAdd(&cnt[pb], 1);
+            if (slot < 4) reinterpret_cast<int *>(kids)[4 * (size_t)pb + slot] = (int)bnode;
+        }
         // the cells that start here, outermost first
         for (int q = 0; q < c; ++q) {
             const int lvl = lo_level + q;
@@ -449,7 +475,10 @@ __global__ void __launch_bounds__(256) k_emit(int n, const uint64_t *__restrict 
             else if (lvl > 0)
                 par = (int32_t)find_cell(keys, lcp, group, n, k, lvl - 1);
             parent[node] = par;
-            if (par >= 0) atomicAdd(&cnt[par], 1);
+            if (par >= 0) {
+                const int slot = atomicAdd(&cnt[par], 1);
+                if (slot < 4) reinterpret_cast<int *>(kids)[4 * (size_t)par + slot] = (int)node;
+            }
             local_max = max(local_max, lvl);
         }
     }
@@ -459,30 +488,64 @@ __global__ void __launch_bounds__(256) k_emit(int n, const uint64_t *__restrict 
 
 // -------------------------------------------------------------- summarize --
 
+__device__ __forceinline__ void cswap(uint32_t &a, uint32_t &b) {
+    const uint32_t lo = min(a, b), hi = max(a, b);
+    a = lo;
+    b = hi;
+}
+
+__device__ __forceinline__ void add_child(const float4 &r, float &cm, float &px, float &py) {
+    const float m = r.z;
+    px += r.x * m;
+    py += r.y * m;
+    cm += m;
+}
+
 // Bottom-up cell mass and centre of mass.  Every node decrements its
-// parent's child counter; the child that brings it to zero computes the
-// parent from all its children, in quadrant order, as SummarizationKernel
-// does (src/RPBHKernels.cu:461-494), and continues upwards.
+// parent's child counter (acquire-release, so the last child sees what the
+// others wrote); the child that brings it to zero computes the parent from
+// all its children, in quadrant order, as SummarizationKernel does
+// (src/RPBHKernels.cu:461-494), and continues upwards.  A cell's children
+// come from the four slots k_emit filled; preorder index order is quadrant
+// order.  Level-32 cells can hold more bodies than four slots and are
+// walked through their next links instead.
 __global__ void __launch_bounds__(256) k_summarize(int n, const uint32_t *__restrict body_node,
                                                    const int32_t *__restrict parent,
-                                                   int32_t *cnt, float4 *nodes, DevState *st) {
+                                                   int32_t *cnt, const int4 *__restrict kids,
+                                                   float4 *nodes, DevState *st) {
     if (st->err || st->poison) return;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         int32_t p = parent[body_node[k]];
         while (p >= 0) {
-            __threadfence();
-            if (atomicSub(&cnt[p], 1) != 1) break;
-            __threadfence();
+            cuda::atomic_ref<int32_t, cuda::thread_scope_device> arrivals(cnt[p]);
+            if (arrivals.fetch_sub(1, cuda::memory_order_acq_rel) != 1) break;
             const float4 prec = __ldcg(&nodes[p]);
-            const uint32_t end = meta_next(__float_as_int(prec.w));
+            const int meta = __float_as_int(prec.w);
             float cm = 0.0f, px = 0.0f, py = 0.0f;
-            for (uint32_t c = (uint32_t)p + 1; c < end;) {
-                const float4 r = __ldcg(&nodes[c]);
-                const float m = r.z;
-                px += r.x * m;
-                py += r.y * m;
-                cm += m;
-                c = meta_next(__float_as_int(r.w));
+            if (meta_level(meta) == kLevels) {
+                const uint32_t end = meta_next(meta);
+                for (uint32_t c = (uint32_t)p + 1; c < end;) {
+                    const float4 r = __ldcg(&nodes[c]);
+                    add_child(r, cm, px, py);
+                    c = meta_next(__float_as_int(r.w));
+                }
+            } else {
+                const int4 kd = __ldcg(&kids[p]);
+                uint32_t c0 = (uint32_t)kd.x, c1 = (uint32_t)kd.y, c2 = (uint32_t)kd.z,
+                         c3 = (uint32_t)kd.w;  // empty slots are -1: sorted last
+                cswap(c0, c1);
+                cswap(c2, c3);
+                cswap(c0, c2);
+                cswap(c1, c3);
+                cswap(c1, c2);
+                const float4 r0 = __ldcg(&nodes[c0]);
+                const float4 r1 = c1 != ~0u ? __ldcg(&nodes[c1]) : make_float4(0, 0, 0, 0);
+                const float4 r2 = c2 != ~0u ? __ldcg(&nodes[c2]) : make_float4(0, 0, 0, 0);
+                const float4 r3 = c3 != ~0u ? __ldcg(&nodes[c3]) : make_float4(0, 0, 0, 0);
+                add_child(r0, cm, px, py);
+                if (c1 != ~0u) add_child(r1, cm, px, py);
+                if (c2 != ~0u) add_child(r2, cm, px, py);
+                if (c3 != ~0u) add_child(r3, cm, px, py);
             }
             const float inv = 1.0f / cm;
             __stcg(&nodes[p], make_float4(px * inv, py * inv, cm, prec.w));
@@ -527,10 +590,23 @@ __global__ void __launch_bounds__(kTravThreads) k_traverse(
     const uint32_t end = st->tree_nodes;
     const int lane = threadIdx.x & 31;
     const int nwarps = (n + 31) >> 5;
-    for (;;) {
-        int w = 0;
-        if (lane == 0) w = (int)atomicAdd(&ctr->trav_ticket, 1u);
-        w = __shfl_sync(kFull, w, 0);
+    // Work split: first a static phase in which the warps of a block take
+    // adjacent groups (neighbouring bodies walk the same tree nodes, which
+    // then stay in L1), then a shared pool handed out one group at a time,
+    // which evens out the load.
+    constexpr int kWarpsPerBlock = kTravThreads / kWarp;
+    const int wid = threadIdx.x >> 5;
+    const int rounds = (nwarps * 3 / 4) / ((int)gridDim.x * kWarpsPerBlock);
+    const int pool0 = rounds * (int)gridDim.x * kWarpsPerBlock;
+    for (int j = 0;; ++j) {
+        int w;
+        if (j < rounds) {
+            w = (j * (int)gridDim.x + (int)blockIdx.x) * kWarpsPerBlock + wid;
+        } else {
+            w = 0;
+            if (lane == 0) w = pool0 + (int)atomicAdd(&ctr->trav_ticket, 1u);
+            w = __shfl_sync(kFull, w, 0);
+        }
         if (w >= nwarps) break;
         const int k = w * 32 + lane;
         const bool active = k < n;
@@ -538,21 +614,27 @@ __global__ void __launch_bounds__(kTravThreads) k_traverse(
         const float px = me.x, py = me.y, kmi = prm.k_r * me.z;
         float ax = 0.0f, ay = 0.0f;
         uint32_t node = 1, n_acc = 0, n_vis = 0;
+        float4 r = __ldg(&nodes[min(node, end - 1)]);
         while (node < end) {
-            const float4 r = __ldg(&nodes[node]);
+            const int meta = __float_as_int(r.w);
+            const uint32_t skip = meta_next(meta);
+            // both possible successors are loaded before the vote decides
+            const float4 r_in = __ldg(&nodes[min(node + 1, end - 1)]);
+            const float4 r_skip = __ldg(&nodes[min(skip, end - 1)]);
             const float dx = px - r.x, dy = py - r.y;
             const float d2 = dx * dx + dy * dy + prm.epssq;
-            const int meta = __float_as_int(r.w);
             const bool ok = !active || d2 >= s_dq[meta_level(meta)];
             ++n_vis;
             if (__all_sync(kFull, ok)) {
-                const float c = kmi * r.z / d2;
+                const float c = __fdividef(kmi * r.z, d2);
                 ax = fmaf(dx, c, ax);
                 ay = fmaf(dy, c, ay);
-                node = meta_next(meta);
+                node = skip;
+                r = r_skip;
                 ++n_acc;
             } else {
                 ++node;
+                r = r_in;
             }
         }
         if (lane == 0) {
@@ -639,12 +721,17 @@ __global__ void __launch_bounds__(kTravThreads) k_traverse(
 
 // --------------------------------------------------------------- displace --
 
-// DisplacementKernel (src/RPFA2Kernels.cu:223-251).
+// DisplacementKernel (src/RPFA2Kernels.cu:223-251), fused with the bounding
+// box of the new positions, which the next iteration's tree needs
+// (BoundingBoxKernel, src/RPBHKernels.cu:70-157).
 __global__ void __launch_bounds__(kDispThreads) k_displace(int n, float2 *__restrict pos,
                                                            const float2 *__restrict f,
-                                                           float2 *__restrict fprev, DevState *st) {
+                                                           float2 *__restrict fprev,
+                                                           float4 *__restrict partial, DevState *st,
+                                                           IterCounters *ctr) {
     if (st->err || st->poison) return;
     const float global_speed = st->global_speed;
+    float4 a = make_float4(FLT_MAX, -FLT_MAX, FLT_MAX, -FLT_MAX);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float2 fi = f[i], fp = fprev[i];
         const float dx = fi.x - fp.x, dy = fi.y - fp.y;
@@ -655,7 +742,9 @@ __global__ void __launch_bounds__(kDispThreads) k_displace(int n, float2 *__rest
         p.y += fi.y * factor;
         pos[i] = p;
         fprev[i] = fi;
+        a = bbox_merge(a, make_float4(p.x, p.x, p.y, p.y));
     }
+    bbox_finish<kDispThreads>(a, partial, &ctr->disp_done, st);
     if (blockIdx.x == 0 && threadIdx.x == 0) st->iters_done += 1;
 }
 
@@ -816,19 +905,19 @@ void launch_runs(const Buffers &b, int perturb, int nsm, cudaStream_t s) {
 }
 
 void launch_tree_count(const Buffers &b, cudaStream_t s) {
-    k_tree_count<<<count_tiles(b.n), kCountThreads, 0, s>>>(b.n, b.keys[0], b.lcp, b.group, b.cnt,
+    k_tree_count<<<count_tiles(b.n), kCountThreads, 0, s>>>(b.n, b.keys[0], b.lcp, b.group, b.cnt, b.kids,
                                                             b.capacity, b.st, b.ctr,
                                                             b.count_status);
 }
 
 void launch_emit(const Buffers &b, int nsm, cudaStream_t s) {
     k_emit<<<grid_for(b.n, 256, nsm * 8), 256, 0, s>>>(b.n, b.keys[0], b.vals[0], b.lcp, b.group,
-                                                       b.pos, b.mass, b.nodes, b.parent, b.cnt,
+                                                       b.pos, b.mass, b.nodes, b.parent, b.cnt, b.kids,
                                                        b.body_node, b.st);
 }
 
 void launch_summarize(const Buffers &b, int nsm, cudaStream_t s) {
-    k_summarize<<<grid_for(b.n, 256, nsm * 8), 256, 0, s>>>(b.n, b.body_node, b.parent, b.cnt,
+    k_summarize<<<grid_for(b.n, 256, nsm * 8), 256, 0, s>>>(b.n, b.body_node, b.parent, b.cnt, b.kids,
                                                             b.nodes, b.st);
 }
 
@@ -838,8 +927,8 @@ void launch_traverse(const Buffers &b, const Params &p, int nblocks, cudaStream_
 }
 
 void launch_displace(const Buffers &b, int nsm, cudaStream_t s) {
-    k_displace<<<grid_for(b.n, kDispThreads, nsm * 4), kDispThreads, 0, s>>>(b.n, b.pos, b.f,
-                                                                            b.fprev, b.st);
+    k_displace<<<grid_for(b.n, kDispThreads, nsm * 4), kDispThreads, 0, s>>>(
+        b.n, b.pos, b.f, b.fprev, b.bbox_partial, b.st, b.ctr);
 }
 
 void launch_attract(const Buffers &b, const Params &p, const AttractPlan &plan, cudaStream_t s) {

@@ -1,0 +1,203 @@
+"""Edge cases of the CUDA engine against the oracle, through the C ABI.
+
+* coincident bodies: the replay path scales later bodies by .99 (reference
+  intent, src/RPBHKernels.cu:271-278) -- same sort order and forces as the
+  oracle's sequential insertion;
+* a pair that separates below level 32: sort order still equals the
+  reference's in-order (deep digits), and the engine keeps computing
+  repulsion (the reference adds none past depth 32);
+* tiny graphs, clustered layouts, parameter changes, the speed state, invalid
+  input, the Python mirror of the C++ interface and the graph_viewer CLI.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, rel_rmse
+
+pytestmark = pytest.mark.gpu
+
+
+def _engine(g, xy, k_r=1.0, k_g=1.0, sg=True):
+    from gpugraphlayout_b200 import Engine
+    e = Engine(g.n, g.sources, g.targets, strong_gravity=sg, gravity=k_g, scale=k_r)
+    e.set_positions(xy)
+    return e
+
+
+def test_coincident_bodies_replayed_like_oracle():
+    from gpugraphlayout_b200 import synth
+    from oracle import oracle as O
+    s, t = synth.ba_edges(400, 2, seed=2)
+    g = O.Graph(s, t)
+    xy = O.random_positions(g.n, 500, 500, 4)
+    xy[7] = xy[3]
+    xy[11] = xy[3]
+    xy[20] = xy[19]
+    e = _engine(g, xy)
+    e.step(1)
+    assert e.stats()["perturb_rounds"] >= 1
+    fo = O.FA2(g, xy, 1.0, 1.0, True)
+    fo.step(1)
+    assert np.array_equal(e.sort_order(), fo.sortd.astype(np.uint32))
+    tot, ga = e.forces()
+    assert rel_rmse(ga, fo.f_ga.reshape(-1, 2)) < 1e-5
+    assert rel_rmse(tot, fo.f_tot.reshape(-1, 2)) < 1e-4
+    # a second step from there needs no replay
+    e.step(1)
+    assert e.stats()["perturb_rounds"] == 0
+
+
+def test_deep_pair_order_and_repulsion():
+    from oracle import oracle as O
+    g = O.Graph(np.array([0, 1, 2], np.uint32), np.array([1, 2, 3], np.uint32))
+    xy = np.array([[-1024.0, -1024.0], [1024.0, 1024.0], [2.0 ** -25, 0.0],
+                   [1.5 * 2.0 ** -24, 0.0]], np.float32)
+    e = _engine(g, xy)
+    e.step(1)
+    t = O.Tree(xy, g.mass)
+    assert t.maxdepth > 32
+    assert np.array_equal(e.sort_order(), t.sort().astype(np.uint32))
+    assert e.stats()["max_level"] == 32
+    tot, ga = e.forces()
+    rep = tot - ga
+    exact = O.exact_repulsion_f64(xy, g.mass, 1.0, np.arange(4, dtype=np.int32))
+    assert rel_rmse(rep, exact) < 1e-3
+
+
+@pytest.mark.parametrize("pairs", [[(0, 1)], [(0, 1), (1, 2)], [(5, 9), (9, 2), (2, 5), (7, 5)]])
+def test_tiny_graphs(pairs):
+    from oracle import oracle as O
+    s = np.array([p[0] for p in pairs], np.uint32)
+    t = np.array([p[1] for p in pairs], np.uint32)
+    g = O.Graph(s, t)
+    xy = O.random_positions(g.n, 100, 100, 3)
+    e = _engine(g, xy)
+    fo = O.FA2(g, xy, 1.0, 1.0, True)
+    for _ in range(3):
+        e.step(1)
+        fo.step(1)
+        assert np.array_equal(e.sort_order(), fo.sortd.astype(np.uint32))
+        assert rel_rmse(e.get_positions(), fo.positions) < 1e-5
+
+
+def test_clustered_layout_matches_oracle():
+    from gpugraphlayout_b200 import synth
+    from oracle import oracle as O
+    s, t = synth.sbm_edges(6000, 12, 0.05, 0.002, 40, seed=3)
+    g = O.Graph(s, t)
+    rng = np.random.default_rng(5)
+    centres = rng.uniform(-5000, 5000, size=(12, 2))
+    xy = (centres[np.arange(g.n) % 12] + rng.normal(0, 2.0, size=(g.n, 2))).astype(np.float32)
+    e = _engine(g, xy, k_r=2.0, sg=False)
+    fo = O.FA2(g, xy, 2.0, 1.0, False)
+    e.step(1)
+    fo.step(1)
+    assert np.array_equal(e.sort_order(), fo.sortd.astype(np.uint32))
+    tot, _ = e.forces()
+    assert rel_rmse(tot, fo.f_tot.reshape(-1, 2)) < 1e-4
+
+
+def test_set_force_params_and_speed_state(ba3k):
+    from oracle import oracle as O
+    g = ba3k
+    xy = O.random_positions(g.n, 2000, 2000, 11)
+    e = _engine(g, xy, k_r=10.0)
+    e.set_force_params(80.0, 2.0)
+    e.step(1)
+    fo = O.FA2(g, xy, 80.0, 2.0, True)
+    fo.step(1)
+    tot, _ = e.forces()
+    assert rel_rmse(tot, fo.f_tot.reshape(-1, 2)) < 1e-4
+    gs, se, fp = e.speed_state()
+    assert gs == pytest.approx(fo.global_speed, rel=1e-5)
+    # restore a checkpoint and continue: same as never having stopped
+    pos = e.get_positions()
+    e.step(2)
+    after = e.get_positions()
+    e.set_positions(pos)
+    e.set_speed_state(gs, se, fp)
+    e.step(2)
+    assert np.array_equal(e.get_positions(), after)
+
+
+def test_deterministic_repeat(ba3k):
+    from oracle import oracle as O
+    xy = O.random_positions(ba3k.n, 2000, 2000, 5)
+    runs = []
+    for _ in range(2):
+        e = _engine(ba3k, xy, k_r=10.0)
+        e.step(10)
+        runs.append(e.get_positions())
+        e.close()
+    assert np.array_equal(runs[0], runs[1])
+
+
+def test_invalid_input_is_reported():
+    from gpugraphlayout_b200 import Engine, Fa2Error
+    with pytest.raises(Fa2Error) as ei:
+        Engine(3, [0, 1], [1, 1])  # self-loop
+    assert ei.value.status == 1
+    with pytest.raises(Fa2Error) as ei:
+        Engine(3, [0], [3])  # id out of range
+    assert ei.value.status == 1
+    with pytest.raises(Fa2Error) as ei:
+        Engine(3, [0], [1], use_barneshut=False)
+    assert ei.value.status == 7
+
+
+def test_python_mirror_and_writers(tmp_path):
+    """UGraph / GraphLayout / CUDAForceAtlas2 mirror; the bin writer writes the
+    reference's record layout (uint32 edge-list id, float x, float y)."""
+    import gpugraphlayout_b200 as G
+    from gpugraphlayout_b200 import synth
+    s, t = synth.ba_edges(1500, 3, seed=4)
+    path = str(tmp_path / "ba.txt")
+    synth.write_edgelist(path, s[::-1] + 7, t[::-1] + 7)
+    g = G.UGraph(path)
+    layout = G.GraphLayout(g)
+    fa2 = G.CUDAForceAtlas2(layout, True, False, 1.0, 80.0)
+    fa2.doSteps(20)
+    fa2.sync_layout()
+    out = str(tmp_path / "o.bin")
+    layout.writeToBin(out)
+    rec = np.fromfile(out, dtype=[("id", "<u4"), ("x", "<f4"), ("y", "<f4")])
+    assert np.array_equal(rec["id"], g.node_map_r)
+    assert np.array_equal(np.stack([rec["x"], rec["y"]], 1), layout.xy)
+    assert np.isfinite(layout.xy).all()
+
+
+def test_graph_viewer_cli_matches_api(tmp_path):
+    """graph_viewer gpu ... bin: same file as the Python mirror with the CLI's
+    defaults (srandom(1234), 10000 x 10000 box)."""
+    import gpugraphlayout_b200 as G
+    from gpugraphlayout_b200 import synth
+    s, t = synth.ba_edges(2000, 3, seed=6)
+    path = str(tmp_path / "g.txt")
+    synth.write_edgelist(path, s, t)
+    outdir = tmp_path / "out"
+    outdir.mkdir()
+    exe = os.path.join(ROOT, "gpugraphlayout_b200", "graph_viewer")
+    r = subprocess.run([exe, "gpu", "30", "1", "sg", "10", "1", "approximate", path, str(outdir),
+                        "bin"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert "fetched" in r.stdout
+    rec = np.fromfile(str(outdir / "g.txt_30.bin"), dtype=[("id", "<u4"), ("x", "<f4"), ("y", "<f4")])
+    g = G.UGraph(path)
+    layout = G.GraphLayout(g)
+    fa2 = G.CUDAForceAtlas2(layout, True, True, 1.0, 10.0)
+    for _ in range(30):
+        fa2.doStep()
+    fa2.sync_layout()
+    assert np.array_equal(rec["id"], g.node_map_r)
+    assert np.array_equal(np.stack([rec["x"], rec["y"]], 1), layout.xy)
+    # an existing output file is refused, as in the reference
+    r2 = subprocess.run([exe, "gpu", "30", "1", "sg", "10", "1", "approximate", path, str(outdir),
+                         "bin"], capture_output=True, text=True, timeout=300)
+    assert r2.returncode != 0 and "File exists" in r2.stdout
+    # exact mode is refused on the GPU path
+    r3 = subprocess.run([exe, "gpu", "3", "1", "sg", "10", "1", "exact", path, str(outdir), "bin"],
+                        capture_output=True, text=True, timeout=60)
+    assert r3.returncode != 0 and "requires Barnes-Hut" in r3.stderr
