@@ -412,7 +412,8 @@ fa2_ctx *fa2_create(const fa2_graph_desc *g, const fa2_params *prm, int *status)
         (s = dalloc(c, &b.keys[1], n)) || (s = dalloc(c, &b.vals[0], n)) ||
         (s = dalloc(c, &b.vals[1], n)) || (s = dalloc(c, &b.lcp, n)) ||
         (s = dalloc(c, &b.group, n)) || (s = dalloc(c, &b.body_node, n)) ||
-        (s = dalloc(c, &b.nodes, cap)) || (s = dalloc(c, &b.parent, cap)) ||
+        (s = dalloc(c, &b.nodes, cap + 1)) ||  // + the traversal's sentinel slot
+        (s = dalloc(c, &b.parent, cap)) ||
         (s = dalloc(c, &b.cnt, cap)) || (s = dalloc(c, &b.kids, cap)) || (s = dalloc(c, &b.warp_partial, (n + 31) / 32)) ||
         (s = dalloc(c, &b.st, 1)) || (s = dalloc(c, &c->stage_xy, n)) ||
         (s = dalloc(c, &c->stage_ids, n)))

@@ -59,9 +59,9 @@ struct IterCounters {
 };
 
 // Sort geometry (one tile per block).
-constexpr int kSortThreads = 256;
+constexpr int kSortThreads = 1024;
 constexpr int kSortWarps = kSortThreads / kWarp;
-constexpr int kSortRounds = 16;
+constexpr int kSortRounds = 4;
 constexpr int kSortTile = kSortThreads * kSortRounds;  // 4096 keys
 constexpr int kCountThreads = 256;
 constexpr int kCountItems = 4;
@@ -120,7 +120,7 @@ struct Params {
 };
 
 constexpr int kBBoxThreads = 512;
-constexpr int kTravThreads = 512;
+constexpr int kTravThreads = 256;
 constexpr int kDispThreads = 512;
 
 // ---------------------------------------------------------------- kernels --

@@ -516,10 +516,12 @@ __global__ void __launch_bounds__(256) k_summarize(int n, const uint32_t *__rest
     if (st->err || st->poison) return;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         int32_t p = parent[body_node[k]];
-        while (p >= 0) {
-            cuda::atomic_ref<int32_t, cuda::thread_scope_device> arrivals(cnt[p]);
-            if (arrivals.fetch_sub(1, cuda::memory_order_acq_rel) != 1) break;
+        // a body publishes nothing (k_emit wrote it): relaxed arrival
+        bool last = atomicSub(&cnt[p], 1) == 1;
+        while (last) {
+            cuda::atomic_thread_fence(cuda::memory_order_acquire, cuda::thread_scope_device);
             const float4 prec = __ldcg(&nodes[p]);
+            const int32_t gp = __ldcg(&parent[p]);
             const int meta = __float_as_int(prec.w);
             float cm = 0.0f, px = 0.0f, py = 0.0f;
             if (meta_level(meta) == kLevels) {
@@ -549,7 +551,11 @@ __global__ void __launch_bounds__(256) k_summarize(int n, const uint32_t *__rest
             }
             const float inv = 1.0f / cm;
             __stcg(&nodes[p], make_float4(px * inv, py * inv, cm, prec.w));
-            p = __ldcg(&parent[p]);
+            if (gp < 0) break;
+            // a cell publishes its summary to whoever completes its parent
+            cuda::atomic_ref<int32_t, cuda::thread_scope_device> arrivals(cnt[gp]);
+            last = arrivals.fetch_sub(1, cuda::memory_order_release) == 1;
+            p = gp;
         }
     }
 }
@@ -565,7 +571,7 @@ __global__ void __launch_bounds__(256) k_summarize(int n, const uint32_t *__rest
 // The tail adds gravity + attraction, forms the swing and traction sums
 // (SpeedKernel, src/RPFA2Kernels.cu:111-202) and, in the last block to
 // finish, updates the adaptive speed (:204-219).
-__global__ void __launch_bounds__(kTravThreads) k_traverse(
+__global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
     int n, const float4 *__restrict nodes, const uint32_t *__restrict body_node,
     const uint32_t *__restrict vals, const float2 *__restrict fag,
     const float2 *__restrict fprev, float2 *__restrict f, float2 *__restrict warp_partial,
@@ -590,57 +596,40 @@ __global__ void __launch_bounds__(kTravThreads) k_traverse(
     const uint32_t end = st->tree_nodes;
     const int lane = threadIdx.x & 31;
     const int nwarps = (n + 31) >> 5;
-    // Work split: first a static phase in which the warps of a block take
-    // adjacent groups (neighbouring bodies walk the same tree nodes, which
-    // then stay in L1), then a shared pool handed out one group at a time,
-    // which evens out the load.
-    constexpr int kWarpsPerBlock = kTravThreads / kWarp;
-    const int wid = threadIdx.x >> 5;
-    const int rounds = (nwarps * 3 / 4) / ((int)gridDim.x * kWarpsPerBlock);
-    const int pool0 = rounds * (int)gridDim.x * kWarpsPerBlock;
-    for (int j = 0;; ++j) {
-        int w;
-        if (j < rounds) {
-            w = (j * (int)gridDim.x + (int)blockIdx.x) * kWarpsPerBlock + wid;
-        } else {
-            w = 0;
-            if (lane == 0) w = pool0 + (int)atomicAdd(&ctr->trav_ticket, 1u);
-            w = __shfl_sync(kFull, w, 0);
-        }
+    // Groups of 32 bodies are handed out one at a time (the work per group
+    // varies with the local density of the layout).
+    for (;;) {
+        int w = 0;
+        if (lane == 0) w = (int)atomicAdd(&ctr->trav_ticket, 1u);
+        w = __shfl_sync(kFull, w, 0);
         if (w >= nwarps) break;
         const int k = w * 32 + lane;
         const bool active = k < n;
         const float4 me = nodes[body_node[active ? k : n - 1]];
-        const float px = me.x, py = me.y, kmi = prm.k_r * me.z;
+        // a lane without a body sits far away: it passes every test and its
+        // (unused) sums never feed anything
+        const float px = active ? me.x : 1e30f, py = active ? me.y : 1e30f;
+        const float kmi = prm.k_r * me.z;
         float ax = 0.0f, ay = 0.0f;
-        uint32_t node = 1, n_acc = 0, n_vis = 0;
-        float4 r = __ldg(&nodes[min(node, end - 1)]);
+        uint32_t node = 1, n_acc = 0;
         while (node < end) {
+            const float4 r = __ldg(&nodes[node]);
             const int meta = __float_as_int(r.w);
-            const uint32_t skip = meta_next(meta);
-            // both possible successors are loaded before the vote decides
-            const float4 r_in = __ldg(&nodes[min(node + 1, end - 1)]);
-            const float4 r_skip = __ldg(&nodes[min(skip, end - 1)]);
             const float dx = px - r.x, dy = py - r.y;
             const float d2 = dx * dx + dy * dy + prm.epssq;
-            const bool ok = !active || d2 >= s_dq[meta_level(meta)];
-            ++n_vis;
-            if (__all_sync(kFull, ok)) {
+            if (__all_sync(kFull, d2 >= s_dq[meta_level(meta)])) {
                 const float c = __fdividef(kmi * r.z, d2);
                 ax = fmaf(dx, c, ax);
                 ay = fmaf(dy, c, ay);
-                node = skip;
-                r = r_skip;
+                node = meta_next(meta);
                 ++n_acc;
             } else {
                 ++node;
-                r = r_in;
             }
         }
         if (lane == 0) {
             const unsigned lanes = (unsigned)min(32, n - w * 32);
             atomicAdd(&st->interactions, (unsigned long long)n_acc * lanes);
-            atomicAdd(&st->visits, (unsigned long long)n_vis * lanes);
         }
         float sw = 0.0f, tr = 0.0f;
         if (active) {

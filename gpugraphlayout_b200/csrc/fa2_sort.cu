@@ -56,7 +56,9 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t *tmp, u
     return wbase + inc - v;
 }
 
-__global__ void __launch_bounds__(kSortThreads) k_sort_pass(
+// Two 1024-thread blocks per SM (32 registers each) keep all tiles of a
+// million-body sort resident in one wave.
+__global__ void __launch_bounds__(kSortThreads, 2) k_sort_pass(
     int n, int pass, const uint64_t *__restrict kin, const uint32_t *__restrict vin,
     uint64_t *__restrict kout, uint32_t *__restrict vout, IterCounters *ctr, uint32_t *status,
     DevState *st) {
@@ -93,19 +95,25 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_pass(
     }
     __syncthreads();
 
-    // 2. per digit (thread = digit): offsets across warps, tile count, look-back
+    // 2. per digit (threads 0..255, thread = digit): offsets across warps,
+    //    tile count, look-back
     const int d = threadIdx.x;
+    const bool digit_thread = d < 256;
     uint32_t run = 0;
-#pragma unroll
-    for (int w = 0; w < kSortWarps; ++w) {
-        uint32_t c = S.whist[w][d];
-        S.whist[w][d] = run;
-        run += c;
+    if (digit_thread) {
+#pragma unroll 8
+        for (int w = 0; w < kSortWarps; ++w) {
+            uint32_t c = S.whist[w][d];
+            S.whist[w][d] = run;
+            run += c;
+        }
     }
     const uint32_t tile_count = run;
     uint32_t *my_status = status + (size_t)tile * 256;
     uint32_t prefix = 0;
-    if (tile == 0) {
+    if (!digit_thread) {
+        // no digit: only the block-wide scans below
+    } else if (tile == 0) {
         atomicExch(&my_status[d], kFlagPre | tile_count);
     } else {
         atomicExch(&my_status[d], kFlagAgg | tile_count);
@@ -127,10 +135,13 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_pass(
         atomicExch(&my_status[d], kFlagPre | (prefix + tile_count));
     }
     // global start of digit d = all keys with smaller digits + earlier tiles' d
-    const uint32_t hist_d = ctr->hist[pass][d];
+    const uint32_t hist_d = digit_thread ? ctr->hist[pass][d] : 0u;
     const uint32_t bin_base = block_excl_scan(hist_d, S.scan_tmp, nullptr);
-    S.gbase[d] = bin_base + prefix;
-    S.tile_off[d] = block_excl_scan(tile_count, S.scan_tmp, nullptr);
+    const uint32_t toff = block_excl_scan(tile_count, S.scan_tmp, nullptr);
+    if (digit_thread) {
+        S.gbase[d] = bin_base + prefix;
+        S.tile_off[d] = toff;
+    }
     __syncthreads();
 
     // 3. regroup by digit in shared memory, then write digit runs

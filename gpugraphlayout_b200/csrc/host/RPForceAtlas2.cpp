@@ -5,6 +5,7 @@
 
 #include <vector>
 
+#include "RPCPUForceAtlas2.hpp"
 #include "RPGPUForceAtlas2.hpp"
 #include "fa2b200.h"
 
@@ -127,4 +128,15 @@ namespace RPGraph
     }
 
     void CUDAForceAtlas2::sync_layout() { retrieveLayoutFromGPU(); }
+
+    CPUForceAtlas2::CPUForceAtlas2(GraphLayout &layout, bool use_barneshut, bool strong_gravity,
+                                   float gravity, float scale)
+        : ForceAtlas2(layout, use_barneshut, strong_gravity, gravity, scale)
+    {
+        fprintf(stderr, "error: this build provides the GPU (CUDAForceAtlas2) path only.\n");
+        exit(EXIT_FAILURE);
+    }
+    CPUForceAtlas2::~CPUForceAtlas2() {}
+    void CPUForceAtlas2::doStep() {}
+    void CPUForceAtlas2::sync_layout() {}
 }

@@ -63,8 +63,12 @@ def test_deep_pair_order_and_repulsion():
     assert e.stats()["max_level"] == 32
     tot, ga = e.forces()
     rep = tot - ga
+    assert np.abs(rep).sum() > 0  # the reference adds nothing here
     exact = O.exact_repulsion_f64(xy, g.mass, 1.0, np.arange(4, dtype=np.int32))
-    assert rel_rmse(rep, exact) < 1e-3
+    # Below level ~21 the cell threshold (2w)^2 is under the softening eps,
+    # so in float d^2+eps and dq+eps both round to eps and the reference's
+    # rule takes the pair's own cell whole: a ~1e-3 effect, not exactness.
+    assert rel_rmse(rep, exact) < 1e-2
 
 
 @pytest.mark.parametrize("pairs", [[(0, 1)], [(0, 1), (1, 2)], [(5, 9), (9, 2), (2, 5), (7, 5)]])
