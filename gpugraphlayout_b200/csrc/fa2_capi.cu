@@ -23,10 +23,10 @@ using namespace fa2;
 
 namespace {
 
-constexpr int kNumSlots = 9;
-const char *const kSlotNames[kNumSlots] = {"attract", "keys",      "sort",     "runs",    "tree_count",
+constexpr int kNumSlots = 8;
+const char *const kSlotNames[kNumSlots] = {"attract", "keys",      "sort",     "tree_count",
                                            "emit",    "summarize", "traverse", "displace"};
-enum Slot { S_ATTRACT, S_KEYS, S_SORT, S_RUNS, S_COUNT, S_EMIT, S_SUMM, S_TRAV, S_DISP };
+enum Slot { S_ATTRACT, S_KEYS, S_SORT, S_COUNT, S_EMIT, S_SUMM, S_TRAV, S_DISP };
 
 constexpr int kMaxReplayRounds = 64;
 
@@ -157,7 +157,9 @@ void build_graph(fa2_ctx *c, const fa2_graph_desc *g, std::vector<uint32_t> &off
         bk.row_end = (int)r1;
         bk.lanes = lanes;
         bk.block_begin = blocks;
-        int rows_per_block = lanes == 256 ? 1 : (256 / 32) * (32 / lanes);
+        int rows_per_block = lanes == 256 ? 1
+                             : lanes == 32 ? 256 / 32
+                                           : (256 / 32) * (32 / lanes) * kAttractBatch;
         blocks += (int)((r1 - r + rows_per_block - 1) / rows_per_block);
         r = r1;
     }
@@ -190,9 +192,6 @@ void enqueue_iteration(fa2_ctx *c, bool full, bool perturb_first, bool timed) {
     mark(S_SORT, 0, A);
     launch_sort(b, A);
     mark(S_SORT, 1, A);
-    mark(S_RUNS, 0, A);
-    launch_runs(b, 0, c->nsm, A);
-    mark(S_RUNS, 1, A);
     mark(S_COUNT, 0, A);
     launch_tree_count(b, A);
     mark(S_COUNT, 1, A);
@@ -425,16 +424,17 @@ fa2_ctx *fa2_create(const fa2_graph_desc *g, const fa2_params *prm, int *status)
     b.csr_off = d_off;
     b.csr_col4 = d_col;
     b.ref_of = d_ref;
-    // one memset clears counters, histograms and look-back flags
-    const size_t sort_status = (size_t)8 * sort_tiles((int)n) * 256;
+    // one memset clears counters, histograms, per-tile digit counts and the
+    // tree-count look-back flags
+    const size_t sort_counts = (size_t)8 * sort_tiles((int)n) * 256;
     const size_t count_status = (size_t)count_tiles((int)n);
-    c->scratch_bytes = sizeof(IterCounters) + 4 * (sort_status + count_status);
+    c->scratch_bytes = sizeof(IterCounters) + 4 * (sort_counts + count_status);
     char *scr = nullptr;
     if ((s = dalloc(c, &scr, c->scratch_bytes))) return fail(s);
     c->scratch = scr;
     b.ctr = (IterCounters *)scr;
-    b.sort_status = (uint32_t *)(scr + sizeof(IterCounters));
-    b.count_status = b.sort_status + sort_status;
+    b.sort_counts = (uint32_t *)(scr + sizeof(IterCounters));
+    b.count_status = b.sort_counts + sort_counts;
 
     if (cudaStreamCreateWithFlags(&c->sA, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->sB, cudaStreamNonBlocking) != cudaSuccess ||

@@ -24,7 +24,6 @@ constexpr int kDeepLevels = 64;    // levels past 32 used to order such a run
 
 // Device error bits (DevState::err).  Any of them stops the iteration.
 enum : int {
-    kErrSortWait = 1,      // a sort tile waited too long on its predecessor
     kErrScanWait = 2,      // a tree-count tile waited too long
     kErrRunTooLong = 4,    // more than kMaxRun bodies share a 64-bit key
     kErrTreeTooLarge = 8,  // the quadtree needs more nodes than allocated
@@ -78,6 +77,7 @@ struct AttractBucket {
     int block_begin;         // first block index of this bucket
 };
 constexpr int kMaxBuckets = 8;
+constexpr int kAttractBatch = 4;  // row groups per warp in short-row buckets
 struct AttractPlan {
     AttractBucket b[kMaxBuckets];
     int nbuckets;
@@ -109,7 +109,7 @@ struct Buffers {
     float2 *warp_partial;     // one per 32 sorted bodies
     DevState *st;
     IterCounters *ctr;
-    uint32_t *sort_status;    // [8][sort tiles][256]
+    uint32_t *sort_counts;    // [8][sort tiles][256]: digit counts per tile and pass
     uint32_t *count_status;   // [count tiles]
 };
 

@@ -145,16 +145,21 @@ __global__ void __launch_bounds__(kBBoxThreads) k_bbox(int n, const float2 *__re
 
 // ------------------------------------------------------------------- keys --
 
+// One block per sort tile: the tile's keys, the digit-0 counts of the tile
+// (the first sort pass's per-tile input) and the tile's share of the digit
+// histograms of all eight passes (order-independent, so counted once here).
 __global__ void __launch_bounds__(256) k_keys(int n, const float2 *__restrict pos,
                                               const DevState *__restrict st,
                                               uint64_t *__restrict keys, uint32_t *__restrict vals,
-                                              IterCounters *ctr) {
+                                              IterCounters *ctr, uint32_t *__restrict counts0) {
     __shared__ unsigned s_hist[8][256];
     if (st->err || st->poison) return;
     for (int j = threadIdx.x; j < 8 * 256; j += blockDim.x) (&s_hist[0][0])[j] = 0;
     __syncthreads();
     const float rx = st->rootx, ry = st->rooty, rr = st->radius;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int tile0 = blockIdx.x * kSortTile;
+    const int tile_end = min(n, tile0 + kSortTile);
+    for (int i = tile0 + threadIdx.x; i < tile_end; i += blockDim.x) {
         float2 p = pos[i];
         uint64_t key = morton_key(p.x, p.y, rx, ry, rr);
         keys[i] = key;
@@ -165,6 +170,7 @@ __global__ void __launch_bounds__(256) k_keys(int n, const float2 *__restrict po
     __syncthreads();
     for (int j = threadIdx.x; j < 8 * 256; j += blockDim.x) {
         unsigned c = (&s_hist[0][0])[j];
+        if (j < 256) counts0[(size_t)blockIdx.x * 256 + j] = c;
         if (c) atomicAdd(&(&ctr->hist[0][0])[j], c);
     }
 }
@@ -201,52 +207,58 @@ __device__ bool deep_less(float2 pa, float2 pb, uint32_t ida, uint32_t idb, floa
     return ida < idb;
 }
 
-// One thread per run of equal keys: order the run, then either flag exactly
-// coincident bodies (perturb == 0) or scale every body that sits on an
-// earlier one (lower reference id) by .99, as the reference's insertion does
-// for the later-inserted body (src/RPBHKernels.cu:271-278).
+// The run of equal keys that starts at sorted body k: order it, then either
+// flag exactly coincident bodies (perturb == 0) or scale every body that sits
+// on an earlier one (lower reference id) by .99, as the reference's insertion
+// does for the later-inserted body (src/RPBHKernels.cu:271-278).
+__device__ void fix_run(int k, int n, const uint64_t *__restrict keys, uint32_t *__restrict vals,
+                        float2 *__restrict pos, const uint32_t *__restrict ref_of, DevState *st,
+                        int perturb) {
+    const uint64_t key = keys[k];
+    int len = 2;
+    while (k + len < n && keys[k + len] == key && len <= kMaxRun) ++len;
+    if (len > kMaxRun) {
+        atomicOr(&st->err, kErrRunTooLong);
+        return;
+    }
+    float cx, cy, cr;
+    key_centre(key, st->rootx, st->rooty, st->radius, cx, cy, cr);
+    uint32_t *v = vals + k;
+    for (int a = 1; a < len; ++a) {  // insertion sort, stable
+        const uint32_t va = v[a];
+        const float2 pa = pos[va];
+        int b = a - 1;
+        while (b >= 0) {
+            const uint32_t vb = v[b];
+            if (!deep_less(pa, pos[vb], ref_of[va], ref_of[vb], cx, cy, cr)) break;
+            v[b + 1] = vb;
+            --b;
+        }
+        v[b + 1] = va;
+    }
+    // coincident neighbours (equal positions are adjacent after ordering)
+    bool any = false;
+    float2 prev = pos[v[0]];
+    for (int a = 1; a < len; ++a) {
+        const float2 p = pos[v[a]];
+        const bool same = p.x == prev.x && p.y == prev.y;
+        prev = p;
+        if (!same) continue;
+        any = true;
+        if (perturb) pos[v[a]] = make_float2((float)((double)p.x * .99), (float)((double)p.y * .99));
+    }
+    if (any && !perturb) atomicAdd(&st->poison, 1);
+}
+
+// Replay path: the runs of the last sort, with the .99 scaling applied.
 __global__ void __launch_bounds__(256) k_runs(int n, const uint64_t *__restrict keys,
                                               uint32_t *__restrict vals, float2 *__restrict pos,
                                               const uint32_t *__restrict ref_of, DevState *st,
                                               int perturb) {
     if (st->err || st->poison) return;
-    const float rx = st->rootx, ry = st->rooty, rr = st->radius;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k + 1 < n; k += gridDim.x * blockDim.x) {
-        uint64_t key = keys[k];
-        if (keys[k + 1] != key || (k > 0 && keys[k - 1] == key)) continue;
-        int len = 2;
-        while (k + len < n && keys[k + len] == key && len <= kMaxRun) ++len;
-        if (len > kMaxRun) {
-            atomicOr(&st->err, kErrRunTooLong);
-            continue;
-        }
-        float cx, cy, cr;
-        key_centre(key, rx, ry, rr, cx, cy, cr);
-        uint32_t *v = vals + k;
-        for (int a = 1; a < len; ++a) {  // insertion sort, stable
-            uint32_t va = v[a];
-            float2 pa = pos[va];
-            int b = a - 1;
-            while (b >= 0) {
-                uint32_t vb = v[b];
-                if (!deep_less(pa, pos[vb], ref_of[va], ref_of[vb], cx, cy, cr)) break;
-                v[b + 1] = vb;
-                --b;
-            }
-            v[b + 1] = va;
-        }
-        // coincident neighbours (equal positions are adjacent after ordering)
-        bool any = false;
-        float2 prev = pos[v[0]];
-        for (int a = 1; a < len; ++a) {
-            float2 p = pos[v[a]];
-            bool same = p.x == prev.x && p.y == prev.y;
-            prev = p;
-            if (!same) continue;
-            any = true;
-            if (perturb) pos[v[a]] = make_float2((float)((double)p.x * .99), (float)((double)p.y * .99));
-        }
-        if (any && !perturb) atomicAdd(&st->poison, 1);
+        if (keys[k + 1] != keys[k] || (k > 0 && keys[k - 1] == keys[k])) continue;
+        fix_run(k, n, keys, vals, pos, ref_of, st, perturb);
     }
 }
 
@@ -264,7 +276,8 @@ __device__ __forceinline__ int cells_at(int k, int Lk, int Lkm1) {
 __global__ void __launch_bounds__(kCountThreads) k_tree_count(
     int n, const uint64_t *__restrict keys, int8_t *__restrict lcp, uint32_t *__restrict group,
     int32_t *__restrict cnt, int4 *__restrict kids, uint32_t capacity, DevState *st, IterCounters *ctr,
-    uint32_t *status) {
+    uint32_t *status, uint32_t *__restrict vals, float2 *__restrict pos,
+    const uint32_t *__restrict ref_of) {
     __shared__ int s_tile;
     __shared__ uint32_t s_warp[kCountThreads / kWarp];
     __shared__ uint32_t s_prefix;
@@ -274,7 +287,7 @@ __global__ void __launch_bounds__(kCountThreads) k_tree_count(
     const int tile = s_tile;
     const int base = tile * kCountTile + threadIdx.x * kCountItems;
     int g[kCountItems];
-    uint32_t sum = 0;
+    uint32_t sum = 0, run_starts = 0;
 #pragma unroll
     for (int e = 0; e < kCountItems; ++e) {
         int k = base + e;
@@ -284,6 +297,8 @@ __global__ void __launch_bounds__(kCountThreads) k_tree_count(
             int Lkm1 = lcp_at(keys, n, k - 1);
             lcp[k] = (int8_t)Lk;
             g[e] = cells_at(k, Lk, Lkm1) + 1;
+            // a run of equal 64-bit keys starts here (trees past depth 32)
+            if (Lk == kLevels && Lkm1 != kLevels) run_starts |= 1u << e;
         }
         sum += (uint32_t)g[e];
     }
@@ -353,6 +368,10 @@ __global__ void __launch_bounds__(kCountThreads) k_tree_count(
         }
         off += (uint32_t)g[e];
     }
+    // after this tile's offsets are published, so a long run delays no one
+#pragma unroll
+    for (int e = 0; e < kCountItems; ++e)
+        if (run_starts & (1u << e)) fix_run(base + e, n, keys, vals, pos, ref_of, st, 0);
 }
 
 // ------------------------------------------------------------------- emit --
@@ -744,44 +763,85 @@ __global__ void __launch_bounds__(kDispThreads) k_displace(int n, float2 *__rest
 // atomics).  Rows hold neighbour ids padded with the row's own id to a
 // multiple of four (a padding entry adds p_i - p_i = 0), so a lane loads four
 // ids with one 16-byte load.  `lanes` lanes share a row and reduce with
-// shuffles; heavy rows take a whole block.
+// shuffles; heavy rows take a whole block.  To keep many loads in flight a
+// warp of a short-row bucket works on kAttractBatch groups of rows at once:
+// all column loads first, then all position gathers.
+__device__ __forceinline__ void add_four(const int4 c, const float2 p,
+                                         const float2 *__restrict pos, float &ax, float &ay) {
+    const float2 q0 = __ldg(&pos[c.x]), q1 = __ldg(&pos[c.y]);
+    const float2 q2 = __ldg(&pos[c.z]), q3 = __ldg(&pos[c.w]);
+    ax += (q0.x - p.x) + (q1.x - p.x) + ((q2.x - p.x) + (q3.x - p.x));
+    ay += (q0.y - p.y) + (q1.y - p.y) + ((q2.y - p.y) + (q3.y - p.y));
+}
+
+__device__ __forceinline__ float2 with_gravity(float2 p, float m, float ax, float ay,
+                                               const Params &prm) {
+    float f_g;
+    if (prm.strong_gravity)
+        f_g = prm.k_g * m;
+    else if (p.x != 0.0f || p.y != 0.0f)
+        f_g = prm.k_g * m * rsqrtf(p.x * p.x + p.y * p.y);
+    else
+        f_g = 0.0f;
+    return make_float2(-p.x * f_g + ax, -p.y * f_g + ay);
+}
+
+// Rows of at most LANES int4 chunks (LANES <= 16): one chunk per lane.
 template <int LANES>
-__device__ __forceinline__ void attract_group(int row, bool valid, const float2 *__restrict pos,
-                                              const float *__restrict mass,
-                                              const uint32_t *__restrict off,
-                                              const int4 *__restrict col4, float2 *__restrict fag,
-                                              const Params &prm, int sl) {
-    float ax = 0.0f, ay = 0.0f;
-    float2 p = make_float2(0.0f, 0.0f);
-    if (valid) {
-        p = pos[row];
-        const uint32_t b = off[row] >> 2, e = off[row + 1] >> 2;
-        for (uint32_t q = b + sl; q < e; q += LANES) {
-            const int4 c = __ldcs(&col4[q]);
-            const float2 q0 = __ldg(&pos[c.x]), q1 = __ldg(&pos[c.y]);
-            const float2 q2 = __ldg(&pos[c.z]), q3 = __ldg(&pos[c.w]);
-            ax += (q0.x - p.x) + (q1.x - p.x) + ((q2.x - p.x) + (q3.x - p.x));
-            ay += (q0.y - p.y) + (q1.y - p.y) + ((q2.y - p.y) + (q3.y - p.y));
-        }
+__device__ __forceinline__ void attract_short_rows(int row0, int row_end,
+                                                   const float2 *__restrict pos,
+                                                   const float *__restrict mass,
+                                                   const uint32_t *__restrict off,
+                                                   const int4 *__restrict col4,
+                                                   float2 *__restrict fag, const Params &prm,
+                                                   int lane) {
+    constexpr int R = 32 / LANES;  // rows per warp and batch
+    const int sub = lane / LANES, sl = lane % LANES;
+    int row[kAttractBatch];
+    bool has[kAttractBatch];
+    int4 c[kAttractBatch];
+    float2 p[kAttractBatch];
+#pragma unroll
+    for (int u = 0; u < kAttractBatch; ++u) {
+        row[u] = row0 + u * R + sub;
+        const bool valid = row[u] < row_end;
+        const uint32_t q = valid ? (off[row[u]] >> 2) + sl : 0u;
+        const uint32_t e = valid ? off[row[u] + 1] >> 2 : 0u;
+        has[u] = q < e;
+        c[u] = has[u] ? __ldcs(&col4[q]) : make_int4(0, 0, 0, 0);
+        p[u] = valid ? pos[row[u]] : make_float2(0.0f, 0.0f);
     }
-    if (LANES > 1) {
+#pragma unroll
+    for (int u = 0; u < kAttractBatch; ++u) {
+        float ax = 0.0f, ay = 0.0f;
+        if (has[u]) add_four(c[u], p[u], pos, ax, ay);
 #pragma unroll
         for (int o = LANES / 2; o > 0; o >>= 1) {
             ax += __shfl_xor_sync(kFull, ax, o);
             ay += __shfl_xor_sync(kFull, ay, o);
         }
+        if (row[u] < row_end && sl == 0)
+            fag[row[u]] = with_gravity(p[u], mass[row[u]], ax, ay, prm);
     }
-    if (valid && sl == 0) {
-        const float m = mass[row];
-        float f_g;
-        if (prm.strong_gravity)
-            f_g = prm.k_g * m;
-        else if (p.x != 0.0f || p.y != 0.0f)
-            f_g = prm.k_g * m * rsqrtf(p.x * p.x + p.y * p.y);
-        else
-            f_g = 0.0f;
-        fag[row] = make_float2(-p.x * f_g + ax, -p.y * f_g + ay);
+}
+
+// Partial attraction of one row over chunks [b + first, e) with stride
+// STRIDE, four chunks in flight per lane.
+template <int STRIDE>
+__device__ __forceinline__ void attract_long_row(uint32_t b, uint32_t e, int first, float2 p,
+                                                 const float2 *__restrict pos,
+                                                 const int4 *__restrict col4, float &ax,
+                                                 float &ay) {
+    uint32_t q = b + first;
+    for (; q + 3 * STRIDE < e; q += 4 * STRIDE) {
+        const int4 c0 = __ldcs(&col4[q]), c1 = __ldcs(&col4[q + STRIDE]);
+        const int4 c2 = __ldcs(&col4[q + 2 * STRIDE]), c3 = __ldcs(&col4[q + 3 * STRIDE]);
+        add_four(c0, p, pos, ax, ay);
+        add_four(c1, p, pos, ax, ay);
+        add_four(c2, p, pos, ax, ay);
+        add_four(c3, p, pos, ax, ay);
     }
+    for (; q < e; q += STRIDE) add_four(__ldcs(&col4[q]), p, pos, ax, ay);
 }
 
 __global__ void __launch_bounds__(256) k_attract(AttractPlan plan, const float2 *__restrict pos,
@@ -801,15 +861,8 @@ __global__ void __launch_bounds__(256) k_attract(AttractPlan plan, const float2 
         // one row per block
         const int row = bk.row_begin + blk;
         const float2 p = pos[row];
-        const uint32_t b = off[row] >> 2, e = off[row + 1] >> 2;
         float ax = 0.0f, ay = 0.0f;
-        for (uint32_t q = b + threadIdx.x; q < e; q += 256) {
-            const int4 c = __ldcs(&col4[q]);
-            const float2 q0 = __ldg(&pos[c.x]), q1 = __ldg(&pos[c.y]);
-            const float2 q2 = __ldg(&pos[c.z]), q3 = __ldg(&pos[c.w]);
-            ax += (q0.x - p.x) + (q1.x - p.x) + ((q2.x - p.x) + (q3.x - p.x));
-            ay += (q0.y - p.y) + (q1.y - p.y) + ((q2.y - p.y) + (q3.y - p.y));
-        }
+        attract_long_row<256>(off[row] >> 2, off[row + 1] >> 2, threadIdx.x, p, pos, col4, ax, ay);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             ax += __shfl_xor_sync(kFull, ax, o);
@@ -824,29 +877,33 @@ __global__ void __launch_bounds__(256) k_attract(AttractPlan plan, const float2 
                 ax += s_red[w].x;
                 ay += s_red[w].y;
             }
-            const float m = mass[row];
-            float f_g;
-            if (prm.strong_gravity)
-                f_g = prm.k_g * m;
-            else if (p.x != 0.0f || p.y != 0.0f)
-                f_g = prm.k_g * m * rsqrtf(p.x * p.x + p.y * p.y);
-            else
-                f_g = 0.0f;
-            fag[row] = make_float2(-p.x * f_g + ax, -p.y * f_g + ay);
+            fag[row] = with_gravity(p, mass[row], ax, ay, prm);
         }
         return;
     }
-    const int rows_per_warp = 32 / bk.lanes;
-    const int sub = lane / bk.lanes, sl = lane % bk.lanes;
-    const int row = bk.row_begin + (blk * (256 / kWarp) + wid) * rows_per_warp + sub;
-    const bool valid = row < bk.row_end;
+    if (bk.lanes == 32) {
+        // one row per warp
+        const int row = bk.row_begin + blk * (256 / kWarp) + wid;
+        if (row >= bk.row_end) return;
+        const float2 p = pos[row];
+        float ax = 0.0f, ay = 0.0f;
+        attract_long_row<32>(off[row] >> 2, off[row + 1] >> 2, lane, p, pos, col4, ax, ay);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            ax += __shfl_xor_sync(kFull, ax, o);
+            ay += __shfl_xor_sync(kFull, ay, o);
+        }
+        if (lane == 0) fag[row] = with_gravity(p, mass[row], ax, ay, prm);
+        return;
+    }
+    // short rows: kAttractBatch groups of 32/lanes rows per warp
+    const int row0 = bk.row_begin + (blk * (256 / kWarp) + wid) * kAttractBatch * (32 / bk.lanes);
     switch (bk.lanes) {
-        case 32: attract_group<32>(row, valid, pos, mass, off, col4, fag, prm, sl); break;
-        case 16: attract_group<16>(row, valid, pos, mass, off, col4, fag, prm, sl); break;
-        case 8: attract_group<8>(row, valid, pos, mass, off, col4, fag, prm, sl); break;
-        case 4: attract_group<4>(row, valid, pos, mass, off, col4, fag, prm, sl); break;
-        case 2: attract_group<2>(row, valid, pos, mass, off, col4, fag, prm, sl); break;
-        default: attract_group<1>(row, valid, pos, mass, off, col4, fag, prm, sl); break;
+        case 16: attract_short_rows<16>(row0, bk.row_end, pos, mass, off, col4, fag, prm, lane); break;
+        case 8: attract_short_rows<8>(row0, bk.row_end, pos, mass, off, col4, fag, prm, lane); break;
+        case 4: attract_short_rows<4>(row0, bk.row_end, pos, mass, off, col4, fag, prm, lane); break;
+        case 2: attract_short_rows<2>(row0, bk.row_end, pos, mass, off, col4, fag, prm, lane); break;
+        default: attract_short_rows<1>(row0, bk.row_end, pos, mass, off, col4, fag, prm, lane); break;
     }
 }
 
@@ -884,8 +941,9 @@ void launch_bbox(const Buffers &b, int nblocks, cudaStream_t s) {
 }
 
 void launch_keys(const Buffers &b, int nsm, cudaStream_t s) {
-    k_keys<<<grid_for(b.n, 256, nsm * 8), 256, 0, s>>>(b.n, b.pos, b.st, b.keys[0], b.vals[0],
-                                                       b.ctr);
+    (void)nsm;
+    k_keys<<<sort_tiles(b.n), 256, 0, s>>>(b.n, b.pos, b.st, b.keys[0], b.vals[0], b.ctr,
+                                           b.sort_counts);
 }
 
 void launch_runs(const Buffers &b, int perturb, int nsm, cudaStream_t s) {
@@ -894,9 +952,9 @@ void launch_runs(const Buffers &b, int perturb, int nsm, cudaStream_t s) {
 }
 
 void launch_tree_count(const Buffers &b, cudaStream_t s) {
-    k_tree_count<<<count_tiles(b.n), kCountThreads, 0, s>>>(b.n, b.keys[0], b.lcp, b.group, b.cnt, b.kids,
-                                                            b.capacity, b.st, b.ctr,
-                                                            b.count_status);
+    k_tree_count<<<count_tiles(b.n), kCountThreads, 0, s>>>(
+        b.n, b.keys[0], b.lcp, b.group, b.cnt, b.kids, b.capacity, b.st, b.ctr, b.count_status,
+        b.vals[0], b.pos, b.ref_of);
 }
 
 void launch_emit(const Buffers &b, int nsm, cudaStream_t s) {
