@@ -23,10 +23,10 @@ using namespace fa2;
 
 namespace {
 
-constexpr int kNumSlots = 8;
-const char *const kSlotNames[kNumSlots] = {"attract", "keys",      "sort",     "tree_count",
-                                           "emit",    "summarize", "traverse", "displace"};
-enum Slot { S_ATTRACT, S_KEYS, S_SORT, S_COUNT, S_EMIT, S_SUMM, S_TRAV, S_DISP };
+constexpr int kNumSlots = 7;
+const char *const kSlotNames[kNumSlots] = {"attract", "keys",     "sort",    "tree_count",
+                                           "emit",    "traverse", "displace"};
+enum Slot { S_ATTRACT, S_KEYS, S_SORT, S_COUNT, S_EMIT, S_TRAV, S_DISP };
 
 constexpr int kMaxReplayRounds = 64;
 
@@ -198,9 +198,6 @@ void enqueue_iteration(fa2_ctx *c, bool full, bool perturb_first, bool timed) {
     mark(S_EMIT, 0, A);
     launch_emit(b, c->nsm, A);
     mark(S_EMIT, 1, A);
-    mark(S_SUMM, 0, A);
-    launch_summarize(b, c->nsm, A);
-    mark(S_SUMM, 1, A);
     if (full) cudaStreamWaitEvent(A, c->evJoin, 0);
     mark(S_TRAV, 0, A);
     launch_traverse(b, c->kp, c->trav_blocks, A);
@@ -412,8 +409,9 @@ fa2_ctx *fa2_create(const fa2_graph_desc *g, const fa2_params *prm, int *status)
         (s = dalloc(c, &b.vals[1], n)) || (s = dalloc(c, &b.lcp, n)) ||
         (s = dalloc(c, &b.group, n)) || (s = dalloc(c, &b.body_node, n)) ||
         (s = dalloc(c, &b.nodes, cap + 1)) ||  // + the traversal's sentinel slot
-        (s = dalloc(c, &b.parent, cap)) ||
-        (s = dalloc(c, &b.cnt, cap)) || (s = dalloc(c, &b.kids, cap)) || (s = dalloc(c, &b.warp_partial, (n + 31) / 32)) ||
+        (s = dalloc(c, &b.pm, (size_t)n + 1)) || (s = dalloc(c, &b.pxy, 2 * ((size_t)n + 1))) ||
+        (s = dalloc(c, &b.lookback, (size_t)count_tiles((int)n))) ||
+        (s = dalloc(c, &b.warp_partial, (n + 31) / 32)) ||
         (s = dalloc(c, &b.st, 1)) || (s = dalloc(c, &c->stage_xy, n)) ||
         (s = dalloc(c, &c->stage_ids, n)))
         return fail(s);

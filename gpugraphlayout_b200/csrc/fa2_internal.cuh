@@ -1,8 +1,8 @@
 // fa2_internal.cuh -- device data layout and kernel entry points of the B200
 // ForceAtlas2 engine.  Host code in fa2_capi.cu enqueues one iteration as
 //
-//   stream A: bbox -> keys -> sort (8 passes) -> runs -> tree_count -> emit
-//             -> summarize -> [join B] -> traverse (+ speed) -> displace
+//   stream A: keys -> sort (8 passes) -> tree_count -> emit -> [join B]
+//             -> traverse (+ speed) -> displace (+ next bounding box)
 //   stream B: attract (gravity + attraction)
 //
 // which replaces the eleven launches of CUDAForceAtlas2::doStep
@@ -84,6 +84,13 @@ struct AttractPlan {
     int nblocks;
 };
 
+// Tile sums of k_tree_count's single-pass scan (written before the tile's
+// flag word is set; see fa2_tree.cu).
+struct LookbackSums {
+    long long agg_m, incl_m;
+    __int128 agg_x, agg_y, incl_x, incl_y;
+};
+
 struct Buffers {
     int n;
     // per node, internal (degree-descending) order
@@ -99,11 +106,11 @@ struct Buffers {
     int8_t *lcp;              // n
     uint32_t *group;          // n: first preorder node of body k's group
     uint32_t *body_node;      // n: preorder node of sorted body k
-    float4 *nodes;            // capacity: x, y, mass, meta
-    int32_t *parent;          // capacity
-    int32_t *cnt;             // capacity: child counters
-    int4 *kids;               // capacity: first four children of each cell
+    float4 *nodes;            // capacity + 1: x, y, mass, meta (+ traversal sentinel)
     uint32_t capacity;
+    long long *pm;            // n + 1: exclusive prefix of mass over sorted bodies
+    __int128 *pxy;            // 2(n + 1): prefix of mass x fixed-point offset, x and y
+    LookbackSums *lookback;   // count tiles: tile sums of the tree-count scan
     // reductions
     float4 *bbox_partial;     // bbox blocks
     float2 *warp_partial;     // one per 32 sorted bodies
@@ -130,7 +137,6 @@ void launch_sort(const Buffers &b, cudaStream_t s);
 void launch_runs(const Buffers &b, int perturb, int nsm, cudaStream_t s);
 void launch_tree_count(const Buffers &b, cudaStream_t s);
 void launch_emit(const Buffers &b, int nsm, cudaStream_t s);
-void launch_summarize(const Buffers &b, int nsm, cudaStream_t s);
 void launch_traverse(const Buffers &b, const Params &p, int nblocks, cudaStream_t s);
 void launch_displace(const Buffers &b, int nsm, cudaStream_t s);
 void launch_attract(const Buffers &b, const Params &p, const AttractPlan &plan, cudaStream_t s);

@@ -1,49 +1,23 @@
 // fa2_kernels.cu -- the per-iteration kernels of the B200 ForceAtlas2 engine
-// except the radix sort (fa2_sort.cu).
+// around the quadtree: bounding box, Morton keys, force traversal (+ speed),
+// displacement, attraction, and the id permutations of the C ABI.  The radix
+// sort is in fa2_sort.cu, the tree build in fa2_tree.cu.
 //
-// Quadtree.  The reference builds its quadtree by concurrent lock-based
-// insertion (src/RPBHKernels.cu:184-329); the shape of that tree does not
-// depend on insertion order: its cells are exactly the quadrant prefixes that
-// hold at least two bodies.  Here the same tree is built without locks:
-//   keys        each body's 32 quadrant digits, computed with the reference's
-//               float cell-centre arithmetic and tie rule (:217-241), form a
-//               64-bit Morton key;
-//   sort        keys ascending = the reference's in-order body order (sortd);
-//   runs        equal keys (only possible past depth 32) are ordered by
-//               deeper digits; exactly coincident bodies are flagged;
-//   tree_count  LCP of neighbouring keys (in quadrant digits) gives, per
-//               body k, the cells that start at k: levels L[k-1]+1 .. L[k];
-//               a scan gives every node its preorder index;
-//   emit        writes each node once: position/mass of bodies, level and
-//               subtree end of cells, parent links;
-//   summarize   bottom-up mass and centre of mass, children in quadrant order
-//               (SummarizationKernel :357-506), with the last child to finish
-//               computing its parent instead of spin-waiting.
-// The tree is stored in preorder with each node's "next" index (the node
-// after its subtree), so the traversal needs no stack.
+// Keys: each body's 32 quadrant digits, computed with the reference's float
+// cell-centre arithmetic and tie rule (src/RPBHKernels.cu:217-241), form a
+// 64-bit Morton key; keys ascending give the reference's in-order body order
+// (sortd).  The tree is stored in preorder with each node's "next" index (the
+// node after its subtree), so the traversal needs no stack.
 #include <float.h>
 #include <stdint.h>
 
-#include <cuda/atomic>
-
-#include "fa2_internal.cuh"
+#include "fa2_device.cuh"
 
 namespace fa2 {
 
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-
-__device__ __forceinline__ int lcp_digits(uint64_t a, uint64_t b) {
-    uint64_t x = a ^ b;
-    return x == 0 ? kLevels : (__clzll(x) >> 1);
-}
-
-__device__ __forceinline__ int meta_level(int meta) { return meta & 63; }
-__device__ __forceinline__ uint32_t meta_next(int meta) { return (uint32_t)meta >> kMetaShift; }
-__device__ __forceinline__ float make_meta(uint32_t next, int level) {
-    return __int_as_float((int)((next << kMetaShift) | (uint32_t)level));
-}
 
 // Quadrant digits of (px, py) under the root cell, computed the way
 // TreeBuildingKernel walks down (src/RPBHKernels.cu:217-241): the child
@@ -148,7 +122,7 @@ __global__ void __launch_bounds__(kBBoxThreads) k_bbox(int n, const float2 *__re
 // One block per sort tile: the tile's keys, the digit-0 counts of the tile
 // (the first sort pass's per-tile input) and the tile's share of the digit
 // histograms of all eight passes (order-independent, so counted once here).
-__global__ void __launch_bounds__(256) k_keys(int n, const float2 *__restrict pos,
+__global__ void __launch_bounds__(1024) k_keys(int n, const float2 *__restrict pos,
                                               const DevState *__restrict st,
                                               uint64_t *__restrict keys, uint32_t *__restrict vals,
                                               IterCounters *ctr, uint32_t *__restrict counts0) {
@@ -172,410 +146,6 @@ __global__ void __launch_bounds__(256) k_keys(int n, const float2 *__restrict po
         unsigned c = (&s_hist[0][0])[j];
         if (j < 256) counts0[(size_t)blockIdx.x * 256 + j] = c;
         if (c) atomicAdd(&(&ctr->hist[0][0])[j], c);
-    }
-}
-
-// ------------------------------------------------------------------- runs --
-
-// Replays the cell centre of a 32-digit key path.
-__device__ __forceinline__ void key_centre(uint64_t key, float rx, float ry, float rr, float &x,
-                                           float &y, float &r) {
-    x = rx;
-    y = ry;
-    r = rr;
-    for (int lvl = 0; lvl < kLevels; ++lvl) {
-        r *= 0.5f;
-        int j = (int)(key >> (2 * (kLevels - 1 - lvl))) & 3;
-        x = __fadd_rn(x, (j & 1) ? r : -r);
-        y = __fadd_rn(y, (j & 2) ? r : -r);
-    }
-}
-
-// Orders two bodies that share all 32 digits by the digits below level 32
-// (the reference keeps splitting: src/RPBHKernels.cu:282-313), then by
-// reference id.  Returns true if a goes first.
-__device__ bool deep_less(float2 pa, float2 pb, uint32_t ida, uint32_t idb, float x, float y,
-                          float r) {
-    for (int lvl = 0; lvl < kDeepLevels; ++lvl) {
-        r *= 0.5f;
-        int ja = (x < pa.x ? 1 : 0) | (y < pa.y ? 2 : 0);
-        int jb = (x < pb.x ? 1 : 0) | (y < pb.y ? 2 : 0);
-        if (ja != jb) return ja < jb;
-        x = __fadd_rn(x, (ja & 1) ? r : -r);
-        y = __fadd_rn(y, (ja & 2) ? r : -r);
-    }
-    return ida < idb;
-}
-
-// The run of equal keys that starts at sorted body k: order it, then either
-// flag exactly coincident bodies (perturb == 0) or scale every body that sits
-// on an earlier one (lower reference id) by .99, as the reference's insertion
-// does for the later-inserted body (src/RPBHKernels.cu:271-278).
-__device__ void fix_run(int k, int n, const uint64_t *__restrict keys, uint32_t *__restrict vals,
-                        float2 *__restrict pos, const uint32_t *__restrict ref_of, DevState *st,
-                        int perturb) {
-    const uint64_t key = keys[k];
-    int len = 2;
-    while (k + len < n && keys[k + len] == key && len <= kMaxRun) ++len;
-    if (len > kMaxRun) {
-        atomicOr(&st->err, kErrRunTooLong);
-        return;
-    }
-    float cx, cy, cr;
-    key_centre(key, st->rootx, st->rooty, st->radius, cx, cy, cr);
-    uint32_t *v = vals + k;
-    for (int a = 1; a < len; ++a) {  // insertion sort, stable
-        const uint32_t va = v[a];
-        const float2 pa = pos[va];
-        int b = a - 1;
-        while (b >= 0) {
-            const uint32_t vb = v[b];
-            if (!deep_less(pa, pos[vb], ref_of[va], ref_of[vb], cx, cy, cr)) break;
-            v[b + 1] = vb;
-            --b;
-        }
-        v[b + 1] = va;
-    }
-    // coincident neighbours (equal positions are adjacent after ordering)
-    bool any = false;
-    float2 prev = pos[v[0]];
-    for (int a = 1; a < len; ++a) {
-        const float2 p = pos[v[a]];
-        const bool same = p.x == prev.x && p.y == prev.y;
-        prev = p;
-        if (!same) continue;
-        any = true;
-        if (perturb) pos[v[a]] = make_float2((float)((double)p.x * .99), (float)((double)p.y * .99));
-    }
-    if (any && !perturb) atomicAdd(&st->poison, 1);
-}
-
-// Replay path: the runs of the last sort, with the .99 scaling applied.
-__global__ void __launch_bounds__(256) k_runs(int n, const uint64_t *__restrict keys,
-                                              uint32_t *__restrict vals, float2 *__restrict pos,
-                                              const uint32_t *__restrict ref_of, DevState *st,
-                                              int perturb) {
-    if (st->err || st->poison) return;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k + 1 < n; k += gridDim.x * blockDim.x) {
-        if (keys[k + 1] != keys[k] || (k > 0 && keys[k - 1] == keys[k])) continue;
-        fix_run(k, n, keys, vals, pos, ref_of, st, perturb);
-    }
-}
-
-// ------------------------------------------------------------- tree count --
-
-__device__ __forceinline__ int lcp_at(const uint64_t *__restrict keys, int n, int k) {
-    return (k < 0 || k >= n - 1) ? -1 : lcp_digits(keys[k], keys[k + 1]);
-}
-
-// cells that start at sorted body k
-__device__ __forceinline__ int cells_at(int k, int Lk, int Lkm1) {
-    return k == 0 ? max(Lk, 0) + 1 : max(0, Lk - Lkm1);
-}
-
-__global__ void __launch_bounds__(kCountThreads) k_tree_count(
-    int n, const uint64_t *__restrict keys, int8_t *__restrict lcp, uint32_t *__restrict group,
-    int32_t *__restrict cnt, int4 *__restrict kids, uint32_t capacity, DevState *st, IterCounters *ctr,
-    uint32_t *status, uint32_t *__restrict vals, float2 *__restrict pos,
-    const uint32_t *__restrict ref_of) {
-    __shared__ int s_tile;
-    __shared__ uint32_t s_warp[kCountThreads / kWarp];
-    __shared__ uint32_t s_prefix;
-    if (st->err || st->poison) return;
-    if (threadIdx.x == 0) s_tile = atomicAdd(&ctr->count_ticket, 1u);
-    __syncthreads();
-    const int tile = s_tile;
-    const int base = tile * kCountTile + threadIdx.x * kCountItems;
-    int g[kCountItems];
-    uint32_t sum = 0, run_starts = 0;
-#pragma unroll
-    for (int e = 0; e < kCountItems; ++e) {
-        int k = base + e;
-        g[e] = 0;
-        if (k < n) {
-            int Lk = lcp_at(keys, n, k);
-            int Lkm1 = lcp_at(keys, n, k - 1);
-            lcp[k] = (int8_t)Lk;
-            g[e] = cells_at(k, Lk, Lkm1) + 1;
-            // a run of equal 64-bit keys starts here (trees past depth 32)
-            if (Lk == kLevels && Lkm1 != kLevels) run_starts |= 1u << e;
-        }
-        sum += (uint32_t)g[e];
-    }
-    // block exclusive scan of per-thread sums
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    uint32_t inc = sum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        uint32_t t = __shfl_up_sync(kFull, inc, o);
-        if (lane >= o) inc += t;
-    }
-    if (lane == 31) s_warp[wid] = inc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        uint32_t run = 0;
-        for (int w = 0; w < kCountThreads / kWarp; ++w) {
-            uint32_t t = s_warp[w];
-            s_warp[w] = run;
-            run += t;
-        }
-        // decoupled look-back over tiles: flag in bit 31, value below
-        const uint32_t kAgg = 1u << 30, kPre = 2u << 30, kMask = (1u << 30) - 1;
-        uint32_t prefix = 0;
-        if (tile == 0) {
-            atomicExch(&status[0], kPre | run);
-        } else {
-            atomicExch(&status[tile], kAgg | run);
-            int t = tile - 1;
-            long spins = 0;
-            while (t >= 0) {
-                uint32_t s = *((volatile uint32_t *)&status[t]);
-                if ((s >> 30) == 0) {
-                    if (++spins > (1L << 22)) {
-                        atomicOr(&st->err, kErrScanWait);
-                        break;
-                    }
-                    continue;
-                }
-                prefix += s & kMask;
-                if ((s >> 30) == 2) break;
-                --t;
-            }
-            atomicExch(&status[tile], kPre | (prefix + run));
-        }
-        s_prefix = prefix;
-    }
-    __syncthreads();
-    uint32_t off = s_prefix + s_warp[wid] + inc - sum;
-#pragma unroll
-    for (int e = 0; e < kCountItems; ++e) {
-        int k = base + e;
-        if (k < n) {
-            group[k] = off;
-            for (int q = 0; q < g[e]; ++q)
-                if (off + q < capacity) {
-                    cnt[off + q] = 0;
-                    kids[off + q] = make_int4(-1, -1, -1, -1);
-                }
-            if (k == n - 1) {
-                uint32_t total = off + (uint32_t)g[e];
-                st->tree_nodes = total;
-                st->max_level = 0;  // raised by k_emit
-                st->interactions = 0;  // counted by k_traverse
-                st->visits = 0;
-                if (total > capacity) atomicOr(&st->err, kErrTreeTooLarge);
-            }
-        }
-        off += (uint32_t)g[e];
-    }
-    // after this tile's offsets are published, so a long run delays no one
-#pragma unroll
-    for (int e = 0; e < kCountItems; ++e)
-        if (run_starts & (1u << e)) fix_run(base + e, n, keys, vals, pos, ref_of, st, 0);
-}
-
-// ------------------------------------------------------------------- emit --
-
-__device__ __forceinline__ int load_lcp(const int8_t *__restrict lcp, int n, int k) {
-    return (k < 0 || k >= n - 1) ? -1 : (int)lcp[k];
-}
-
-// preorder index of sorted body b
-__device__ __forceinline__ uint32_t body_index(const int8_t *__restrict lcp,
-                                               const uint32_t *__restrict group, int n, int b) {
-    int Lb = load_lcp(lcp, n, b), Lbm1 = load_lcp(lcp, n, b - 1);
-    return group[b] + (uint32_t)cells_at(b, Lb, Lbm1);
-}
-
-// Index of the cell at level lam that contains sorted body k, given that it
-// starts before k: its first body a is the smallest j with LCP(K_j, K_k) >= lam.
-__device__ uint32_t find_cell(const uint64_t *__restrict keys, const int8_t *__restrict lcp,
-                              const uint32_t *__restrict group, int n, int k, int lam) {
-    const uint64_t kk = keys[k];
-    int ok = k - 1;  // known to satisfy
-    int step = 1, bad = -1;
-    for (;;) {
-        int j = ok - step;
-        if (j < 0) {
-            bad = -1;
-            break;
-        }
-        if (lcp_digits(keys[j], kk) >= lam) {
-            ok = j;
-            step <<= 1;
-        } else {
-            bad = j;
-            break;
-        }
-    }
-    // smallest satisfying index in (bad, ok]
-    int lo = bad + 1, hi = ok;
-    while (lo < hi) {
-        int mid = (lo + hi) >> 1;
-        if (lcp_digits(keys[mid], kk) >= lam)
-            hi = mid;
-        else
-            lo = mid + 1;
-    }
-    const int a = lo;
-    const int lo_level = a == 0 ? 0 : load_lcp(lcp, n, a - 1) + 1;
-    return group[a] + (uint32_t)(lam - lo_level);
-}
-
-// Largest j >= k with LCP(K_k, K_j) >= lvl (the last body of the cell at
-// level lvl that starts at k).
-__device__ int find_end(const uint64_t *__restrict keys, int n, int k, int lvl) {
-    const uint64_t kk = keys[k];
-    int ok = k, step = 1, bad = n;
-    for (;;) {
-        int j = ok + step;
-        if (j >= n) {
-            bad = n;
-            break;
-        }
-        if (lcp_digits(keys[j], kk) >= lvl) {
-            ok = j;
-            step <<= 1;
-        } else {
-            bad = j;
-            break;
-        }
-    }
-    int lo = ok, hi = bad - 1;  // largest satisfying in [ok, bad)
-    while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (lcp_digits(keys[mid], kk) >= lvl)
-            lo = mid;
-        else
-            hi = mid - 1;
-    }
-    return lo;
-}
-
-__global__ void __launch_bounds__(256) k_emit(int n, const uint64_t *__restrict keys,
-                                              const uint32_t *__restrict vals,
-                                              const int8_t *__restrict lcp,
-                                              const uint32_t *__restrict group,
-                                              const float2 *__restrict pos,
-                                              const float *__restrict mass, float4 *__restrict nodes,
-                                              int32_t *__restrict parent, int32_t *__restrict cnt,
-                                              int4 *__restrict kids,
-                                              uint32_t *__restrict body_node, DevState *st) {
-    if (st->err || st->poison) return;
-    int local_max = 0;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const int Lk = load_lcp(lcp, n, k), Lkm1 = load_lcp(lcp, n, k - 1);
-        const int c = cells_at(k, Lk, Lkm1);
-        const uint32_t Gk = group[k];
-        const uint32_t bnode = Gk + (uint32_t)c;
-        const int lo_level = k == 0 ? 0 : Lkm1 + 1;
-        // the body
-        const uint32_t i = vals[k];
-        const float2 p = pos[i];
-        nodes[bnode] = make_float4(p.x, p.y, mass[i], make_meta(bnode + 1, kBodyLevel));
-        body_node[k] = bnode;
-        const int lam = max(max(Lk, Lkm1), 0);
-        const uint32_t pb = c > 0 ? bnode - 1 : find_cell(keys, lcp, group, n, k, lam);
-        parent[bnode] = (int32_t)pb;
-        {
-            const int slot = atomicAdd(&cnt[pb], 1);
-            if (slot < 4) reinterpret_cast<int *>(kids)[4 * (size_t)pb + slot] = (int)bnode;
-        }
-        // the cells that start here, outermost first
-        for (int q = 0; q < c; ++q) {
-            const int lvl = lo_level + q;
-            const uint32_t node = Gk + (uint32_t)q;
-            const int b = lvl == 0 ? n - 1 : find_end(keys, n, k, lvl);
-            const uint32_t next = body_index(lcp, group, n, b) + 1;
-            nodes[node] = make_float4(0.0f, 0.0f, 0.0f, make_meta(next, lvl));
-            int32_t par = -1;
-            if (q > 0)
-                par = (int32_t)node - 1;
-            else if (lvl > 0)
-                par = (int32_t)find_cell(keys, lcp, group, n, k, lvl - 1);
-            parent[node] = par;
-            if (par >= 0) {
-                const int slot = atomicAdd(&cnt[par], 1);
-                if (slot < 4) reinterpret_cast<int *>(kids)[4 * (size_t)par + slot] = (int)node;
-            }
-            local_max = max(local_max, lvl);
-        }
-    }
-    local_max = __reduce_max_sync(kFull, local_max);
-    if ((threadIdx.x & 31) == 0 && local_max > 0) atomicMax(&st->max_level, local_max);
-}
-
-// -------------------------------------------------------------- summarize --
-
-__device__ __forceinline__ void cswap(uint32_t &a, uint32_t &b) {
-    const uint32_t lo = min(a, b), hi = max(a, b);
-    a = lo;
-    b = hi;
-}
-
-__device__ __forceinline__ void add_child(const float4 &r, float &cm, float &px, float &py) {
-    const float m = r.z;
-    px += r.x * m;
-    py += r.y * m;
-    cm += m;
-}
-
-// Bottom-up cell mass and centre of mass.  Every node decrements its
-// parent's child counter (acquire-release, so the last child sees what the
-// others wrote); the child that brings it to zero computes the parent from
-// all its children, in quadrant order, as SummarizationKernel does
-// (src/RPBHKernels.cu:461-494), and continues upwards.  A cell's children
-// come from the four slots k_emit filled; preorder index order is quadrant
-// order.  Level-32 cells can hold more bodies than four slots and are
-// walked through their next links instead.
-__global__ void __launch_bounds__(256) k_summarize(int n, const uint32_t *__restrict body_node,
-                                                   const int32_t *__restrict parent,
-                                                   int32_t *cnt, const int4 *__restrict kids,
-                                                   float4 *nodes, DevState *st) {
-    if (st->err || st->poison) return;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        int32_t p = parent[body_node[k]];
-        // a body publishes nothing (k_emit wrote it): relaxed arrival
-        bool last = atomicSub(&cnt[p], 1) == 1;
-        while (last) {
-            cuda::atomic_thread_fence(cuda::memory_order_acquire, cuda::thread_scope_device);
-            const float4 prec = __ldcg(&nodes[p]);
-            const int32_t gp = __ldcg(&parent[p]);
-            const int meta = __float_as_int(prec.w);
-            float cm = 0.0f, px = 0.0f, py = 0.0f;
-            if (meta_level(meta) == kLevels) {
-                const uint32_t end = meta_next(meta);
-                for (uint32_t c = (uint32_t)p + 1; c < end;) {
-                    const float4 r = __ldcg(&nodes[c]);
-                    add_child(r, cm, px, py);
-                    c = meta_next(__float_as_int(r.w));
-                }
-            } else {
-                const int4 kd = __ldcg(&kids[p]);
-                uint32_t c0 = (uint32_t)kd.x, c1 = (uint32_t)kd.y, c2 = (uint32_t)kd.z,
-                         c3 = (uint32_t)kd.w;  // empty slots are -1: sorted last
-                cswap(c0, c1);
-                cswap(c2, c3);
-                cswap(c0, c2);
-                cswap(c1, c3);
-                cswap(c1, c2);
-                const float4 r0 = __ldcg(&nodes[c0]);
-                const float4 r1 = c1 != ~0u ? __ldcg(&nodes[c1]) : make_float4(0, 0, 0, 0);
-                const float4 r2 = c2 != ~0u ? __ldcg(&nodes[c2]) : make_float4(0, 0, 0, 0);
-                const float4 r3 = c3 != ~0u ? __ldcg(&nodes[c3]) : make_float4(0, 0, 0, 0);
-                add_child(r0, cm, px, py);
-                if (c1 != ~0u) add_child(r1, cm, px, py);
-                if (c2 != ~0u) add_child(r2, cm, px, py);
-                if (c3 != ~0u) add_child(r3, cm, px, py);
-            }
-            const float inv = 1.0f / cm;
-            __stcg(&nodes[p], make_float4(px * inv, py * inv, cm, prec.w));
-            if (gp < 0) break;
-            // a cell publishes its summary to whoever completes its parent
-            cuda::atomic_ref<int32_t, cuda::thread_scope_device> arrivals(cnt[gp]);
-            last = arrivals.fetch_sub(1, cuda::memory_order_release) == 1;
-            p = gp;
-        }
     }
 }
 
@@ -942,31 +512,13 @@ void launch_bbox(const Buffers &b, int nblocks, cudaStream_t s) {
 
 void launch_keys(const Buffers &b, int nsm, cudaStream_t s) {
     (void)nsm;
-    k_keys<<<sort_tiles(b.n), 256, 0, s>>>(b.n, b.pos, b.st, b.keys[0], b.vals[0], b.ctr,
+    k_keys<<<sort_tiles(b.n), 1024, 0, s>>>(b.n, b.pos, b.st, b.keys[0], b.vals[0], b.ctr,
                                            b.sort_counts);
 }
 
-void launch_runs(const Buffers &b, int perturb, int nsm, cudaStream_t s) {
-    k_runs<<<grid_for(b.n, 256, nsm * 8), 256, 0, s>>>(b.n, b.keys[0], b.vals[0], b.pos, b.ref_of,
-                                                       b.st, perturb);
-}
 
-void launch_tree_count(const Buffers &b, cudaStream_t s) {
-    k_tree_count<<<count_tiles(b.n), kCountThreads, 0, s>>>(
-        b.n, b.keys[0], b.lcp, b.group, b.cnt, b.kids, b.capacity, b.st, b.ctr, b.count_status,
-        b.vals[0], b.pos, b.ref_of);
-}
 
-void launch_emit(const Buffers &b, int nsm, cudaStream_t s) {
-    k_emit<<<grid_for(b.n, 256, nsm * 8), 256, 0, s>>>(b.n, b.keys[0], b.vals[0], b.lcp, b.group,
-                                                       b.pos, b.mass, b.nodes, b.parent, b.cnt, b.kids,
-                                                       b.body_node, b.st);
-}
 
-void launch_summarize(const Buffers &b, int nsm, cudaStream_t s) {
-    k_summarize<<<grid_for(b.n, 256, nsm * 8), 256, 0, s>>>(b.n, b.body_node, b.parent, b.cnt, b.kids,
-                                                            b.nodes, b.st);
-}
 
 void launch_traverse(const Buffers &b, const Params &p, int nblocks, cudaStream_t s) {
     k_traverse<<<nblocks, kTravThreads, 0, s>>>(b.n, b.nodes, b.body_node, b.vals[0], b.fag,

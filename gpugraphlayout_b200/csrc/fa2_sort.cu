@@ -30,6 +30,7 @@ struct SortSmem {
     uint32_t whist[kSortWarps][256];  // per-warp digit counts, then offsets
     uint32_t tile_off[256];           // exclusive scan of tile digit counts
     uint32_t gbase[256];              // global start of this tile's digit run
+    uint32_t part[kSortThreads / 256][256];  // partial prefixes over earlier tiles
     uint32_t scan_tmp[kSortWarps];
 };
 
@@ -64,6 +65,22 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_sort_pass(
     const int base = tile * kSortTile + wid * (kSortTile / kSortWarps);
     const unsigned lt_mask = (1u << lane) - 1u;
 
+    // 0. this tile's prefix per digit: the counts of all earlier tiles, summed
+    //    by 4 threads per digit with 8 loads in flight each, started first so
+    //    that the loads overlap the ranking below
+    uint32_t prefix_part;
+    {
+        const uint32_t *cp = counts + (size_t)pass * ntiles * 256 + (threadIdx.x & 255);
+        uint32_t a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        int t = threadIdx.x >> 8;
+        for (; t + 28 < tile; t += 32) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) a[j] += __ldcg(cp + (size_t)(t + 4 * j) * 256);
+        }
+        for (; t < tile; t += 4) a[0] += __ldcg(cp + (size_t)t * 256);
+        prefix_part = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+    }
+
     // 1. load the warp's chunk (all loads in flight), then rank round by round
     uint64_t k[kSortRounds];
     uint32_t v[kSortRounds];
@@ -93,6 +110,8 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_sort_pass(
     //    earlier tiles, global start
     const int d = threadIdx.x;
     const bool digit_thread = d < 256;
+    S.part[threadIdx.x >> 8][threadIdx.x & 255] = prefix_part;
+    __syncthreads();
     uint32_t tile_count = 0, prefix = 0, hist_d = 0;
     if (digit_thread) {
 #pragma unroll 8
@@ -101,17 +120,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_sort_pass(
             S.whist[w][d] = tile_count;
             tile_count += c;
         }
-        const uint32_t *cp = counts + (size_t)pass * ntiles * 256 + d;
-        uint32_t p0 = 0, p1 = 0, p2 = 0, p3 = 0;
-        int t = 0;
-        for (; t + 3 < tile; t += 4) {
-            p0 += __ldcg(cp + (size_t)t * 256);
-            p1 += __ldcg(cp + (size_t)(t + 1) * 256);
-            p2 += __ldcg(cp + (size_t)(t + 2) * 256);
-            p3 += __ldcg(cp + (size_t)(t + 3) * 256);
-        }
-        for (; t < tile; ++t) p0 += __ldcg(cp + (size_t)t * 256);
-        prefix = (p0 + p1) + (p2 + p3);
+        prefix = (S.part[0][d] + S.part[1][d]) + (S.part[2][d] + S.part[3][d]);
         hist_d = ctr->hist[pass][d];
     }
     const uint32_t bin_base = block_excl_scan(hist_d, S.scan_tmp);
