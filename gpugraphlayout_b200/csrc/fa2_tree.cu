@@ -12,7 +12,7 @@
 //                 plus itself), and one single-pass scan over the sorted
 //                 bodies that gives every node its preorder index and, in the
 //                 same pass, exact prefix sums of mass and mass x position
-//                 (integers: mass is degree + 1; positions in 2^-32 steps of
+//                 (integers: mass is degree + 1; positions in 2^-48 steps of
 //                 the root radius; 128-bit sums), so any cell's mass and centre
 //                 of mass are two prefix differences.  It also orders runs of
 //                 equal 64-bit keys (trees deeper than 32 levels) and flags
@@ -155,11 +155,14 @@ __device__ __forceinline__ double i128_to_double(i128 v) {
     return (double)hi * 18446744073709551616.0 + (double)lo;
 }
 
-// Fixed-point offset from the root centre, in 2^-32 root radii, kept within
-// +-2^39 so that mass (< 2^24) x offset fits 64 bits.
+// Fixed-point offset from the root centre, in 2^-48 root radii (finer than a
+// float32 ulp of any coordinate but the tiniest), kept within +-2^55 (a body
+// scaled by .99 may sit outside the box); mass (< 2^24) x offset is formed in
+// 128 bits and a sum over 2^25 bodies stays below 2^105.
+constexpr double kFixedScale = 281474976710656.0;  // 2^48
 __device__ __forceinline__ long long fixed_offset(float p, float root, double scale) {
     double q = ((double)p - (double)root) * scale;
-    q = fmin(fmax(q, -549755813888.0), 549755813888.0);
+    q = fmin(fmax(q, -36028797018963968.0), 36028797018963968.0);
     return __double2ll_rn(q);
 }
 
@@ -190,7 +193,7 @@ __global__ void __launch_bounds__(kCountThreads) k_tree_count(
     __syncthreads();
     const int tile = s_tile;
     const int base = tile * kCountTile + threadIdx.x * kCountItems;
-    const double scale = st->radius > 0.0f ? 4294967296.0 / (double)st->radius : 1.0;
+    const double scale = st->radius > 0.0f ? kFixedScale / (double)st->radius : 1.0;
     const float rx = st->rootx, ry = st->rooty;
     int g[kCountItems];
     long long im[kCountItems], qx[kCountItems], qy[kCountItems];
@@ -392,7 +395,7 @@ __global__ void __launch_bounds__(256) k_emit(int n, const uint64_t *__restrict 
                                               float4 *__restrict nodes,
                                               uint32_t *__restrict body_node, DevState *st) {
     if (st->err || st->poison) return;
-    const double inv_scale = st->radius > 0.0f ? (double)st->radius / 4294967296.0 : 1.0;
+    const double inv_scale = st->radius > 0.0f ? (double)st->radius / kFixedScale : 1.0;
     const double rx = st->rootx, ry = st->rooty;
     int local_max = 0;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
