@@ -27,7 +27,6 @@ enum : int {
     kErrScanWait = 2,      // a tree-count tile waited too long
     kErrRunTooLong = 4,    // more than kMaxRun bodies share a 64-bit key
     kErrTreeTooLarge = 8,  // the quadtree needs more nodes than allocated
-    kErrWorkWait = 16,     // a traversal warp waited too long for a work chunk
 };
 
 // Scalars that live on the device for the whole run.
@@ -129,7 +128,6 @@ struct Params {
 
 constexpr int kBBoxThreads = 512;
 constexpr int kTravThreads = 1024;
-constexpr int kTravChunk = 32;  // groups of 32 bodies per work chunk of a block
 constexpr int kDispThreads = 512;
 
 // ---------------------------------------------------------------- kernels --

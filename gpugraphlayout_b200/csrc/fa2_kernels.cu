@@ -168,10 +168,8 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
     __shared__ float s_dq[64];
     __shared__ bool s_last;
     __shared__ float s_red[2][kTravThreads / kWarp];
-    __shared__ unsigned s_claim;  // current chunk << 16 | next group in it
     if (st->err || st->poison) return;
     if (threadIdx.x == 0) {
-        s_claim = atomicAdd(&ctr->trav_ticket, 1u) << 16;
         // src/RPBHKernels.cu:579-592: dq for the children of the root is
         // (2 radius)^2 / theta^2 + eps, quartering per level.
         float tmp = st->radius * 2;
@@ -187,39 +185,13 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
     const uint32_t end = st->tree_nodes;
     const int lane = threadIdx.x & 31;
     const int nwarps = (n + 31) >> 5;
-    // Groups of 32 bodies are handed out dynamically (the work per group
-    // varies with the local density of the layout), in chunks of kTravChunk
-    // adjacent groups per block: the warps of a block walk nearby bodies and
-    // share the tree nodes they load in L1.  The warp that first finds the
-    // block's chunk used up takes the next chunk from the global counter; the
-    // others wait for it (a bounded wait).
-    const unsigned nchunks = (unsigned)((nwarps + kTravChunk - 1) / kTravChunk);
+    // Groups of 32 bodies are handed out one at a time from a global ticket:
+    // the work per group varies with the local density of the layout, and
+    // warps that take consecutive tickets walk neighbouring bodies, so the
+    // nodes they load are shared in L2.
     for (;;) {
         int w = 0;
-        if (lane == 0) {
-            w = -1;
-            for (int spin = 0; spin < (1 << 20); ++spin) {
-                const unsigned c = atomicAdd(&s_claim, 1u);
-                const unsigned chunk = c >> 16, idx = c & 0xffffu;
-                if (chunk >= nchunks) {
-                    w = nwarps;
-                    break;
-                }
-                if (idx < (unsigned)kTravChunk) {
-                    w = (int)(chunk * kTravChunk + idx);
-                    break;
-                }
-                if (idx == (unsigned)kTravChunk) {
-                    atomicExch(&s_claim, atomicAdd(&ctr->trav_ticket, 1u) << 16);
-                    continue;
-                }
-                __nanosleep(64);
-            }
-            if (w < 0) {
-                atomicOr(&st->err, kErrWorkWait);
-                w = nwarps;
-            }
-        }
+        if (lane == 0) w = (int)atomicAdd(&ctr->trav_ticket, 1u);
         w = __shfl_sync(kFull, w, 0);
         if (w >= nwarps) break;
         const int k = w * 32 + lane;
