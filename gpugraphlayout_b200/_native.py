@@ -17,7 +17,7 @@ EXPORTS = (
     "fa2_default_params", "fa2_create", "fa2_destroy", "fa2_set_positions",
     "fa2_get_positions", "fa2_step", "fa2_step_timed", "fa2_kernel_name",
     "fa2_get_stats", "fa2_get_forces", "fa2_get_sort_order", "fa2_set_speed_state",
-    "fa2_get_speed_state", "fa2_set_force_params", "fa2_ugraph_load",
+    "fa2_get_speed_state", "fa2_set_force_params", "fa2_repulsion_noalloc", "fa2_ugraph_load",
     "fa2_ugraph_from_pairs", "fa2_ugraph_free", "fa2_ugraph_num_nodes",
     "fa2_ugraph_num_edges", "fa2_ugraph_node_map_r", "fa2_ugraph_degrees",
     "fa2_ugraph_edges", "fa2_random_positions", "fa2_write_layout",
@@ -25,6 +25,7 @@ EXPORTS = (
 )
 
 FA2_OK = 0
+FA2_NOALLOC_MAX_BODIES = 8192  # include/fa2b200.h
 STATUS_NAMES = {
     0: "FA2_OK", 1: "FA2_ERR_INVALID_ARGUMENT", 2: "FA2_ERR_NO_DEVICE", 3: "FA2_ERR_CUDA",
     4: "FA2_ERR_OUT_OF_MEMORY", 5: "FA2_ERR_DEVICE_LIMIT", 6: "FA2_ERR_TOO_LARGE",
@@ -93,6 +94,7 @@ def lib():
     L.fa2_set_speed_state.argtypes = [vp, C.c_float, C.c_float, vp]
     L.fa2_get_speed_state.argtypes = [vp, f32p, f32p, vp]
     L.fa2_set_force_params.argtypes = [vp, C.c_float, C.c_float]
+    L.fa2_repulsion_noalloc.argtypes = [vp, vp, C.c_uint32, C.POINTER(Params), vp, vp]
     L.fa2_ugraph_load.restype = vp
     L.fa2_ugraph_load.argtypes = [C.c_char_p, ip]
     L.fa2_ugraph_from_pairs.restype = vp

@@ -144,6 +144,47 @@ int fa2_get_speed_state(fa2_ctx *ctx, float *global_speed, float *speed_efficien
 int fa2_set_force_params(fa2_ctx *ctx, float scale, float gravity);
 
 /* ------------------------------------------------------------------------
+ * Repulsion without allocation.  No counterpart in the reference: there the
+ * repulsion runs only inside CUDAForceAtlas2::doStep, on buffers that the
+ * constructor allocated (src/RPGPUForceAtlas2.cu:109-149).
+ * ---------------------------------------------------------------------- */
+
+/* Largest body count fa2_repulsion_noalloc accepts. */
+#define FA2_NOALLOC_MAX_BODIES 8192
+
+/* Barnes-Hut repulsion of n bodies whose positions (d_xy, n interleaved x,y
+ * floats) and masses (d_mass) already sit in device memory of prm->device;
+ * writes the n repulsive forces (interleaved x,y) to d_force there.  They are
+ * the repulsion fa2_step computes for the same positions and masses: the same
+ * quadtree, cell test (prm->theta, prm->epssq) and strength k_r = prm->scale.
+ * Gravity, attraction, the speed rule and the displacement are not applied.
+ *
+ * For callers that must not allocate at the point of the call: code under a
+ * fixed device-memory budget, or inside a host framework whose caching
+ * allocator it may not touch, or a process that reserved the device's memory
+ * up front.  No call allocates device or host memory.  All scratch lives in
+ * one fixed array in the library's device memory, about 5 MB per device,
+ * held from the time the library's kernels are loaded on that device.
+ *
+ *  - n > FA2_NOALLOC_MAX_BODIES returns FA2_ERR_TOO_LARGE before any work.
+ *  - The first call on a device does set-up: it looks up the scratch array's
+ *    address with that device current and sets kernel attributes (and, like
+ *    any first CUDA call, may create the device's context).  Make it before
+ *    any stream capture.
+ *  - The work is enqueued on `stream` (a cudaStream_t; NULL is the default
+ *    stream) and the call waits for that stream before it returns, then
+ *    reports: coincident bodies -> FA2_ERR_INVALID_ARGUMENT (fa2_step would
+ *    move them apart; this call does not), a device-side bound ->
+ *    FA2_ERR_DEVICE_LIMIT.
+ *  - There is one scratch array per device: calls that overlap on the same
+ *    device (several host threads, or several streams) race on it and give
+ *    wrong forces.  Serialise them.
+ *  - d_xy and d_force 8-byte aligned, d_mass 4-byte aligned; d_force must not
+ *    overlap d_xy or d_mass. */
+int fa2_repulsion_noalloc(const float *d_xy, const float *d_mass, uint32_t n,
+                          const fa2_params *prm, void *stream, float *d_force);
+
+/* ------------------------------------------------------------------------
  * Host graph layer: RPGraph::UGraph and GraphLayout behind plain C, for
  * callers that bind the C ABI instead of the C++ classes.
  * ---------------------------------------------------------------------- */

@@ -1,0 +1,78 @@
+"""fa2_repulsion_noalloc (all scratch in a static device array, nothing
+allocated per call) against the repulsion of fa2_step on the same positions
+and masses, through the C ABI.
+
+fa2_step's forces come back as the total and the gravity + attraction part;
+their difference is the repulsion, rounded once more by the subtraction, so
+the comparison is a relative RMSE of at most 1e-5 (the same tree, cell tests
+and walk order give the same terms).  Two calls in a row, on different
+positions, check that each call starts from cleared scratch.  This file runs
+last in the suite and also passes on its own in a fresh process, where its
+first call does the per-device set-up.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import rel_rmse
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def _params(scale):
+    from gpugraphlayout_b200 import _native
+    prm = _native.Params()
+    _native.lib().fa2_default_params(C.byref(prm))
+    prm.scale = scale
+    return prm
+
+
+def _noalloc(xy_dev, mass_dev, out_dev, prm, n=None):
+    from gpugraphlayout_b200 import _native
+    n = xy_dev.shape[0] if n is None else n
+    return _native.lib().fa2_repulsion_noalloc(
+        C.c_void_p(xy_dev.data_ptr()), C.c_void_p(mass_dev.data_ptr()), n, C.byref(prm), None,
+        C.c_void_p(out_dev.data_ptr()))
+
+
+def _step_repulsion(g, xy, scale):
+    from gpugraphlayout_b200 import Engine
+    e = Engine(g.n, g.sources, g.targets, strong_gravity=False, gravity=1.0, scale=scale)
+    e.set_positions(xy)
+    e.step(1)
+    tot, ga = e.forces()
+    return tot - ga
+
+
+def test_noalloc_matches_step_on_two_calls_in_a_row():
+    """The largest accepted size, then a smaller graph: the second call must
+    not see anything the first one left in the scratch."""
+    import torch
+    from gpugraphlayout_b200 import _native, synth
+    from oracle import oracle as O
+    prm = _params(10.0)
+    for n, seed in ((_native.FA2_NOALLOC_MAX_BODIES, 11), (3000, 12)):
+        s, t = synth.ba_edges(n, 3, seed=seed)
+        g = O.Graph(s, t)
+        assert g.n == n
+        xy = O.random_positions(g.n, 2000, 2000, seed)
+        out = torch.full((g.n, 2), float("nan"), dtype=torch.float32, device="cuda")
+        mass = torch.from_numpy(g.mass).cuda()
+        assert _noalloc(torch.from_numpy(xy).cuda(), mass, out, prm) == 0
+        got = out.cpu().numpy()
+        assert np.isfinite(got).all()
+        assert rel_rmse(got, _step_repulsion(g, xy, 10.0)) <= TOL, n
+
+
+def test_noalloc_rejects_more_bodies_than_its_scratch_holds():
+    import torch
+    from gpugraphlayout_b200 import _native
+    n = _native.FA2_NOALLOC_MAX_BODIES + 1
+    xy = torch.zeros((n, 2), dtype=torch.float32, device="cuda")
+    mass = torch.ones(n, dtype=torch.float32, device="cuda")
+    out = torch.full((n, 2), 7.0, dtype=torch.float32, device="cuda")
+    assert _noalloc(xy, mass, out, _params(1.0)) == 6  # FA2_ERR_TOO_LARGE
+    assert bool((out == 7.0).all())  # nothing ran
