@@ -409,6 +409,7 @@ fa2_ctx *fa2_create(const fa2_graph_desc *g, const fa2_params *prm, int *status)
         (s = dalloc(c, &b.vals[1], n)) || (s = dalloc(c, &b.lcp, n)) ||
         (s = dalloc(c, &b.group, n)) || (s = dalloc(c, &b.body_node, n)) ||
         (s = dalloc(c, &b.nodes, cap + 1)) ||  // + the traversal's sentinel slot
+        (s = dalloc(c, &b.owner, cap)) ||
         (s = dalloc(c, &b.pm, (size_t)n + 1)) || (s = dalloc(c, &b.pxy, 2 * ((size_t)n + 1))) ||
         (s = dalloc(c, &b.lookback, (size_t)count_tiles((int)n))) ||
         (s = dalloc(c, &b.warp_partial, (n + 31) / 32)) ||

@@ -106,6 +106,7 @@ struct Buffers {
     int8_t *lcp;              // n
     uint32_t *group;          // n: first preorder node of body k's group
     uint32_t *body_node;      // n: preorder node of sorted body k
+    uint32_t *owner;          // capacity: per node, sorted body k << 6 | cell offset (63: body)
     float4 *nodes;            // capacity + 1: x, y, mass, meta (+ traversal sentinel)
     uint32_t capacity;
     long long *pm;            // n + 1: exclusive prefix of mass over sorted bodies

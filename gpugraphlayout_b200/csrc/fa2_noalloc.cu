@@ -48,7 +48,8 @@ constexpr size_t kOffLcp = up256(kOffVals1 + 4ull * kMaxBodies);
 constexpr size_t kOffGroup = up256(kOffLcp + 1ull * kMaxBodies);
 constexpr size_t kOffBodyNode = up256(kOffGroup + 4ull * kMaxBodies);
 constexpr size_t kOffNodes = up256(kOffBodyNode + 4ull * kMaxBodies);
-constexpr size_t kOffPm = up256(kOffNodes + 16ull * (kMaxNodes + 1));
+constexpr size_t kOffOwner = up256(kOffNodes + 16ull * (kMaxNodes + 1));
+constexpr size_t kOffPm = up256(kOffOwner + 4ull * kMaxNodes);
 constexpr size_t kOffPxy = up256(kOffPm + 8ull * (kMaxBodies + 1));
 constexpr size_t kOffLookback =
     up256(kOffPxy + 2ull * sizeof(__int128) * (kMaxBodies + 1));
@@ -56,15 +57,27 @@ constexpr size_t kOffWarp =
     up256(kOffLookback + sizeof(LookbackSums) * tiles_of(kMaxBodies, kCountTile));
 constexpr size_t kOffBBox = up256(kOffWarp + 8ull * ((kMaxBodies + 31) / 32));
 constexpr size_t kScratchBytes = up256(kOffBBox + 16ull * 4 * kMaxSMs);
-static_assert(kScratchBytes < (6u << 20), "the static scratch is meant to stay near 5 MB");
+static_assert(kScratchBytes < (7u << 20), "the static scratch is meant to stay near 6 MB");
 
 // The scratch: one per device, in the library's device image.  Static device
 // memory starts zeroed when the module is loaded.
 __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
-__global__ void k_identity(uint32_t n, uint32_t *__restrict out) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        out[i] = i;
+// Error bit of this entry point: a mass that is not a whole number in
+// [0, 2^24).  The tree sums masses as exact integers, which FA2's masses
+// (degree + 1) always are.
+constexpr int kErrMass = 1 << 8;
+
+// Reference ids (the caller's indices) and the mass check.
+__global__ void k_prepare(uint32_t n, const float *__restrict mass, uint32_t *__restrict ids,
+                          DevState *st) {
+    bool bad = false;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        ids[i] = i;
+        const float m = mass[i];
+        bad |= !(m >= 0.0f && m < 16777216.0f && m == truncf(m));
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&st->err, kErrMass);
 }
 
 struct DeviceSetup {
@@ -124,6 +137,7 @@ int run(const float *d_xy, const float *d_mass, uint32_t n, const fa2_params *pr
     b.group = reinterpret_cast<uint32_t *>(base + kOffGroup);
     b.body_node = reinterpret_cast<uint32_t *>(base + kOffBodyNode);
     b.nodes = reinterpret_cast<float4 *>(base + kOffNodes);
+    b.owner = reinterpret_cast<uint32_t *>(base + kOffOwner);
     b.capacity = (uint32_t)kMaxNodes;
     b.pm = reinterpret_cast<long long *>(base + kOffPm);
     b.pxy = reinterpret_cast<__int128 *>(base + kOffPxy);
@@ -153,7 +167,7 @@ int run(const float *d_xy, const float *d_mass, uint32_t n, const fa2_params *pr
     cudaMemsetAsync(b.ctr, 0, zero_bytes, s);
     cudaMemsetAsync(b.st, 0, sizeof(DevState), s);
     cudaMemsetAsync(b.fag, 0, (size_t)n * sizeof(float2), s);
-    k_identity<<<(n + 255) / 256, 256, 0, s>>>(n, const_cast<uint32_t *>(b.ref_of));
+    k_prepare<<<(n + 255) / 256, 256, 0, s>>>(n, d_mass, const_cast<uint32_t *>(b.ref_of), b.st);
     launch_bbox(b, d.nsm * 2, s);
     launch_keys(b, d.nsm, s);
     launch_sort(b, s);
@@ -168,6 +182,7 @@ int run(const float *d_xy, const float *d_mass, uint32_t n, const fa2_params *pr
     e = cudaMemcpyAsync(flags, &b.st->poison, sizeof(flags), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return status_of(e);
+    if (flags[1] & kErrMass) return FA2_ERR_INVALID_ARGUMENT;
     if (flags[1]) return FA2_ERR_DEVICE_LIMIT;
     if (flags[0]) return FA2_ERR_INVALID_ARGUMENT;  // coincident bodies
     return FA2_OK;

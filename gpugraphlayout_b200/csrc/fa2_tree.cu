@@ -14,10 +14,12 @@
 //                 same pass, exact prefix sums of mass and mass x position
 //                 (integers: mass is degree + 1; positions in 2^-48 steps of
 //                 the root radius; 128-bit sums), so any cell's mass and centre
-//                 of mass are two prefix differences.  It also orders runs of
+//                 of mass are two prefix differences.  Each node's owner (the
+//                 body that starts it) is recorded.  It also orders runs of
 //                 equal 64-bit keys (trees deeper than 32 levels) and flags
 //                 exactly coincident bodies.
-//   k_emit        writes every node once: bodies from their positions; cells
+//   k_emit        writes every node once, one thread per node: bodies from
+//                 their positions; cells
 //                 with level, mass, centre of mass (prefix differences over
 //                 the cell's body range) and the index of the node after their
 //                 subtree.  No parent links, atomics or fences are needed.
@@ -143,6 +145,14 @@ __device__ __forceinline__ i128 shfl_up_i128(i128 v, int o) {
     return ((i128)hi2 << 64) | (i128)lo2;
 }
 
+__device__ __forceinline__ i128 shfl_xor_i128(i128 v, int o) {
+    const unsigned long long lo = (unsigned long long)v;
+    const long long hi = (long long)(v >> 64);
+    const unsigned long long lo2 = __shfl_xor_sync(kFull, lo, o);
+    const long long hi2 = __shfl_xor_sync(kFull, hi, o);
+    return ((i128)hi2 << 64) | (i128)lo2;
+}
+
 // 128-bit load that bypasses L1 (the value was written by another block)
 __device__ __forceinline__ i128 ldcg_i128(const i128 *p) {
     const longlong2 v = __ldcg(reinterpret_cast<const longlong2 *>(p));
@@ -181,7 +191,8 @@ __device__ __forceinline__ void sums_add(NodeSums &a, const NodeSums &b) {
 
 __global__ void __launch_bounds__(kCountThreads) k_tree_count(
     int n, const uint64_t *__restrict keys, int8_t *__restrict lcp, uint32_t *__restrict group,
-    uint32_t capacity, DevState *st, IterCounters *ctr, uint32_t *status,
+    uint32_t *__restrict owner, uint32_t capacity, DevState *st, IterCounters *ctr,
+    uint32_t *status,
     LookbackSums *__restrict lb, uint32_t *__restrict vals, float2 *__restrict pos,
     const float *__restrict mass, const uint32_t *__restrict ref_of,
     long long *__restrict pm, i128 *__restrict pxy) {
@@ -236,62 +247,92 @@ __global__ void __launch_bounds__(kCountThreads) k_tree_count(
     }
     if (lane == 31) s_warp[wid] = inc;
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (wid == 0) {
         NodeSums run{0, 0, 0, 0};
-        for (int w = 0; w < kCountThreads / kWarp; ++w) {
-            const NodeSums t = s_warp[w];
-            s_warp[w] = run;
-            sums_add(run, t);
+        if (lane == 0) {
+            for (int w = 0; w < kCountThreads / kWarp; ++w) {
+                const NodeSums t = s_warp[w];
+                s_warp[w] = run;
+                sums_add(run, t);
+            }
         }
-        // decoupled look-back over tiles: the flag word holds the node count,
-        // the mass sums sit beside it and are written before the flag
+        // Decoupled look-back over tiles: the flag word holds the node count,
+        // the mass sums sit beside it and are written before the flag.  The
+        // whole warp looks back: lane j reads the flag of tile (hi - j), so
+        // one round trip covers 32 earlier tiles.  The tiles needed are those
+        // from the nearest one with an inclusive prefix up to this one.
         const uint32_t kAgg = 1u << 30, kPre = 2u << 30, kMask = (1u << 30) - 1;
         NodeSums prefix{0, 0, 0, 0};
         if (tile == 0) {
-            lb[0].incl_m = run.m;
-            lb[0].incl_x = run.x;
-            lb[0].incl_y = run.y;
-            __threadfence();
-            atomicExch(&status[0], kPre | run.g);
+            if (lane == 0) {
+                lb[0].incl_m = run.m;
+                lb[0].incl_x = run.x;
+                lb[0].incl_y = run.y;
+                __threadfence();
+                atomicExch(&status[0], kPre | run.g);
+            }
         } else {
-            lb[tile].agg_m = run.m;
-            lb[tile].agg_x = run.x;
-            lb[tile].agg_y = run.y;
-            __threadfence();
-            atomicExch(&status[tile], kAgg | run.g);
-            int t = tile - 1;
+            if (lane == 0) {
+                lb[tile].agg_m = run.m;
+                lb[tile].agg_x = run.x;
+                lb[tile].agg_y = run.y;
+                __threadfence();
+                atomicExch(&status[tile], kAgg | run.g);
+            }
+            int hi = tile - 1;
             long spins = 0;
-            while (t >= 0) {
-                const uint32_t s = *((volatile uint32_t *)&status[t]);
-                if ((s >> 30) == 0) {
+            for (;;) {
+                const int t = hi - lane;
+                // tile 0 always ends with an inclusive prefix, so a lane past
+                // it is never needed
+                const uint32_t s = t >= 0 ? *((volatile uint32_t *)&status[t]) : kPre;
+                const unsigned pre = __ballot_sync(kFull, (s >> 30) == 2);
+                const unsigned zero = __ballot_sync(kFull, (s >> 30) == 0);
+                const int first = pre ? __ffs(pre) - 1 : 31;
+                const unsigned need = first == 31 ? kFull : ((2u << first) - 1u);
+                if (zero & need) {
                     if (++spins > (1L << 22)) {
-                        atomicOr(&st->err, kErrScanWait);
+                        if (lane == 0) atomicOr(&st->err, kErrScanWait);
                         break;
                     }
                     continue;
                 }
                 __threadfence();
-                prefix.g += s & kMask;
-                if ((s >> 30) == 2) {
-                    prefix.m += __ldcg(&lb[t].incl_m);
-                    prefix.x += ldcg_i128(&lb[t].incl_x);
-                    prefix.y += ldcg_i128(&lb[t].incl_y);
-                    break;
+                NodeSums v{0, 0, 0, 0};
+                if (((need >> lane) & 1u) && t >= 0) {
+                    v.g = s & kMask;
+                    if ((s >> 30) == 2) {
+                        v.m = __ldcg(&lb[t].incl_m);
+                        v.x = ldcg_i128(&lb[t].incl_x);
+                        v.y = ldcg_i128(&lb[t].incl_y);
+                    } else {
+                        v.m = __ldcg(&lb[t].agg_m);
+                        v.x = ldcg_i128(&lb[t].agg_x);
+                        v.y = ldcg_i128(&lb[t].agg_y);
+                    }
                 }
-                prefix.m += __ldcg(&lb[t].agg_m);
-                prefix.x += ldcg_i128(&lb[t].agg_x);
-                prefix.y += ldcg_i128(&lb[t].agg_y);
-                --t;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    v.g += __shfl_xor_sync(kFull, v.g, o);
+                    v.m += __shfl_xor_sync(kFull, v.m, o);
+                    v.x += shfl_xor_i128(v.x, o);
+                    v.y += shfl_xor_i128(v.y, o);
+                }
+                sums_add(prefix, v);
+                if (pre) break;
+                hi -= 32;
             }
-            NodeSums incl = prefix;
-            sums_add(incl, run);
-            lb[tile].incl_m = incl.m;
-            lb[tile].incl_x = incl.x;
-            lb[tile].incl_y = incl.y;
-            __threadfence();
-            atomicExch(&status[tile], kPre | incl.g);
+            if (lane == 0) {
+                NodeSums incl = prefix;
+                sums_add(incl, run);
+                lb[tile].incl_m = incl.m;
+                lb[tile].incl_x = incl.x;
+                lb[tile].incl_y = incl.y;
+                __threadfence();
+                atomicExch(&status[tile], kPre | incl.g);
+            }
         }
-        s_prefix = prefix;
+        if (lane == 0) s_prefix = prefix;
     }
     __syncthreads();
     NodeSums off = s_prefix;
@@ -309,6 +350,12 @@ __global__ void __launch_bounds__(kCountThreads) k_tree_count(
             pm[k] = off.m;
             pxy[2 * (size_t)k] = off.x;
             pxy[2 * (size_t)k + 1] = off.y;
+            // the owner of each node body k starts: its cells, then itself
+            const uint32_t c = (uint32_t)g[e] - 1u;
+            for (uint32_t q = 0; q <= c; ++q) {
+                const uint32_t idx = off.g + q;
+                if (idx < capacity) owner[idx] = ((uint32_t)k << 6) | (q < c ? q : 63u);
+            }
         }
         off.g += (uint32_t)g[e];
         off.m += im[e];
@@ -384,10 +431,16 @@ __device__ int find_end(const uint64_t *__restrict keys, const int8_t *__restric
     return lo;
 }
 
+// One thread per tree node (grid-stride over the preorder index): a body
+// writes its own record; a cell finds its last body, then forms its mass and
+// centre of mass from the prefix sums at its two ends.  Node-parallel, so the
+// body that starts many nested cells (body 0 starts one per level) spreads
+// their searches over many threads.
 __global__ void __launch_bounds__(256) k_emit(int n, const uint64_t *__restrict keys,
                                               const uint32_t *__restrict vals,
                                               const int8_t *__restrict lcp,
                                               const uint32_t *__restrict group,
+                                              const uint32_t *__restrict owner,
                                               const float2 *__restrict pos,
                                               const float *__restrict mass,
                                               const long long *__restrict pm,
@@ -395,36 +448,31 @@ __global__ void __launch_bounds__(256) k_emit(int n, const uint64_t *__restrict 
                                               float4 *__restrict nodes,
                                               uint32_t *__restrict body_node, DevState *st) {
     if (st->err || st->poison) return;
+    const uint32_t total = st->tree_nodes;
     const double inv_scale = st->radius > 0.0f ? (double)st->radius / kFixedScale : 1.0;
     const double rx = st->rootx, ry = st->rooty;
     int local_max = 0;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const int Lk = load_lcp(lcp, n, k), Lkm1 = load_lcp(lcp, n, k - 1);
-        const int c = cells_at(k, Lk, Lkm1);
-        const uint32_t Gk = group[k];
-        const uint32_t bnode = Gk + (uint32_t)c;
-        // the body
-        const uint32_t i = vals[k];
-        const float2 p = pos[i];
-        nodes[bnode] = make_float4(p.x, p.y, mass[i], make_meta(bnode + 1, kBodyLevel));
-        body_node[k] = bnode;
-        if (c == 0) continue;
-        // the cells that start here, outermost first: levels lo .. lo + c - 1
-        const int lo_level = k == 0 ? 0 : Lkm1 + 1;
-        const long long m0 = pm[k];
-        const i128 x0 = pxy[2 * (size_t)k], y0 = pxy[2 * (size_t)k + 1];
-        for (int q = 0; q < c; ++q) {
-            const int lvl = lo_level + q;
-            const int b = lvl == 0 ? n - 1 : find_end(keys, lcp, n, k, lvl);
-            const uint32_t next = body_index(lcp, group, n, b) + 1;
-            const double cm = (double)(pm[b + 1] - m0);
-            const double sx = i128_to_double(pxy[2 * (size_t)(b + 1)] - x0);
-            const double sy = i128_to_double(pxy[2 * (size_t)(b + 1) + 1] - y0);
-            nodes[Gk + (uint32_t)q] =
-                make_float4((float)(rx + sx / cm * inv_scale), (float)(ry + sy / cm * inv_scale),
-                            (float)cm, make_meta(next, lvl));
-            local_max = max(local_max, lvl);
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total;
+         g += gridDim.x * blockDim.x) {
+        const uint32_t w = owner[g];
+        const int k = (int)(w >> 6), q = (int)(w & 63u);
+        if (q == 63) {
+            const uint32_t i = vals[k];
+            const float2 p = pos[i];
+            nodes[g] = make_float4(p.x, p.y, mass[i], make_meta(g + 1, kBodyLevel));
+            body_node[k] = g;
+            continue;
         }
+        // the cells that start at body k have levels lo .. lo + c - 1
+        const int lvl = (k == 0 ? 0 : load_lcp(lcp, n, k - 1) + 1) + q;
+        const int b = lvl == 0 ? n - 1 : find_end(keys, lcp, n, k, lvl);
+        const uint32_t next = body_index(lcp, group, n, b) + 1;
+        const double cm = (double)(pm[b + 1] - pm[k]);
+        const double sx = i128_to_double(pxy[2 * (size_t)(b + 1)] - pxy[2 * (size_t)k]);
+        const double sy = i128_to_double(pxy[2 * (size_t)(b + 1) + 1] - pxy[2 * (size_t)k + 1]);
+        nodes[g] = make_float4((float)(rx + sx / cm * inv_scale), (float)(ry + sy / cm * inv_scale),
+                               (float)cm, make_meta(next, lvl));
+        local_max = max(local_max, lvl);
     }
     local_max = __reduce_max_sync(kFull, local_max);
     if ((threadIdx.x & 31) == 0 && local_max > 0) atomicMax(&st->max_level, local_max);
@@ -444,13 +492,14 @@ void launch_runs(const Buffers &b, int perturb, int nsm, cudaStream_t s) {
 
 void launch_tree_count(const Buffers &b, cudaStream_t s) {
     k_tree_count<<<count_tiles(b.n), kCountThreads, 0, s>>>(
-        b.n, b.keys[0], b.lcp, b.group, b.capacity, b.st, b.ctr, b.count_status, b.lookback,
+        b.n, b.keys[0], b.lcp, b.group, b.owner, b.capacity, b.st, b.ctr, b.count_status,
+        b.lookback,
         b.vals[0], b.pos, b.mass, b.ref_of, b.pm, reinterpret_cast<i128 *>(b.pxy));
 }
 
 void launch_emit(const Buffers &b, int nsm, cudaStream_t s) {
     k_emit<<<grid_for(b.n, 256, nsm * 8), 256, 0, s>>>(
-        b.n, b.keys[0], b.vals[0], b.lcp, b.group, b.pos, b.mass, b.pm,
+        b.n, b.keys[0], b.vals[0], b.lcp, b.group, b.owner, b.pos, b.mass, b.pm,
         reinterpret_cast<const i128 *>(b.pxy), b.nodes, b.body_node, b.st);
 }
 

@@ -163,7 +163,7 @@ int fa2_set_force_params(fa2_ctx *ctx, float scale, float gravity);
  * fixed device-memory budget, or inside a host framework whose caching
  * allocator it may not touch, or a process that reserved the device's memory
  * up front.  No call allocates device or host memory.  All scratch lives in
- * one fixed array in the library's device memory, about 5 MB per device,
+ * one fixed array in the library's device memory, about 6 MB per device,
  * held from the time the library's kernels are loaded on that device.
  *
  *  - n > FA2_NOALLOC_MAX_BODIES returns FA2_ERR_TOO_LARGE before any work.
@@ -173,9 +173,10 @@ int fa2_set_force_params(fa2_ctx *ctx, float scale, float gravity);
  *    any stream capture.
  *  - The work is enqueued on `stream` (a cudaStream_t; NULL is the default
  *    stream) and the call waits for that stream before it returns, then
- *    reports: coincident bodies -> FA2_ERR_INVALID_ARGUMENT (fa2_step would
- *    move them apart; this call does not), a device-side bound ->
- *    FA2_ERR_DEVICE_LIMIT.
+ *    reports: coincident bodies, or a mass that is not a whole number in
+ *    [0, 2^24) -> FA2_ERR_INVALID_ARGUMENT (fa2_step moves coincident bodies
+ *    apart, and its masses are degree + 1; this call does neither), a
+ *    device-side bound -> FA2_ERR_DEVICE_LIMIT.
  *  - There is one scratch array per device: calls that overlap on the same
  *    device (several host threads, or several streams) race on it and give
  *    wrong forces.  Serialise them.

@@ -76,3 +76,24 @@ def test_noalloc_rejects_more_bodies_than_its_scratch_holds():
     out = torch.full((n, 2), 7.0, dtype=torch.float32, device="cuda")
     assert _noalloc(xy, mass, out, _params(1.0)) == 6  # FA2_ERR_TOO_LARGE
     assert bool((out == 7.0).all())  # nothing ran
+
+
+def test_noalloc_reports_inputs_it_does_not_handle():
+    """Coincident bodies (fa2_step would move them apart) and masses that are
+    not whole numbers below 2^24 (fa2_step's are degree + 1) are refused with
+    FA2_ERR_INVALID_ARGUMENT; the next call works again."""
+    import torch
+    from oracle import oracle as O
+    n = 500
+    xy = O.random_positions(n, 100, 100, 3)
+    mass = torch.ones(n, dtype=torch.float32, device="cuda")
+    out = torch.empty((n, 2), dtype=torch.float32, device="cuda")
+    prm = _params(1.0)
+    same = xy.copy()
+    same[7] = same[3]
+    assert _noalloc(torch.from_numpy(same).cuda(), mass, out, prm) == 1
+    frac = mass.clone()
+    frac[11] = 1.5
+    assert _noalloc(torch.from_numpy(xy).cuda(), frac, out, prm) == 1
+    assert _noalloc(torch.from_numpy(xy).cuda(), mass, out, prm) == 0
+    assert bool(torch.isfinite(out).all())
