@@ -249,6 +249,15 @@ def run_ours(args, world, rank, local):
                 "unit": "GB/s", "frac": att_gbs / hbm, "traffic": None,
                 "note": f"peak = {pk_kind} HBM copy bandwidth; dominant kernel by time is "
                         f"'{dom}' ({kms.get(dom, 0.0):.3f} ms/launch)"}
+    # The walk is bound by instruction issue and dependent-load latency, not by
+    # HBM or tensor cores: its work is 10 FP32 operations per interaction,
+    # reported against the nominal FP32 rate of the SMs.
+    fp32_peak = 148 * 128 * 2 * float(pk.get("sm_max_mhz", 1965.0)) * 1e6 / 1e12
+    trav_tflops = 10.0 * inter / (trav_ms * 1e-3) / 1e12 if trav_ms else 0.0
+    roofline_traverse = {"kernel": "traverse", "bound": "fp32 issue / load latency",
+                         "achieved": trav_tflops, "peak": fp32_peak, "unit": "TFLOP/s",
+                         "frac": trav_tflops / fp32_peak, "flop_per_interaction": 10,
+                         "note": "peak = nominal FP32 (148 SMs x 128 lanes x 2 x max SM clock)"}
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": ms_max / args.steps,
@@ -259,6 +268,7 @@ def run_ours(args, world, rank, local):
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * n,
                 "d2h_bytes_per_step": 8 * n},
         "roofline": roofline,
+        "roofline_traverse": roofline_traverse,
         "kernels": kernels,
         "tree": {"nodes": st["tree_nodes"], "cells": st["tree_cells"],
                  "max_level": st["max_level"]},

@@ -213,7 +213,7 @@ int capture(fa2_ctx *c, bool timed, cudaGraphExec_t *out) {
     enqueue_iteration(c, true, false, timed);
     cudaError_t e = cudaStreamEndCapture(c->sA, &graph);
     if (e != cudaSuccess) return cuda_status(e);
-    e = cudaGraphInstantiate(out, graph, 0);
+    e = cudaGraphInstantiate(out, graph, cudaGraphInstantiateFlagUseNodePriority);
     if (e == cudaSuccess && timed) {
         size_t nn = 0;
         cudaGraphGetNodes(graph, nullptr, &nn);
@@ -425,7 +425,8 @@ fa2_ctx *fa2_create(const fa2_graph_desc *g, const fa2_params *prm, int *status)
     b.ref_of = d_ref;
     // one memset clears counters, histograms, per-tile digit counts and the
     // tree-count look-back flags
-    const size_t sort_counts = (size_t)8 * sort_tiles((int)n) * 256;
+    b.sort_rounds = sort_rounds((int)n, c->nsm);
+    const size_t sort_counts = (size_t)8 * sort_tiles_max((int)n) * 256;
     const size_t count_status = (size_t)count_tiles((int)n);
     c->scratch_bytes = sizeof(IterCounters) + 4 * (sort_counts + count_status);
     char *scr = nullptr;
@@ -435,8 +436,14 @@ fa2_ctx *fa2_create(const fa2_graph_desc *g, const fa2_params *prm, int *status)
     b.sort_counts = (uint32_t *)(scr + sizeof(IterCounters));
     b.count_status = b.sort_counts + sort_counts;
 
-    if (cudaStreamCreateWithFlags(&c->sA, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&c->sB, cudaStreamNonBlocking) != cudaSuccess ||
+    // The tree chain (stream A) is the critical path; the attraction (stream B)
+    // only has to finish before the traversal.  With A at the higher priority
+    // the block scheduler starts A's blocks first and fills the rest of the
+    // SMs with attraction blocks, instead of holding the chain behind them.
+    int prio_low = 0, prio_high = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+    if (cudaStreamCreateWithPriority(&c->sA, cudaStreamNonBlocking, prio_high) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&c->sB, cudaStreamNonBlocking, prio_low) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->evFork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->evJoin, cudaEventDisableTiming) != cudaSuccess)
         return fail(FA2_ERR_CUDA);
@@ -540,6 +547,10 @@ int fa2_get_stats(fa2_ctx *c, fa2_stats *out) {
     DevState st;
     memset(&st, 0, sizeof(st));
     if (c->n) {
+        // interaction and visit counts: one counting walk over the last tree
+        CK(cudaMemsetAsync(&c->b.st->interactions, 0, 2 * sizeof(unsigned long long), c->sA));
+        launch_count_interactions(c->b, c->kp, c->trav_blocks, c->sA);
+        CK(cudaGetLastError());
         int s = read_state(c, &st);
         if (s) return s;
     }

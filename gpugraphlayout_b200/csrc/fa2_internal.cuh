@@ -16,7 +16,8 @@ namespace fa2 {
 
 constexpr int kWarp = 32;
 constexpr int kLevels = 32;        // quadrant digits in a 64-bit Morton key
-constexpr int kBodyLevel = 63;     // level code of a body (leaf) node
+constexpr int kBodyLevel = 32;     // level code of a body (leaf) node; it shares the walk's
+                                   // always-accept threshold with level-32 cells
 constexpr int kMetaShift = 6;      // node meta = next_index << 6 | level code
 constexpr uint32_t kMaxTreeNodes = 1u << 26;
 constexpr int kMaxRun = 1024;      // longest run of equal 64-bit keys handled
@@ -43,6 +44,7 @@ struct DevState {
     float swg_sum, etra_sum;
     unsigned long long interactions;  // body-node force terms of the last traversal
     unsigned long long visits;        // body-node acceptance tests of the last traversal
+    float trav_radius;                // root radius the last traversal used
 };
 
 // Per-iteration scratch, cleared by one memset at the start of an iteration.
@@ -57,16 +59,30 @@ struct IterCounters {
     unsigned hist[8][256];  // per-pass digit histograms of the sort keys
 };
 
-// Sort geometry (one tile per block).
+// Sort geometry: one tile per block, kSortThreads threads holding `rounds`
+// keys each.  The rounds (4, 5 or 6) are chosen per context so that, where
+// possible, every tile gets an SM of its own (see sort_rounds).
 constexpr int kSortThreads = 1024;
 constexpr int kSortWarps = kSortThreads / kWarp;
-constexpr int kSortRounds = 4;
-constexpr int kSortTile = kSortThreads * kSortRounds;  // 4096 keys
+constexpr int kSortMinRounds = 4;
+constexpr int kSortMaxRounds = 6;
+constexpr int kSortTileMin = kSortThreads * kSortMinRounds;  // 4096 keys
 constexpr int kCountThreads = 256;
 constexpr int kCountItems = 4;
 constexpr int kCountTile = kCountThreads * kCountItems;  // 1024 bodies
 
-inline int sort_tiles(int n) { return (n + kSortTile - 1) / kSortTile; }
+inline int sort_tiles(int n, int rounds) {
+    const int tile = kSortThreads * rounds;
+    return (n + tile - 1) / tile;
+}
+// Upper bound on the tiles of any rounds choice (for sizing buffers).
+inline int sort_tiles_max(int n) { return sort_tiles(n, kSortMinRounds); }
+// The fewest rounds that give no more tiles than SMs; past that, the minimum.
+inline int sort_rounds(int n, int nsm) {
+    for (int r = kSortMinRounds; r <= kSortMaxRounds; ++r)
+        if (sort_tiles(n, r) <= nsm) return r;
+    return kSortMinRounds;
+}
 inline int count_tiles(int n) { return (n + kCountTile - 1) / kCountTile; }
 
 // Attraction work split: rows (nodes in degree-descending order) with the
@@ -117,6 +133,7 @@ struct Buffers {
     float2 *warp_partial;     // one per 32 sorted bodies
     DevState *st;
     IterCounters *ctr;
+    int sort_rounds;          // keys per sort thread (tile = kSortThreads x rounds)
     uint32_t *sort_counts;    // [8][sort tiles][256]: digit counts per tile and pass
     uint32_t *count_status;   // [count tiles]
 };
@@ -140,6 +157,7 @@ void launch_tree_count(const Buffers &b, cudaStream_t s);
 void launch_emit(const Buffers &b, int nsm, cudaStream_t s);
 void launch_traverse(const Buffers &b, const Params &p, int nblocks, cudaStream_t s);
 void launch_displace(const Buffers &b, int nsm, cudaStream_t s);
+void launch_count_interactions(const Buffers &b, const Params &p, int nblocks, cudaStream_t s);
 void launch_attract(const Buffers &b, const Params &p, const AttractPlan &plan, cudaStream_t s);
 void launch_scatter_xy(int n, const uint32_t *ref_of, const float2 *src_ref, float2 *dst_int,
                        cudaStream_t s);

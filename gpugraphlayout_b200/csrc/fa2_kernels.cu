@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(kBBoxThreads) k_bbox(int n, const float2 *__re
 // One block per sort tile: the tile's keys, the digit-0 counts of the tile
 // (the first sort pass's per-tile input) and the tile's share of the digit
 // histograms of all eight passes (order-independent, so counted once here).
-__global__ void __launch_bounds__(1024) k_keys(int n, const float2 *__restrict pos,
+__global__ void __launch_bounds__(1024) k_keys(int n, int tile, const float2 *__restrict pos,
                                               const DevState *__restrict st,
                                               uint64_t *__restrict keys, uint32_t *__restrict vals,
                                               IterCounters *ctr, uint32_t *__restrict counts0) {
@@ -131,8 +131,8 @@ __global__ void __launch_bounds__(1024) k_keys(int n, const float2 *__restrict p
     for (int j = threadIdx.x; j < 8 * 256; j += blockDim.x) (&s_hist[0][0])[j] = 0;
     __syncthreads();
     const float rx = st->rootx, ry = st->rooty, rr = st->radius;
-    const int tile0 = blockIdx.x * kSortTile;
-    const int tile_end = min(n, tile0 + kSortTile);
+    const int tile0 = blockIdx.x * tile;
+    const int tile_end = min(n, tile0 + tile);
     for (int i = tile0 + threadIdx.x; i < tile_end; i += blockDim.x) {
         float2 p = pos[i];
         uint64_t key = morton_key(p.x, p.y, rx, ry, rr);
@@ -180,11 +180,18 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
             dq = dq * 0.25f;
         }
         for (int l = kLevels + 1; l < 64; ++l) s_dq[l] = 0.0f;
+        if (blockIdx.x == 0) st->trav_radius = st->radius;
     }
     __syncthreads();
     const uint32_t end = st->tree_nodes;
     const int lane = threadIdx.x & 31;
     const int nwarps = (n + 31) >> 5;
+    // Cell thresholds live one per lane: a node's level code, the low bits of
+    // its meta word, is the lane a shuffle reads its threshold from.  Lane 0
+    // holds 0, the threshold of bodies (always used) and of level-32 cells:
+    // there dq[32] is (2 radius / 2^32)^2 + eps, which float rounds to eps for
+    // any root radius below ~2e4, and d^2 + eps >= eps always holds.
+    const float lane_dq = lane == 0 ? 0.0f : s_dq[lane];
     // Groups of 32 bodies are handed out one at a time from a global ticket:
     // the work per group varies with the local density of the layout, and
     // warps that take consecutive tickets walk neighbouring bodies, so the
@@ -200,28 +207,30 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
         // a lane without a body sits far away: it passes every test and its
         // (unused) sums never feed anything
         const float px = active ? me.x : 1e30f, py = active ? me.y : 1e30f;
-        const float kmi = prm.k_r * me.z;
+        // sum of m_j d / (d^2 + eps) over the accepted nodes; the body's own
+        // k_r m_i multiplies the sum once at the end
         float ax = 0.0f, ay = 0.0f;
-        uint32_t node = 1, n_acc = 0;
-        while (node < end) {
+        // The walk ends past the sentinel node at index end, whose NaN
+        // position fails every lane's test: it is opened like a cell, and only
+        // an opening step needs the end test.
+        uint32_t node = 1;
+        for (;;) {
             const float4 r = __ldg(&nodes[node]);
             const int meta = __float_as_int(r.w);
             const float dx = px - r.x, dy = py - r.y;
             const float d2 = dx * dx + dy * dy + prm.epssq;
-            if (__all_sync(kFull, d2 >= s_dq[meta_level(meta)])) {
-                const float c = __fdividef(kmi * r.z, d2);
+            if (__all_sync(kFull, d2 >= __shfl_sync(kFull, lane_dq, meta))) {
+                const float c = __fdividef(r.z, d2);
                 ax = fmaf(dx, c, ax);
                 ay = fmaf(dy, c, ay);
                 node = meta_next(meta);
-                ++n_acc;
-            } else {
-                ++node;
+            } else if (++node > end) {
+                break;
             }
         }
-        if (lane == 0) {
-            const unsigned lanes = (unsigned)min(32, n - w * 32);
-            atomicAdd(&st->interactions, (unsigned long long)n_acc * lanes);
-        }
+        const float kmi = prm.k_r * me.z;
+        ax *= kmi;
+        ay *= kmi;
         float sw = 0.0f, tr = 0.0f;
         if (active) {
             const uint32_t i = vals[k];
@@ -296,6 +305,60 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
         gs += fminf(targetSpeed - gs, max_rise * gs);
         st->speed_efficiency = se;
         st->global_speed = gs;
+    }
+}
+
+// The walk of k_traverse without the force arithmetic, over the tree still in
+// the node array (the last step's), with the root radius that step used:
+// counts its body-node interactions and acceptance tests.  Diagnostics only;
+// the stepping path does not launch it.
+__global__ void __launch_bounds__(kTravThreads) k_count_interactions(
+    int n, const float4 *__restrict nodes, const uint32_t *__restrict body_node, DevState *st,
+    Params prm) {
+    __shared__ float s_dq[64];
+    // no tree yet, or the last step stopped before its tree was complete
+    if (st->err || st->poison || st->tree_nodes == 0) return;
+    if (threadIdx.x == 0) {
+        float tmp = st->trav_radius * 2;
+        float dq = tmp * tmp * prm.itolsq;
+        s_dq[0] = 0.0f;
+        for (int l = 1; l <= kLevels; ++l) {
+            s_dq[l] = dq + prm.epssq;
+            dq = dq * 0.25f;
+        }
+        for (int l = kLevels + 1; l < 64; ++l) s_dq[l] = 0.0f;
+    }
+    __syncthreads();
+    const uint32_t end = st->tree_nodes;
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (n + 31) >> 5;
+    const int stride = (int)(gridDim.x * blockDim.x) >> 5;
+    const float lane_dq = lane == 0 ? 0.0f : s_dq[lane];  // as in k_traverse
+    for (int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); w < nwarps; w += stride) {
+        const int k = w * 32 + lane;
+        const bool active = k < n;
+        const float4 me = nodes[body_node[active ? k : n - 1]];
+        const float px = active ? me.x : 1e30f, py = active ? me.y : 1e30f;
+        unsigned long long acc = 0, steps = 0;
+        uint32_t node = 1;
+        while (node < end) {
+            const float4 r = nodes[node];
+            const int meta = __float_as_int(r.w);
+            const float dx = px - r.x, dy = py - r.y;
+            const float d2 = dx * dx + dy * dy + prm.epssq;
+            ++steps;
+            if (__all_sync(kFull, d2 >= __shfl_sync(kFull, lane_dq, meta))) {
+                ++acc;
+                node = meta_next(meta);
+            } else {
+                ++node;
+            }
+        }
+        if (lane == 0) {
+            const unsigned long long lanes = (unsigned long long)min(32, n - w * 32);
+            atomicAdd(&st->interactions, acc * lanes);
+            atomicAdd(&st->visits, steps * lanes);
+        }
     }
 }
 
@@ -514,8 +577,9 @@ void launch_bbox(const Buffers &b, int nblocks, cudaStream_t s) {
 
 void launch_keys(const Buffers &b, int nsm, cudaStream_t s) {
     (void)nsm;
-    k_keys<<<sort_tiles(b.n), 1024, 0, s>>>(b.n, b.pos, b.st, b.keys[0], b.vals[0], b.ctr,
-                                           b.sort_counts);
+    k_keys<<<sort_tiles(b.n, b.sort_rounds), 1024, 0, s>>>(
+        b.n, kSortThreads * b.sort_rounds, b.pos, b.st, b.keys[0], b.vals[0], b.ctr,
+        b.sort_counts);
 }
 
 
@@ -530,6 +594,10 @@ void launch_traverse(const Buffers &b, const Params &p, int nblocks, cudaStream_
 void launch_displace(const Buffers &b, int nsm, cudaStream_t s) {
     k_displace<<<grid_for(b.n, kDispThreads, nsm * 4), kDispThreads, 0, s>>>(
         b.n, b.pos, b.f, b.fprev, b.bbox_partial, b.st, b.ctr);
+}
+
+void launch_count_interactions(const Buffers &b, const Params &p, int nblocks, cudaStream_t s) {
+    k_count_interactions<<<nblocks, kTravThreads, 0, s>>>(b.n, b.nodes, b.body_node, b.st, p);
 }
 
 void launch_attract(const Buffers &b, const Params &p, const AttractPlan &plan, cudaStream_t s) {

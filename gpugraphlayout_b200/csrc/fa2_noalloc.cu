@@ -33,7 +33,7 @@ constexpr int tiles_of(uint32_t n, int tile) { return (int)((n + tile - 1) / til
 // Byte offsets of the sub-buffers inside the static array, each on a
 // 256-byte boundary.  The first region is the one cleared on every call.
 constexpr size_t kZeroBytes = sizeof(IterCounters) +
-                              4 * ((size_t)8 * tiles_of(kMaxBodies, kSortTile) * 256 +
+                              4 * ((size_t)8 * tiles_of(kMaxBodies, kSortTileMin) * 256 +
                                    (size_t)tiles_of(kMaxBodies, kCountTile));
 constexpr size_t kOffZero = 0;
 constexpr size_t kOffSt = up256(kOffZero + kZeroBytes);
@@ -146,7 +146,8 @@ int run(const float *d_xy, const float *d_mass, uint32_t n, const fa2_params *pr
     b.bbox_partial = reinterpret_cast<float4 *>(base + kOffBBox);
     b.st = reinterpret_cast<DevState *>(base + kOffSt);
     b.ctr = reinterpret_cast<IterCounters *>(base + kOffZero);
-    const size_t sort_counts = (size_t)8 * sort_tiles((int)n) * 256;
+    b.sort_rounds = sort_rounds((int)n, d.nsm);
+    const size_t sort_counts = (size_t)8 * sort_tiles(b.n, b.sort_rounds) * 256;
     b.sort_counts = reinterpret_cast<uint32_t *>(base + kOffZero + sizeof(IterCounters));
     b.count_status = b.sort_counts + sort_counts;
     const size_t zero_bytes = sizeof(IterCounters) + 4 * (sort_counts + count_tiles((int)n));

@@ -1,19 +1,22 @@
 // fa2_sort.cu -- stable LSD radix sort of (64-bit Morton key, 32-bit node id)
 // pairs, 8 passes of 8-bit digits, one kernel per pass, no inter-block waits.
 //
-// The keys are cut into fixed tiles of kSortTile.  For pass p every tile
-// needs, per digit, how many keys with that digit lie in the tiles before it.
-// Those per-tile counts are produced one pass ahead: k_keys counts pass 0's
-// digits of each tile, and the pass-p kernel, when it writes a key to its
-// output position, counts the key's pass-(p+1) digit for the output tile
-// (global atomics).  A tile's prefix is then a plain sum over the counts of the
-// earlier tiles (read in parallel), and the global start of each digit comes
-// from the all-pass histograms that k_keys also builds.  So a pass is one
-// kernel with no look-back, no spin-wait and no ticket:
-//   1. load the tile (all loads issued first), rank keys by digit per warp
-//      with __match_any_sync in key order (stable);
-//   2. per digit: offsets across warps, prefix over earlier tiles, global base;
-//   3. regroup by digit in shared memory, write digit runs, count next digits.
+// The keys are cut into fixed tiles of kSortThreads x R keys (R = 4..6 rounds
+// per thread, chosen per context so that the tiles fit one per SM where they
+// can: a pass is one wave, and no SM runs two tiles while others idle).  For
+// pass p every tile needs, per digit, how many keys with that digit lie in
+// the tiles before it.  Those per-tile counts are produced one pass ahead:
+// k_keys counts pass 0's digits of each tile, and the pass-p kernel, when it
+// writes a key to its output position, counts the key's pass-(p+1) digit for
+// the output tile (global atomics).  A tile's prefix is then a plain sum over
+// the counts of the earlier tiles (read in parallel), and the global start of
+// each digit comes from the all-pass histograms that k_keys also builds.  So
+// a pass is one kernel with no look-back, no spin-wait and no ticket:
+//   1. issue the tile's loads, then the loads of the earlier tiles' counts;
+//   2. rank keys by digit per warp in key order (stable): the lanes that share
+//      a digit are the AND of eight ballots, one per digit bit;
+//   3. per digit: offsets across warps, prefix over earlier tiles, global base;
+//   4. regroup by digit in shared memory, write digit runs, count next digits.
 #include <stdint.h>
 
 #include "fa2_internal.cuh"
@@ -23,80 +26,77 @@ namespace fa2 {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
+constexpr int kQuarters = kSortThreads / 256;  // threads per digit in the scans
 
+template <int R>
 struct SortSmem {
-    uint64_t keys[kSortTile];
-    uint32_t vals[kSortTile];
-    uint32_t whist[kSortWarps][256];  // per-warp digit counts, then offsets
-    uint32_t tile_off[256];           // exclusive scan of tile digit counts
-    uint32_t gbase[256];              // global start of this tile's digit run
-    uint32_t part[kSortThreads / 256][256];  // partial prefixes over earlier tiles
-    uint32_t scan_tmp[kSortWarps];
+    uint64_t keys[kSortThreads * R];
+    uint32_t vals[kSortThreads * R];
+    uint32_t whist[kSortWarps][256];    // per-warp digit counts, then offsets
+    uint32_t tile_off[256];             // exclusive scan of tile digit counts
+    uint32_t gbase[256];                // global start of this tile's digit run
+    uint32_t part[kQuarters][256];      // partial prefixes over earlier tiles
+    uint32_t qsum[kQuarters][256];      // per-quarter sums of the warp counts
+    uint32_t scan_h[8], scan_t[8];      // warp totals of the two digit scans
 };
 
-// Block-wide exclusive scan of one value per thread.
-__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t *tmp) {
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    uint32_t inc = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        uint32_t t = __shfl_up_sync(kFull, inc, o);
-        if (lane >= o) inc += t;
-    }
-    if (lane == 31) tmp[wid] = inc;
-    __syncthreads();
-    uint32_t wbase = 0;
-    for (int w = 0; w < wid; ++w) wbase += tmp[w];
-    __syncthreads();
-    return wbase + inc - v;
-}
-
-__global__ void __launch_bounds__(kSortThreads, 2) k_sort_pass(
+template <int R>
+__global__ void __launch_bounds__(kSortThreads, R == kSortMinRounds ? 2 : 1) k_sort_pass(
     int n, int pass, const uint64_t *__restrict kin, const uint32_t *__restrict vin,
     uint64_t *__restrict kout, uint32_t *__restrict vout, const IterCounters *__restrict ctr,
     uint32_t *__restrict counts, int ntiles, const DevState *__restrict st) {
+    constexpr int kTile = kSortThreads * R;
+    constexpr int kChunk = kTile / kSortWarps;  // keys per warp
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    SortSmem &S = *reinterpret_cast<SortSmem *>(smem_raw);
+    SortSmem<R> &S = *reinterpret_cast<SortSmem<R> *>(smem_raw);
     if (st->err || st->poison) return;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int shift = 8 * pass;
     const int tile = blockIdx.x;
-    for (int j = threadIdx.x; j < kSortWarps * 256; j += kSortThreads) (&S.whist[0][0])[j] = 0;
-    const int base = tile * kSortTile + wid * (kSortTile / kSortWarps);
+    const int base = tile * kTile + wid * kChunk;
     const unsigned lt_mask = (1u << lane) - 1u;
 
-    // 0. this tile's prefix per digit: the counts of all earlier tiles, summed
-    //    by 4 threads per digit with 8 loads in flight each, started first so
-    //    that the loads overlap the ranking below
-    uint32_t prefix_part;
-    {
-        const uint32_t *cp = counts + (size_t)pass * ntiles * 256 + (threadIdx.x & 255);
-        uint32_t a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        int t = threadIdx.x >> 8;
-        for (; t + 28 < tile; t += 32) {
+    // 1. the warp's chunk (all loads in flight) ...
+    uint64_t k[R];
+    uint32_t v[R];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) a[j] += __ldcg(cp + (size_t)(t + 4 * j) * 256);
-        }
-        for (; t < tile; t += 4) a[0] += __ldcg(cp + (size_t)t * 256);
-        prefix_part = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
-    }
-
-    // 1. load the warp's chunk (all loads in flight), then rank round by round
-    uint64_t k[kSortRounds];
-    uint32_t v[kSortRounds];
-#pragma unroll
-    for (int r = 0; r < kSortRounds; ++r) {
+    for (int r = 0; r < R; ++r) {
         const int idx = base + r * 32 + lane;
         k[r] = idx < n ? kin[idx] : 0ull;
         v[r] = idx < n ? vin[idx] : 0u;
     }
-    __syncthreads();
-    uint32_t rank[kSortRounds];
+    // ... and this tile's prefix per digit: the counts of all earlier tiles,
+    // summed by 4 threads per digit with 8 loads in flight each
+    uint32_t prefix_part;
+    {
+        const uint32_t *cp = counts + (size_t)pass * ntiles * 256 + (threadIdx.x & 255);
+        uint32_t a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int t = threadIdx.x >> 8; t < tile; t += 4 * 8) {
 #pragma unroll
-    for (int r = 0; r < kSortRounds; ++r) {
+            for (int j = 0; j < 8; ++j)
+                if (t + 4 * j < tile) a[j] += __ldcg(cp + (size_t)(t + 4 * j) * 256);
+        }
+        prefix_part = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+    }
+    for (int j = threadIdx.x; j < kSortWarps * 256; j += kSortThreads) (&S.whist[0][0])[j] = 0;
+    S.part[threadIdx.x >> 8][threadIdx.x & 255] = prefix_part;
+    __syncthreads();
+
+    // 2. rank round by round; an invalid lane gets a 9th digit bit so that it
+    //    shares no valid lane's digit
+    uint32_t rank[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
         const bool valid = base + r * 32 + lane < n;
-        const uint32_t d = valid ? (uint32_t)(k[r] >> shift) & 255u : 256u + lane;
-        const unsigned peers = __match_any_sync(kFull, d);
+        const uint32_t d = (uint32_t)(k[r] >> shift) & 255u;
+        unsigned peers = __ballot_sync(kFull, valid);
+        if (!valid) peers = ~peers;
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+            const bool bit = (d >> b) & 1u;
+            const unsigned m = __ballot_sync(kFull, bit);
+            peers &= bit ? m : ~m;
+        }
         uint32_t before = 0;
         if (valid) before = S.whist[wid][d];
         rank[r] = before + __popc(peers & lt_mask);
@@ -106,35 +106,71 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_sort_pass(
     }
     __syncthreads();
 
-    // 2. per digit (threads 0..255): offsets across warps, prefix over the
-    //    earlier tiles, global start
-    const int d = threadIdx.x;
-    const bool digit_thread = d < 256;
-    S.part[threadIdx.x >> 8][threadIdx.x & 255] = prefix_part;
+    // 3. per digit: exclusive offsets across the 32 warps (4 threads per
+    //    digit, 8 warps each), the tile's digit counts, the prefix over the
+    //    earlier tiles and the global start
+    const int dg = threadIdx.x & 255, qt = threadIdx.x >> 8;
+    {
+        uint32_t q = 0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) q += S.whist[qt * 8 + w][dg];
+        S.qsum[qt][dg] = q;
+    }
     __syncthreads();
-    uint32_t tile_count = 0, prefix = 0, hist_d = 0;
-    if (digit_thread) {
-#pragma unroll 8
-        for (int w = 0; w < kSortWarps; ++w) {
-            const uint32_t c = S.whist[w][d];
-            S.whist[w][d] = tile_count;
+    uint32_t tile_count = 0, hist_d = 0, prefix = 0;
+    {
+        uint32_t run = 0;
+#pragma unroll
+        for (int q = 0; q < kQuarters; ++q) {
+            const uint32_t c = S.qsum[q][dg];
+            if (q < qt) run += c;
             tile_count += c;
         }
-        prefix = (S.part[0][d] + S.part[1][d]) + (S.part[2][d] + S.part[3][d]);
-        hist_d = ctr->hist[pass][d];
+#pragma unroll
+        for (int w = 0; w < 8; ++w) {
+            const uint32_t c = S.whist[qt * 8 + w][dg];
+            S.whist[qt * 8 + w][dg] = run;
+            run += c;
+        }
     }
-    const uint32_t bin_base = block_excl_scan(hist_d, S.scan_tmp);
-    const uint32_t toff = block_excl_scan(tile_count, S.scan_tmp);
+    // both digit scans (global histogram, tile counts) in warps 0..7
+    const bool digit_thread = threadIdx.x < 256;
+    uint32_t inc_h = 0, inc_t = 0;
     if (digit_thread) {
-        S.gbase[d] = bin_base + prefix;
-        S.tile_off[d] = toff;
+        prefix = (S.part[0][dg] + S.part[1][dg]) + (S.part[2][dg] + S.part[3][dg]);
+        hist_d = ctr->hist[pass][dg];
+        inc_h = hist_d;
+        inc_t = tile_count;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t th = __shfl_up_sync(kFull, inc_h, o);
+            const uint32_t tt = __shfl_up_sync(kFull, inc_t, o);
+            if (lane >= o) {
+                inc_h += th;
+                inc_t += tt;
+            }
+        }
+        if (lane == 31) {
+            S.scan_h[wid] = inc_h;
+            S.scan_t[wid] = inc_t;
+        }
+    }
+    __syncthreads();
+    if (digit_thread) {
+        uint32_t bh = 0, bt = 0;
+        for (int w = 0; w < wid; ++w) {
+            bh += S.scan_h[w];
+            bt += S.scan_t[w];
+        }
+        S.gbase[dg] = bh + inc_h - hist_d + prefix;
+        S.tile_off[dg] = bt + inc_t - tile_count;
     }
     __syncthreads();
 
-    // 3. regroup by digit in shared memory, then write digit runs and count
+    // 4. regroup by digit in shared memory, then write digit runs and count
     //    the next pass's digits per output tile
 #pragma unroll
-    for (int r = 0; r < kSortRounds; ++r) {
+    for (int r = 0; r < R; ++r) {
         if (base + r * 32 + lane < n) {
             const uint32_t dd = (uint32_t)(k[r] >> shift) & 255u;
             const uint32_t p = S.tile_off[dd] + S.whist[wid][dd] + rank[r];
@@ -143,7 +179,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_sort_pass(
         }
     }
     __syncthreads();
-    const int tile_n = min(kSortTile, n - tile * kSortTile);
+    const int tile_n = min(kTile, n - tile * kTile);
     uint32_t *next = pass < 7 ? counts + (size_t)(pass + 1) * ntiles * 256 : nullptr;
     for (int j = threadIdx.x; j < tile_n; j += kSortThreads) {
         const uint64_t key = S.keys[j];
@@ -152,24 +188,37 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_sort_pass(
         kout[out] = key;
         vout[out] = S.vals[j];
         if (next)
-            atomicAdd(&next[(size_t)(out / kSortTile) * 256 + ((uint32_t)(key >> (shift + 8)) & 255u)], 1u);
+            atomicAdd(&next[(size_t)(out / kTile) * 256 + ((uint32_t)(key >> (shift + 8)) & 255u)], 1u);
+    }
+}
+
+template <int R>
+void launch_passes(const Buffers &b, cudaStream_t s) {
+    const int tiles = sort_tiles(b.n, R);
+    for (int pass = 0; pass < 8; ++pass) {
+        const int src = pass & 1, dst = src ^ 1;
+        k_sort_pass<R><<<tiles, kSortThreads, sizeof(SortSmem<R>), s>>>(
+            b.n, pass, b.keys[src], b.vals[src], b.keys[dst], b.vals[dst], b.ctr, b.sort_counts,
+            tiles, b.st);
     }
 }
 
 }  // namespace
 
 void sort_set_smem_attr() {
-    cudaFuncSetAttribute(k_sort_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)sizeof(SortSmem));
+    cudaFuncSetAttribute(k_sort_pass<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(SortSmem<4>));
+    cudaFuncSetAttribute(k_sort_pass<5>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(SortSmem<5>));
+    cudaFuncSetAttribute(k_sort_pass<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(SortSmem<6>));
 }
 
 void launch_sort(const Buffers &b, cudaStream_t s) {
-    const int tiles = sort_tiles(b.n);
-    for (int pass = 0; pass < 8; ++pass) {
-        const int src = pass & 1, dst = src ^ 1;
-        k_sort_pass<<<tiles, kSortThreads, sizeof(SortSmem), s>>>(
-            b.n, pass, b.keys[src], b.vals[src], b.keys[dst], b.vals[dst], b.ctr, b.sort_counts,
-            tiles, b.st);
+    switch (b.sort_rounds) {
+        case 5: launch_passes<5>(b, s); break;
+        case 6: launch_passes<6>(b, s); break;
+        default: launch_passes<4>(b, s); break;
     }
 }
 

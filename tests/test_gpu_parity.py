@@ -78,3 +78,20 @@ def test_repulsion_error_vs_fp64(ba3k):
     err_ref = rel_rmse(rep_ref, exact)
     assert err_gpu <= err_ref + 1e-4, (err_gpu, err_ref)
     assert err_gpu < 0.05
+
+
+def test_walk_visits_match_oracle(ba3k):
+    """Node tests of the warp walk (every accept or open, times the group's
+    lanes) against the oracle's restatement of the reference walk on the same
+    positions: the same tree and the same vote decide every step, so the counts
+    agree up to the rare test that float rounding of a cell centre flips."""
+    from oracle import oracle as O
+    g = ba3k
+    xy = O.random_positions(g.n, 2000, 2000, 99)
+    e = _engine(g, xy, 10.0, 1.0, True)
+    e.step(1)
+    st = e.stats()
+    _, ovf, visits = O.Tree(xy, g.mass).repulsion(10.0)
+    assert not ovf and visits > 0
+    assert abs(st["visits"] - visits) <= 1e-3 * visits, (st["visits"], visits)
+    assert 0 < st["interactions"] < st["visits"]
