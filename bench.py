@@ -41,6 +41,11 @@ SCALE, DRAWS = 20, 16_777_216
 K_R, K_G, STRONG = 10.0, 1.0, True
 WIDTH = 2.0e4
 KERNELS_PER_ITER = 14  # attract, keys, 8 sort passes, tree_count, emit, traverse, displace
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_attract
+# launch at this workload, from an ncu capture of
+#   ncu --set full --clock-control none -k regex:k_attract -s 4 -c 1 \
+#       python bench.py --steps 3 --warmup 3 --no-cpu-baseline
+ATTRACT_TRAFFIC_BYTES = 144_659_712
 
 
 def clocks_sampler(device: int, path: str):
@@ -210,6 +215,14 @@ def run_ours(args, world, rank, local):
     ms_max = barrier_max(world, ms)
     value = world * args.steps / (ms_max / 1000.0)
 
+    # per-kernel times with every kernel running alone (the attraction is
+    # otherwise spread over the tree build's gaps): the roofline denominators
+    iso_steps = min(args.steps, 10)
+    eng.set_overlap(False)
+    eng.step(3)
+    _, kms_iso = eng.step_timed(iso_steps)
+    eng.set_overlap(True)
+
     # end to end through the C ABI with pinned host buffers
     host = torch.empty((n, 2), dtype=torch.float32, pin_memory=True)
     host.numpy()[:] = eng.get_positions()
@@ -232,23 +245,27 @@ def run_ours(args, world, rank, local):
     nnz = st["nnz_padded"]
     attract_bytes = 4 * nnz + 4 * (n + 1) + 8 * n + 4 * n + 8 * n
     disp_bytes = 40 * n
-    trav_ms = kms.get("traverse", 0.0)
+    trav_ms = kms_iso.get("traverse", 0.0)
     kernels = {}
     for nm in names:
-        kernels[nm] = {"ms": kms.get(nm, 0.0)}
+        kernels[nm] = {"ms": kms.get(nm, 0.0), "ms_alone": kms_iso.get(nm, 0.0)}
+    att_ms = kms_iso["attract"]
     kernels["attract"].update(bytes=attract_bytes,
-                              gbs=attract_bytes / (kms["attract"] * 1e6) if kms["attract"] else None)
+                              gbs=attract_bytes / (att_ms * 1e6) if att_ms else None)
+    dsp_ms = kms_iso["displace"]
     kernels["displace"].update(bytes=disp_bytes,
-                               gbs=disp_bytes / (kms["displace"] * 1e6) if kms["displace"] else None)
+                               gbs=disp_bytes / (dsp_ms * 1e6) if dsp_ms else None)
     inter = st["interactions"]
     kernels["traverse"].update(interactions=inter, visits=st["visits"],
                                interactions_per_s=inter / (trav_ms * 1e-3) if trav_ms else None)
-    dom = max(names, key=lambda k: kms.get(k, 0.0))
+    dom = max(names, key=lambda k: kms_iso.get(k, 0.0))
     att_gbs = kernels["attract"]["gbs"] or 0.0
     roofline = {"kernel": "attract", "bound": "hbm", "achieved": att_gbs, "peak": hbm,
-                "unit": "GB/s", "frac": att_gbs / hbm, "traffic": None,
-                "note": f"peak = {pk_kind} HBM copy bandwidth; dominant kernel by time is "
-                        f"'{dom}' ({kms.get(dom, 0.0):.3f} ms/launch)"}
+                "unit": "GB/s", "frac": att_gbs / hbm,
+                "traffic": ATTRACT_TRAFFIC_BYTES, "traffic_unit": "bytes per launch",
+                "note": f"peak = {pk_kind} HBM copy bandwidth; achieved = algorithmic bytes / "
+                        f"the kernel's CUDA-event time running alone; dominant kernel by time "
+                        f"is '{dom}' ({kms_iso.get(dom, 0.0):.3f} ms/launch alone)"}
     # The walk is bound by instruction issue and dependent-load latency, not by
     # HBM or tensor cores: its work is 10 FP32 operations per interaction,
     # reported against the nominal FP32 rate of the SMs.

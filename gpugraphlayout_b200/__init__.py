@@ -56,7 +56,8 @@ class Engine:
 
     def __init__(self, num_nodes: int, sources, targets, *, strong_gravity: bool = False,
                  gravity: float = 1.0, scale: float = 1.0, theta: float = 1.0,
-                 epssq: float = 0.05 * 0.05, device: int = 0, use_barneshut: bool = True):
+                 epssq: float = 0.05 * 0.05, device: int = 0, use_barneshut: bool = True,
+                 linlog: bool = False):
         L = lib()
         self._src = np.ascontiguousarray(sources, np.uint32)
         self._dst = np.ascontiguousarray(targets, np.uint32)
@@ -66,6 +67,7 @@ class Engine:
         p.use_barneshut = int(use_barneshut)
         p.strong_gravity = int(strong_gravity)
         p.gravity, p.scale, p.theta, p.epssq, p.device = gravity, scale, theta, epssq, device
+        p.linlog = int(linlog)
         st = C.c_int(0)
         self._ctx = L.fa2_create(C.byref(g), C.byref(p), C.byref(st))
         check(st.value, "fa2_create")
@@ -117,6 +119,14 @@ class Engine:
 
     def set_force_params(self, scale: float, gravity: float) -> None:
         check(lib().fa2_set_force_params(self._ctx, scale, gravity), "fa2_set_force_params")
+
+    def set_linlog(self, enable: bool) -> None:
+        """Linear-log (True) or linear (False) attraction from the next step on."""
+        check(lib().fa2_set_linlog(self._ctx, 1 if enable else 0), "fa2_set_linlog")
+
+    def set_overlap(self, enable: bool) -> None:
+        """Attraction beside the tree build (default) or alone before it."""
+        check(lib().fa2_set_overlap(self._ctx, 1 if enable else 0), "fa2_set_overlap")
 
     # -- inspection ----------------------------------------------------------
     def forces(self):
@@ -261,6 +271,10 @@ class CUDAForceAtlas2:
                              gravity=gravity, scale=scale, device=device)
         self.engine.set_positions(layout.xy)
         self.iteration = 0
+        # ForceAtlas2's public flags (src/RPForceAtlas2.hpp:44); the engine
+        # honours use_linlog (linear-log attraction)
+        self.use_linlog = False
+        self.prevent_overlap = False
 
     def setScale(self, s: float):
         self.k_r = s
@@ -275,6 +289,7 @@ class CUDAForceAtlas2:
         self.doSteps(1)
 
     def doSteps(self, n: int):
+        self.engine.set_linlog(self.use_linlog)
         self.engine.set_force_params(self.k_r, self.k_g)
         self.engine.step(n)
         self.iteration += n

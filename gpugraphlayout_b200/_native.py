@@ -17,7 +17,7 @@ EXPORTS = (
     "fa2_default_params", "fa2_create", "fa2_destroy", "fa2_set_positions",
     "fa2_get_positions", "fa2_step", "fa2_step_timed", "fa2_kernel_name",
     "fa2_get_stats", "fa2_get_forces", "fa2_get_sort_order", "fa2_set_speed_state",
-    "fa2_get_speed_state", "fa2_set_force_params", "fa2_repulsion_noalloc", "fa2_ugraph_load",
+    "fa2_get_speed_state", "fa2_set_force_params", "fa2_set_linlog", "fa2_set_overlap", "fa2_repulsion_noalloc", "fa2_ugraph_load",
     "fa2_ugraph_from_pairs", "fa2_ugraph_free", "fa2_ugraph_num_nodes",
     "fa2_ugraph_num_edges", "fa2_ugraph_node_map_r", "fa2_ugraph_degrees",
     "fa2_ugraph_edges", "fa2_random_positions", "fa2_write_layout",
@@ -42,7 +42,7 @@ class Params(C.Structure):
     _fields_ = [("use_barneshut", C.c_int32), ("strong_gravity", C.c_int32),
                 ("gravity", C.c_float), ("scale", C.c_float), ("theta", C.c_float),
                 ("epssq", C.c_float), ("jitter_tolerance", C.c_float), ("k_s_max", C.c_float),
-                ("device", C.c_int32)]
+                ("device", C.c_int32), ("linlog", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -94,6 +94,8 @@ def lib():
     L.fa2_set_speed_state.argtypes = [vp, C.c_float, C.c_float, vp]
     L.fa2_get_speed_state.argtypes = [vp, f32p, f32p, vp]
     L.fa2_set_force_params.argtypes = [vp, C.c_float, C.c_float]
+    L.fa2_set_overlap.argtypes = [vp, C.c_int32]
+    L.fa2_set_linlog.argtypes = [vp, C.c_int32]
     L.fa2_repulsion_noalloc.argtypes = [vp, vp, C.c_uint32, C.POINTER(Params), vp, vp]
     L.fa2_ugraph_load.restype = vp
     L.fa2_ugraph_load.argtypes = [C.c_char_p, ip]

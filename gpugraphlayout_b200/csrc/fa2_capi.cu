@@ -49,7 +49,7 @@ struct fa2_ctx {
     size_t scratch_bytes = 0;
     float2 *stage_xy = nullptr;    // n, reference order
     uint32_t *stage_ids = nullptr; // n
-    int bbox_blocks = 0, trav_blocks = 0;
+    int bbox_blocks = 0, trav_blocks = 0, attract_grid = 0;
     cudaStream_t sA = nullptr, sB = nullptr;
     cudaEvent_t evFork = nullptr, evJoin = nullptr;
     // graphs
@@ -60,9 +60,19 @@ struct fa2_ctx {
     std::vector<cudaEvent_t> slot_events;      // events captured into the timed graph
     std::vector<cudaEvent_t> event_pool;       // per (iteration, slot, start/end)
     int last_perturb_rounds = 0;
+    bool overlap = true;  // attraction on stream B beside the tree build
 };
 
 namespace {
+
+// Drops the captured iteration graphs; the next step captures them again.
+void drop_graphs(fa2_ctx *c) {
+    if (c->exec) cudaGraphExecDestroy(c->exec);
+    if (c->exec_timed) cudaGraphExecDestroy(c->exec_timed);
+    if (c->graph_timed) cudaGraphDestroy(c->graph_timed);
+    c->exec = c->exec_timed = nullptr;
+    c->graph_timed = nullptr;
+}
 
 int cuda_status(cudaError_t e) {
     if (e == cudaSuccess) return FA2_OK;
@@ -177,11 +187,15 @@ void enqueue_iteration(fa2_ctx *c, bool full, bool perturb_first, bool timed) {
             cudaEventRecordWithFlags(c->slot_events[slot * 2 + end], s, cudaEventRecordExternal);
     };
     cudaMemsetAsync(c->scratch, 0, c->scratch_bytes, A);
-    if (full) {
+    if (full && !c->overlap) {
+        mark(S_ATTRACT, 0, A);
+        launch_attract(b, c->kp, c->plan, c->attract_grid, A);
+        mark(S_ATTRACT, 1, A);
+    } else if (full) {
         cudaEventRecord(c->evFork, A);
         cudaStreamWaitEvent(B, c->evFork, 0);
         mark(S_ATTRACT, 0, B);
-        launch_attract(b, c->kp, c->plan, B);
+        launch_attract(b, c->kp, c->plan, c->attract_grid, B);
         mark(S_ATTRACT, 1, B);
         cudaEventRecord(c->evJoin, B);
     }
@@ -198,7 +212,7 @@ void enqueue_iteration(fa2_ctx *c, bool full, bool perturb_first, bool timed) {
     mark(S_EMIT, 0, A);
     launch_emit(b, c->nsm, A);
     mark(S_EMIT, 1, A);
-    if (full) cudaStreamWaitEvent(A, c->evJoin, 0);
+    if (full && c->overlap) cudaStreamWaitEvent(A, c->evJoin, 0);
     mark(S_TRAV, 0, A);
     launch_traverse(b, c->kp, c->trav_blocks, A);
     mark(S_TRAV, 1, A);
@@ -334,6 +348,7 @@ void fa2_default_params(fa2_params *p) {
     p->jitter_tolerance = 1.0f;
     p->k_s_max = 10.0f;
     p->device = 0;
+    p->linlog = 0;
 }
 
 fa2_ctx *fa2_create(const fa2_graph_desc *g, const fa2_params *prm, int *status) {
@@ -381,6 +396,7 @@ fa2_ctx *fa2_create(const fa2_graph_desc *g, const fa2_params *prm, int *status)
     c->kp.itolsq = 1.0f / (prm->theta * prm->theta);  // src/RPForceAtlas2.cpp:47
     c->kp.epssq = prm->epssq;
     c->kp.strong_gravity = prm->strong_gravity;
+    c->kp.linlog = prm->linlog != 0;
 
     std::vector<uint32_t> off;
     std::vector<int32_t> col;
@@ -408,7 +424,7 @@ fa2_ctx *fa2_create(const fa2_graph_desc *g, const fa2_params *prm, int *status)
         (s = dalloc(c, &b.keys[1], n)) || (s = dalloc(c, &b.vals[0], n)) ||
         (s = dalloc(c, &b.vals[1], n)) || (s = dalloc(c, &b.lcp, n)) ||
         (s = dalloc(c, &b.group, n)) || (s = dalloc(c, &b.body_node, n)) ||
-        (s = dalloc(c, &b.nodes, cap + 1)) ||  // + the traversal's sentinel slot
+        (s = dalloc(c, &b.nodes, cap + 1)) ||  // + one spare slot
         (s = dalloc(c, &b.owner, cap)) ||
         (s = dalloc(c, &b.pm, (size_t)n + 1)) || (s = dalloc(c, &b.pxy, 2 * ((size_t)n + 1))) ||
         (s = dalloc(c, &b.lookback, (size_t)count_tiles((int)n))) ||
@@ -452,6 +468,7 @@ fa2_ctx *fa2_create(const fa2_graph_desc *g, const fa2_params *prm, int *status)
         if (cudaEventCreate(&e) != cudaSuccess) return fail(FA2_ERR_CUDA);
     sort_set_smem_attr();
     c->trav_blocks = c->nsm * traverse_blocks_per_sm();
+    c->attract_grid = attract_grid((int)n, c->nsm);
 
     cudaStream_t A = c->sA;
     if (cudaMemcpyAsync(d_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice, A) ||
@@ -646,11 +663,28 @@ int fa2_set_force_params(fa2_ctx *c, float scale, float gravity) {
     c->prm.scale = scale;
     c->prm.gravity = gravity;
     // the captured graphs hold the old values as kernel arguments
-    if (c->exec) cudaGraphExecDestroy(c->exec);
-    if (c->exec_timed) cudaGraphExecDestroy(c->exec_timed);
-    if (c->graph_timed) cudaGraphDestroy(c->graph_timed);
-    c->exec = c->exec_timed = nullptr;
-    c->graph_timed = nullptr;
+    drop_graphs(c);
+    return FA2_OK;
+}
+
+int fa2_set_linlog(fa2_ctx *c, int32_t enable) {
+    if (!c) return FA2_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(c->device));
+    if (c->kp.linlog == (enable != 0)) return FA2_OK;
+    CK(cudaStreamSynchronize(c->sA));
+    c->kp.linlog = enable != 0;
+    c->prm.linlog = enable != 0;
+    drop_graphs(c);
+    return FA2_OK;
+}
+
+int fa2_set_overlap(fa2_ctx *c, int32_t enable) {
+    if (!c) return FA2_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(c->device));
+    if (c->overlap == (enable != 0)) return FA2_OK;
+    CK(cudaStreamSynchronize(c->sA));
+    c->overlap = enable != 0;
+    drop_graphs(c);  // recaptured with the new stream layout at the next step
     return FA2_OK;
 }
 

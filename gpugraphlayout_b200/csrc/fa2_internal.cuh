@@ -16,8 +16,7 @@ namespace fa2 {
 
 constexpr int kWarp = 32;
 constexpr int kLevels = 32;        // quadrant digits in a 64-bit Morton key
-constexpr int kBodyLevel = 32;     // level code of a body (leaf) node; it shares the walk's
-                                   // always-accept threshold with level-32 cells
+constexpr int kBodyLevel = 63;     // level code of a body (leaf) node
 constexpr int kMetaShift = 6;      // node meta = next_index << 6 | level code
 constexpr uint32_t kMaxTreeNodes = 1u << 26;
 constexpr int kMaxRun = 1024;      // longest run of equal 64-bit keys handled
@@ -55,7 +54,8 @@ struct IterCounters {
     unsigned trav_ticket;
     unsigned trav_done;
     unsigned disp_done;
-    unsigned pad[3];
+    unsigned attract_ticket;
+    unsigned pad[2];
     unsigned hist[8][256];  // per-pass digit histograms of the sort keys
 };
 
@@ -94,6 +94,8 @@ struct AttractBucket {
 };
 constexpr int kMaxBuckets = 8;
 constexpr int kAttractBatch = 4;  // row groups per warp in short-row buckets
+constexpr int kHubNodes = 6144;   // highest-degree nodes whose positions the attraction
+                                  // keeps in shared memory (48 KB)
 struct AttractPlan {
     AttractBucket b[kMaxBuckets];
     int nbuckets;
@@ -123,7 +125,7 @@ struct Buffers {
     uint32_t *group;          // n: first preorder node of body k's group
     uint32_t *body_node;      // n: preorder node of sorted body k
     uint32_t *owner;          // capacity: per node, sorted body k << 6 | cell offset (63: body)
-    float4 *nodes;            // capacity + 1: x, y, mass, meta (+ traversal sentinel)
+    float4 *nodes;            // capacity + 1: x, y, mass, meta
     uint32_t capacity;
     long long *pm;            // n + 1: exclusive prefix of mass over sorted bodies
     __int128 *pxy;            // 2(n + 1): prefix of mass x fixed-point offset, x and y
@@ -141,6 +143,7 @@ struct Buffers {
 struct Params {
     float k_r, k_g, itolsq, epssq;
     int strong_gravity;
+    int linlog;  // linear-log attraction
     int nsm;
 };
 
@@ -158,7 +161,9 @@ void launch_emit(const Buffers &b, int nsm, cudaStream_t s);
 void launch_traverse(const Buffers &b, const Params &p, int nblocks, cudaStream_t s);
 void launch_displace(const Buffers &b, int nsm, cudaStream_t s);
 void launch_count_interactions(const Buffers &b, const Params &p, int nblocks, cudaStream_t s);
-void launch_attract(const Buffers &b, const Params &p, const AttractPlan &plan, cudaStream_t s);
+void launch_attract(const Buffers &b, const Params &p, const AttractPlan &plan, int grid,
+                    cudaStream_t s);
+int attract_grid(int n, int nsm);
 void launch_scatter_xy(int n, const uint32_t *ref_of, const float2 *src_ref, float2 *dst_int,
                        cudaStream_t s);
 void launch_gather_xy(int n, const uint32_t *ref_of, const float2 *src_int, float2 *dst_ref,

@@ -186,12 +186,6 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
     const uint32_t end = st->tree_nodes;
     const int lane = threadIdx.x & 31;
     const int nwarps = (n + 31) >> 5;
-    // Cell thresholds live one per lane: a node's level code, the low bits of
-    // its meta word, is the lane a shuffle reads its threshold from.  Lane 0
-    // holds 0, the threshold of bodies (always used) and of level-32 cells:
-    // there dq[32] is (2 radius / 2^32)^2 + eps, which float rounds to eps for
-    // any root radius below ~2e4, and d^2 + eps >= eps always holds.
-    const float lane_dq = lane == 0 ? 0.0f : s_dq[lane];
     // Groups of 32 bodies are handed out one at a time from a global ticket:
     // the work per group varies with the local density of the layout, and
     // warps that take consecutive tickets walk neighbouring bodies, so the
@@ -210,22 +204,24 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
         // sum of m_j d / (d^2 + eps) over the accepted nodes; the body's own
         // k_r m_i multiplies the sum once at the end
         float ax = 0.0f, ay = 0.0f;
-        // The walk ends past the sentinel node at index end, whose NaN
-        // position fails every lane's test: it is opened like a cell, and only
-        // an opening step needs the end test.
         uint32_t node = 1;
-        for (;;) {
-            const float4 r = __ldg(&nodes[node]);
-            const int meta = __float_as_int(r.w);
-            const float dx = px - r.x, dy = py - r.y;
-            const float d2 = dx * dx + dy * dy + prm.epssq;
-            if (__all_sync(kFull, d2 >= __shfl_sync(kFull, lane_dq, meta))) {
-                const float c = __fdividef(r.z, d2);
-                ax = fmaf(dx, c, ax);
-                ay = fmaf(dy, c, ay);
-                node = meta_next(meta);
-            } else if (++node > end) {
-                break;
+        // An opened cell's first child is node + 1 and always exists, so only
+        // a jump to "next" can end the walk.
+        if (node < end) {
+            for (;;) {
+                const float4 r = __ldg(&nodes[node]);
+                const int meta = __float_as_int(r.w);
+                const float dx = px - r.x, dy = py - r.y;
+                const float d2 = dx * dx + dy * dy + prm.epssq;
+                if (__all_sync(kFull, d2 >= s_dq[meta_level(meta)])) {
+                    const float c = __fdividef(r.z, d2);
+                    ax = fmaf(dx, c, ax);
+                    ay = fmaf(dy, c, ay);
+                    node = meta_next(meta);
+                    if (node >= end) break;
+                } else {
+                    ++node;
+                }
             }
         }
         const float kmi = prm.k_r * me.z;
@@ -333,7 +329,6 @@ __global__ void __launch_bounds__(kTravThreads) k_count_interactions(
     const int lane = threadIdx.x & 31;
     const int nwarps = (n + 31) >> 5;
     const int stride = (int)(gridDim.x * blockDim.x) >> 5;
-    const float lane_dq = lane == 0 ? 0.0f : s_dq[lane];  // as in k_traverse
     for (int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); w < nwarps; w += stride) {
         const int k = w * 32 + lane;
         const bool active = k < n;
@@ -347,7 +342,7 @@ __global__ void __launch_bounds__(kTravThreads) k_count_interactions(
             const float dx = px - r.x, dy = py - r.y;
             const float d2 = dx * dx + dy * dy + prm.epssq;
             ++steps;
-            if (__all_sync(kFull, d2 >= __shfl_sync(kFull, lane_dq, meta))) {
+            if (__all_sync(kFull, d2 >= s_dq[meta_level(meta)])) {
                 ++acc;
                 node = meta_next(meta);
             } else {
@@ -401,12 +396,41 @@ __global__ void __launch_bounds__(kDispThreads) k_displace(int n, float2 *__rest
 // shuffles; heavy rows take a whole block.  To keep many loads in flight a
 // warp of a short-row bucket works on kAttractBatch groups of rows at once:
 // all column loads first, then all position gathers.
-__device__ __forceinline__ void add_four(const int4 c, const float2 p,
-                                         const float2 *__restrict pos, float &ax, float &ay) {
-    const float2 q0 = __ldg(&pos[c.x]), q1 = __ldg(&pos[c.y]);
-    const float2 q2 = __ldg(&pos[c.z]), q3 = __ldg(&pos[c.w]);
-    ax += (q0.x - p.x) + (q1.x - p.x) + ((q2.x - p.x) + (q3.x - p.x));
-    ay += (q0.y - p.y) + (q1.y - p.y) + ((q2.y - p.y) + (q3.y - p.y));
+// One neighbour's pull: p_j - p_i, or with linear-log attraction (use_linlog
+// of the reference's CPU path, RPCPUForceAtlas2.cpp:59-67) that vector times
+// log(1 + d) / d, d = 0 taken as FLT_MAX (padding ids give the zero vector).
+template <bool LINLOG>
+__device__ __forceinline__ float2 pull(float2 q, float2 p) {
+    float dx = q.x - p.x, dy = q.y - p.y;
+    if (LINLOG) {
+        const float ex = p.x - q.x, ey = p.y - q.y;
+        const float dist = sqrtf(ex * ex + ey * ey);
+        const float w = dist == 0.0f ? FLT_MAX : logf(1 + dist) / dist;
+        dx *= w;
+        dy *= w;
+    }
+    return make_float2(dx, dy);
+}
+
+// Neighbour-position gathers: the first hub_n internal ids, the nodes of
+// highest degree, come from a copy in shared memory (at R-MAT scale 20 the top
+// 6,144 take 40 % of all gathers); the rest through L1/L2.
+struct Gather {
+    const float2 *__restrict pos;
+    const float2 *hub;
+    int hub_n;
+    __device__ __forceinline__ float2 operator()(int c) const {
+        return c < hub_n ? hub[c] : __ldg(&pos[c]);
+    }
+};
+
+template <bool LINLOG>
+__device__ __forceinline__ void add_four(const int4 c, const float2 p, const Gather &g,
+                                         float &ax, float &ay) {
+    const float2 q0 = pull<LINLOG>(g(c.x), p), q1 = pull<LINLOG>(g(c.y), p);
+    const float2 q2 = pull<LINLOG>(g(c.z), p), q3 = pull<LINLOG>(g(c.w), p);
+    ax += q0.x + q1.x + (q2.x + q3.x);
+    ay += q0.y + q1.y + (q2.y + q3.y);
 }
 
 __device__ __forceinline__ float2 with_gravity(float2 p, float m, float ax, float ay,
@@ -422,9 +446,8 @@ __device__ __forceinline__ float2 with_gravity(float2 p, float m, float ax, floa
 }
 
 // Rows of at most LANES int4 chunks (LANES <= 16): one chunk per lane.
-template <int LANES>
-__device__ __forceinline__ void attract_short_rows(int row0, int row_end,
-                                                   const float2 *__restrict pos,
+template <int LANES, bool LINLOG>
+__device__ __forceinline__ void attract_short_rows(int row0, int row_end, const Gather &g,
                                                    const float *__restrict mass,
                                                    const uint32_t *__restrict off,
                                                    const int4 *__restrict col4,
@@ -444,12 +467,12 @@ __device__ __forceinline__ void attract_short_rows(int row0, int row_end,
         const uint32_t e = valid ? off[row[u] + 1] >> 2 : 0u;
         has[u] = q < e;
         c[u] = has[u] ? __ldcs(&col4[q]) : make_int4(0, 0, 0, 0);
-        p[u] = valid ? pos[row[u]] : make_float2(0.0f, 0.0f);
+        p[u] = valid ? g.pos[row[u]] : make_float2(0.0f, 0.0f);
     }
 #pragma unroll
     for (int u = 0; u < kAttractBatch; ++u) {
         float ax = 0.0f, ay = 0.0f;
-        if (has[u]) add_four(c[u], p[u], pos, ax, ay);
+        if (has[u]) add_four<LINLOG>(c[u], p[u], g, ax, ay);
 #pragma unroll
         for (int o = LANES / 2; o > 0; o >>= 1) {
             ax += __shfl_xor_sync(kFull, ax, o);
@@ -462,42 +485,46 @@ __device__ __forceinline__ void attract_short_rows(int row0, int row_end,
 
 // Partial attraction of one row over chunks [b + first, e) with stride
 // STRIDE, four chunks in flight per lane.
-template <int STRIDE>
+template <int STRIDE, bool LINLOG>
 __device__ __forceinline__ void attract_long_row(uint32_t b, uint32_t e, int first, float2 p,
-                                                 const float2 *__restrict pos,
+                                                 const Gather &g,
                                                  const int4 *__restrict col4, float &ax,
                                                  float &ay) {
     uint32_t q = b + first;
     for (; q + 3 * STRIDE < e; q += 4 * STRIDE) {
         const int4 c0 = __ldcs(&col4[q]), c1 = __ldcs(&col4[q + STRIDE]);
         const int4 c2 = __ldcs(&col4[q + 2 * STRIDE]), c3 = __ldcs(&col4[q + 3 * STRIDE]);
-        add_four(c0, p, pos, ax, ay);
-        add_four(c1, p, pos, ax, ay);
-        add_four(c2, p, pos, ax, ay);
-        add_four(c3, p, pos, ax, ay);
+        add_four<LINLOG>(c0, p, g, ax, ay);
+        add_four<LINLOG>(c1, p, g, ax, ay);
+        add_four<LINLOG>(c2, p, g, ax, ay);
+        add_four<LINLOG>(c3, p, g, ax, ay);
     }
-    for (; q < e; q += STRIDE) add_four(__ldcs(&col4[q]), p, pos, ax, ay);
+    for (; q < e; q += STRIDE) add_four<LINLOG>(__ldcs(&col4[q]), p, g, ax, ay);
 }
 
-__global__ void __launch_bounds__(256) k_attract(AttractPlan plan, const float2 *__restrict pos,
-                                                 const float *__restrict mass,
-                                                 const uint32_t *__restrict off,
-                                                 const int4 *__restrict col4,
-                                                 float2 *__restrict fag, Params prm) {
-    __shared__ float2 s_red[256 / kWarp];
+// One work block of the attraction plan (a row for the block-per-row
+// bucket, 8 rows for the warp-per-row bucket, batches of short rows).
+template <bool LINLOG>
+__device__ __forceinline__ void attract_block(int vb, const AttractPlan &plan, const Gather &g,
+                                              const float *__restrict mass,
+                                              const uint32_t *__restrict off,
+                                              const int4 *__restrict col4,
+                                              float2 *__restrict fag, const Params &prm,
+                                              float2 *s_red) {
     int bi = 0;
 #pragma unroll 1
     for (int q = 1; q < plan.nbuckets; ++q)
-        if ((int)blockIdx.x >= plan.b[q].block_begin) bi = q;
+        if (vb >= plan.b[q].block_begin) bi = q;
     const AttractBucket bk = plan.b[bi];
-    const int blk = blockIdx.x - bk.block_begin;
+    const int blk = vb - bk.block_begin;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (bk.lanes == 256) {
         // one row per block
         const int row = bk.row_begin + blk;
-        const float2 p = pos[row];
+        const float2 p = g.pos[row];
         float ax = 0.0f, ay = 0.0f;
-        attract_long_row<256>(off[row] >> 2, off[row + 1] >> 2, threadIdx.x, p, pos, col4, ax, ay);
+        attract_long_row<256, LINLOG>(off[row] >> 2, off[row + 1] >> 2, threadIdx.x, p, g, col4,
+                                      ax, ay);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             ax += __shfl_xor_sync(kFull, ax, o);
@@ -520,9 +547,9 @@ __global__ void __launch_bounds__(256) k_attract(AttractPlan plan, const float2 
         // one row per warp
         const int row = bk.row_begin + blk * (256 / kWarp) + wid;
         if (row >= bk.row_end) return;
-        const float2 p = pos[row];
+        const float2 p = g.pos[row];
         float ax = 0.0f, ay = 0.0f;
-        attract_long_row<32>(off[row] >> 2, off[row + 1] >> 2, lane, p, pos, col4, ax, ay);
+        attract_long_row<32, LINLOG>(off[row] >> 2, off[row + 1] >> 2, lane, p, g, col4, ax, ay);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             ax += __shfl_xor_sync(kFull, ax, o);
@@ -534,11 +561,36 @@ __global__ void __launch_bounds__(256) k_attract(AttractPlan plan, const float2 
     // short rows: kAttractBatch groups of 32/lanes rows per warp
     const int row0 = bk.row_begin + (blk * (256 / kWarp) + wid) * kAttractBatch * (32 / bk.lanes);
     switch (bk.lanes) {
-        case 16: attract_short_rows<16>(row0, bk.row_end, pos, mass, off, col4, fag, prm, lane); break;
-        case 8: attract_short_rows<8>(row0, bk.row_end, pos, mass, off, col4, fag, prm, lane); break;
-        case 4: attract_short_rows<4>(row0, bk.row_end, pos, mass, off, col4, fag, prm, lane); break;
-        case 2: attract_short_rows<2>(row0, bk.row_end, pos, mass, off, col4, fag, prm, lane); break;
-        default: attract_short_rows<1>(row0, bk.row_end, pos, mass, off, col4, fag, prm, lane); break;
+        case 16: attract_short_rows<16, LINLOG>(row0, bk.row_end, g, mass, off, col4, fag, prm, lane); break;
+        case 8: attract_short_rows<8, LINLOG>(row0, bk.row_end, g, mass, off, col4, fag, prm, lane); break;
+        case 4: attract_short_rows<4, LINLOG>(row0, bk.row_end, g, mass, off, col4, fag, prm, lane); break;
+        case 2: attract_short_rows<2, LINLOG>(row0, bk.row_end, g, mass, off, col4, fag, prm, lane); break;
+        default: attract_short_rows<1, LINLOG>(row0, bk.row_end, g, mass, off, col4, fag, prm, lane); break;
+    }
+}
+
+// The attraction pass: a grid that fills the GPU once, each block copying
+// the hub positions into shared memory and then taking work blocks of the
+// plan from a ticket until none are left.
+template <bool LINLOG>
+__global__ void __launch_bounds__(256) k_attract(AttractPlan plan, const float2 *__restrict pos,
+                                                 const float *__restrict mass,
+                                                 const uint32_t *__restrict off,
+                                                 const int4 *__restrict col4,
+                                                 float2 *__restrict fag, Params prm,
+                                                 unsigned *ticket, int hub_n) {
+    extern __shared__ float2 s_hub[];
+    __shared__ float2 s_red[256 / kWarp];
+    __shared__ int s_vb;
+    for (int i = threadIdx.x; i < hub_n; i += blockDim.x) s_hub[i] = pos[i];
+    const Gather g{pos, s_hub, hub_n};
+    for (;;) {
+        if (threadIdx.x == 0) s_vb = (int)atomicAdd(ticket, 1u);
+        __syncthreads();  // the ticket, and on the first round the hub copy
+        const int vb = s_vb;
+        if (vb >= plan.nblocks) break;
+        attract_block<LINLOG>(vb, plan, g, mass, off, col4, fag, prm, s_red);
+        __syncthreads();  // s_vb and s_red are reused
     }
 }
 
@@ -600,9 +652,31 @@ void launch_count_interactions(const Buffers &b, const Params &p, int nblocks, c
     k_count_interactions<<<nblocks, kTravThreads, 0, s>>>(b.n, b.nodes, b.body_node, b.st, p);
 }
 
-void launch_attract(const Buffers &b, const Params &p, const AttractPlan &plan, cudaStream_t s) {
+int attract_hub_nodes(int n) { return n < kHubNodes ? n : kHubNodes; }
+
+int attract_grid(int n, int nsm) {
+    const size_t smem = sizeof(float2) * (size_t)attract_hub_nodes(n);
+    int bl = 0, bl2 = 0;
+    cudaFuncSetAttribute(k_attract<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_attract<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bl, k_attract<false>, 256, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bl2, k_attract<true>, 256, smem);
+    bl = bl2 < bl ? bl2 : bl;
+    return nsm * (bl < 1 ? 1 : bl);
+}
+
+void launch_attract(const Buffers &b, const Params &p, const AttractPlan &plan, int grid,
+                    cudaStream_t s) {
     if (plan.nblocks == 0) return;
-    k_attract<<<plan.nblocks, 256, 0, s>>>(plan, b.pos, b.mass, b.csr_off, b.csr_col4, b.fag, p);
+    const int hub_n = attract_hub_nodes(b.n);
+    const size_t smem = sizeof(float2) * (size_t)hub_n;
+    if (grid > plan.nblocks) grid = plan.nblocks;
+    if (p.linlog)
+        k_attract<true><<<grid, 256, smem, s>>>(plan, b.pos, b.mass, b.csr_off, b.csr_col4, b.fag,
+                                                p, &b.ctr->attract_ticket, hub_n);
+    else
+        k_attract<false><<<grid, 256, smem, s>>>(plan, b.pos, b.mass, b.csr_off, b.csr_col4, b.fag,
+                                                 p, &b.ctr->attract_ticket, hub_n);
 }
 
 void launch_scatter_xy(int n, const uint32_t *ref_of, const float2 *src_ref, float2 *dst_int,

@@ -22,7 +22,7 @@ namespace {
 
 constexpr uint32_t kMaxBodies = FA2_NOALLOC_MAX_BODIES;
 // nodes of the quadtree: at most 33 per body (the bound fa2_create allocates)
-// plus the traversal's sentinel slot
+// plus one spare slot
 constexpr uint64_t kMaxNodes = 33ull * kMaxBodies + 64;
 constexpr int kMaxSMs = 256;  // k_bbox runs 2 blocks per SM, k_displace is not run
 constexpr int kMaxDevices = 64;
@@ -158,6 +158,7 @@ int run(const float *d_xy, const float *d_mass, uint32_t n, const fa2_params *pr
     kp.itolsq = 1.0f / (prm->theta * prm->theta);  // src/RPForceAtlas2.cpp:47
     kp.epssq = prm->epssq;
     kp.strong_gravity = 0;
+    kp.linlog = 0;
     kp.nsm = d.nsm;
 
     // Must start at zero on every call: the counters, histograms, per-tile

@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(kCountThreads) k_tree_count(
     uint32_t *status,
     LookbackSums *__restrict lb, uint32_t *__restrict vals, float2 *__restrict pos,
     const float *__restrict mass, const uint32_t *__restrict ref_of,
-    long long *__restrict pm, i128 *__restrict pxy, float4 *__restrict nodes) {
+    long long *__restrict pm, i128 *__restrict pxy) {
     __shared__ int s_tile;
     __shared__ NodeSums s_warp[kCountThreads / kWarp];
     __shared__ NodeSums s_prefix;
@@ -366,11 +366,6 @@ __global__ void __launch_bounds__(kCountThreads) k_tree_count(
             pxy[2 * (size_t)n] = off.x;
             pxy[2 * (size_t)n + 1] = off.y;
             st->tree_nodes = off.g;
-            // the traversal's sentinel after the last node (slot capacity
-            // exists for it): a NaN position no lane accepts
-            if (off.g <= capacity)
-                nodes[off.g] = make_float4(__int_as_float(0x7fc00000), __int_as_float(0x7fc00000),
-                                           0.0f, 0.0f);
             st->max_level = 0;     // raised by k_emit
             st->interactions = 0;  // counted by k_traverse
             st->visits = 0;
@@ -499,7 +494,7 @@ void launch_tree_count(const Buffers &b, cudaStream_t s) {
     k_tree_count<<<count_tiles(b.n), kCountThreads, 0, s>>>(
         b.n, b.keys[0], b.lcp, b.group, b.owner, b.capacity, b.st, b.ctr, b.count_status,
         b.lookback,
-        b.vals[0], b.pos, b.mass, b.ref_of, b.pm, reinterpret_cast<i128 *>(b.pxy), b.nodes);
+        b.vals[0], b.pos, b.mass, b.ref_of, b.pm, reinterpret_cast<i128 *>(b.pxy));
 }
 
 void launch_emit(const Buffers &b, int nsm, cudaStream_t s) {

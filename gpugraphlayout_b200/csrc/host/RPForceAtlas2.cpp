@@ -97,6 +97,13 @@ namespace RPGraph
 
     void CUDAForceAtlas2::push_params()
     {
+        // use_linlog is public in ForceAtlas2; the reference's GPU path
+        // ignores it, this engine honours it (linear-log attraction)
+        if (use_linlog != applied_linlog)
+        {
+            check(fa2_set_linlog(ctx, use_linlog ? 1 : 0), "setting linlog");
+            applied_linlog = use_linlog;
+        }
         if (k_r == applied_k_r && k_g == applied_k_g) return;
         check(fa2_set_force_params(ctx, k_r, k_g), "setting scale/gravity");
         applied_k_r = k_r;

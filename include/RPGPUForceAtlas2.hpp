@@ -29,6 +29,7 @@ namespace RPGraph
     private:
         fa2_ctx *ctx;
         float applied_k_r, applied_k_g;
+        bool applied_linlog = false;
         void push_params();
         void sendLayoutToGPU();
         void retrieveLayoutFromGPU();

@@ -64,6 +64,10 @@ typedef struct {
     float jitter_tolerance;   /* 1.0 (:40) */
     float k_s_max;            /* 10.0 (:43) */
     int32_t device;           /* CUDA device ordinal */
+    int32_t linlog;           /* 1: linear-log attraction, f_a = log(1 + d) (use_linlog,
+                                 src/RPForceAtlas2.hpp:44; honoured by the reference's
+                                 CPU path only, src/RPCPUForceAtlas2.cpp:59-67).  0 by
+                                 default, as in the reference (src/RPForceAtlas2.cpp:52) */
 } fa2_params;
 
 /* Fills the reference defaults (weak gravity, gravity 1, scale 1). */
@@ -142,6 +146,18 @@ int fa2_get_speed_state(fa2_ctx *ctx, float *global_speed, float *speed_efficien
 /* Changes k_r and k_g between steps: ForceAtlas2::setScale / setGravity
  * (src/RPForceAtlas2.cpp:64-72), which the reference passes to every launch. */
 int fa2_set_force_params(fa2_ctx *ctx, float scale, float gravity);
+
+/* Switches between linear (0) and linear-log (1) attraction between steps:
+ * fa2_params.linlog after creation.  No counterpart on the reference's GPU
+ * path, which ignores ForceAtlas2::use_linlog. */
+int fa2_set_linlog(fa2_ctx *ctx, int32_t enable);
+
+/* Measurement hook, no reference counterpart.  enable = 1 (the default) runs
+ * the attraction on a second stream beside the tree build, the two sharing
+ * the GPU; enable = 0 runs it alone before the tree build, so that the
+ * per-kernel times of fa2_step_timed are those of each kernel on its own.
+ * Results are the same either way. */
+int fa2_set_overlap(fa2_ctx *ctx, int32_t enable);
 
 /* ------------------------------------------------------------------------
  * Repulsion without allocation.  No counterpart in the reference: there the

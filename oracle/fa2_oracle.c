@@ -11,6 +11,7 @@
 #define _DEFAULT_SOURCE
 #include "fa2_oracle.h"
 
+#include <float.h>
 #include <math.h>
 #include <pthread.h>
 #include <unistd.h>
@@ -186,6 +187,27 @@ void orc_attraction(int64_t n_edges, const int32_t *sources, const int32_t *targ
         fy[s] += dy;
         fx[t] += -dx;
         fy[t] += -dy;
+    }
+}
+
+/* Linear-log attraction, use_linlog in the reference's CPU path
+ * (RPCPUForceAtlas2.cpp:55-78): per edge the distance vector p_t - p_s times
+ * log(1 + d) / d, with d = 0 taken as FLT_MAX; added to s and subtracted
+ * from t, in the edge order of the linear form above. */
+void orc_attraction_linlog(int64_t n_edges, const int32_t *sources, const int32_t *targets,
+                           const float *xy, float *fx, float *fy) {
+    for (int64_t e = 0; e < n_edges; ++e) {
+        const int32_t s = sources[e], t = targets[e];
+        const float ex = xy[2 * s] - xy[2 * t];
+        const float ey = xy[2 * s + 1] - xy[2 * t + 1];
+        const float dist = sqrtf(ex * ex + ey * ey);
+        const float w = dist == 0.0f ? FLT_MAX : logf(1 + dist) / dist;
+        const float dx = xy[2 * t] - xy[2 * s];
+        const float dy = xy[2 * t + 1] - xy[2 * s + 1];
+        fx[s] += dx * w;
+        fy[s] += dy * w;
+        fx[t] += dx * -w;
+        fy[t] += dy * -w;
     }
 }
 
@@ -668,7 +690,10 @@ int32_t orc_fa2_step(orc_fa2 *s) {
     const int32_t n = s->n;
     /* fx, fy are zero here: the previous displacement cleared them. */
     orc_gravity(n, s->xy, s->mass, s->k_g, s->strong_gravity, s->fx, s->fy);
-    orc_attraction(s->m, s->sources, s->targets, s->xy, s->fx, s->fy);
+    if (s->linlog)
+        orc_attraction_linlog(s->m, s->sources, s->targets, s->xy, s->fx, s->fy);
+    else
+        orc_attraction(s->m, s->sources, s->targets, s->xy, s->fx, s->fy);
     if (s->f_ga_out)
         for (int32_t i = 0; i < n; ++i) {
             s->f_ga_out[2 * i] = s->fx[i];

@@ -57,6 +57,8 @@ void orc_gravity(int32_t n, const float *xy, const float *mass, float k_g,
 
 /* AttractiveForceKernel (src/RPFA2Kernels.cu:75-109) with its atomics applied
  * in edge order; adds to fx, fy. */
+void orc_attraction_linlog(int64_t n_edges, const int32_t *sources, const int32_t *targets,
+                           const float *xy, float *fx, float *fy);
 void orc_attraction(int64_t n_edges, const int32_t *sources, const int32_t *targets,
                     const float *xy, float *fx, float *fy);
 
@@ -160,6 +162,7 @@ typedef struct {
      * 1, as maxdepthd starts), the others describe the last step */
     int32_t maxdepth, n_perturbed, depth_overflow;
     float swg_sum, etra_sum;
+    int32_t linlog;                     /* 1: linear-log attraction */
 } orc_fa2;
 
 /* One CUDAForceAtlas2::doStep (src/RPGPUForceAtlas2.cu:206-248) in its kernel

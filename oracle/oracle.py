@@ -44,6 +44,7 @@ def lib():
         L.orc_random_positions.argtypes = [C.c_int32, C.c_float, C.c_float, C.c_uint32, _f32p]
         L.orc_gravity.argtypes = [C.c_int32, _f32p, _f32p, C.c_float, C.c_int32, _f32p, _f32p]
         L.orc_attraction.argtypes = [C.c_int64, _i32p, _i32p, _f32p, _f32p, _f32p]
+        L.orc_attraction_linlog.argtypes = [C.c_int64, _i32p, _i32p, _f32p, _f32p, _f32p]
         L.orc_tree_build.restype = C.c_void_p
         L.orc_tree_build.argtypes = [C.c_int32, _f32p, C.POINTER(C.c_int32)]
         L.orc_tree_free.argtypes = [C.c_void_p]
@@ -110,13 +111,14 @@ def random_positions(n: int, width: float, height: float, seed: int = 1234) -> n
 
 # ---------------------------------------------------------------- pieces --
 
-def gravity_attraction(g: Graph, xy: np.ndarray, k_g: float, strong: bool):
+def gravity_attraction(g: Graph, xy: np.ndarray, k_g: float, strong: bool, linlog: bool = False):
     n = g.n
     fx = np.zeros(n, np.float32)
     fy = np.zeros(n, np.float32)
     p = np.ascontiguousarray(xy, np.float32).reshape(-1)
     lib().orc_gravity(n, p, g.mass, k_g, int(strong), fx, fy)
-    lib().orc_attraction(g.m, g.sources, g.targets, p, fx, fy)
+    attract = lib().orc_attraction_linlog if linlog else lib().orc_attraction
+    attract(g.m, g.sources, g.targets, p, fx, fy)
     return np.stack([fx, fy], 1)
 
 
@@ -206,14 +208,15 @@ class _OrcFa2(C.Structure):
         ("jitter_tolerance", C.c_float), ("k_s_max", C.c_float),
         ("sortd_out", C.c_void_p), ("f_ga_out", C.c_void_p), ("f_tot_out", C.c_void_p),
         ("maxdepth", C.c_int32), ("n_perturbed", C.c_int32), ("depth_overflow", C.c_int32),
-        ("swg_sum", C.c_float), ("etra_sum", C.c_float),
+        ("swg_sum", C.c_float), ("etra_sum", C.c_float), ("linlog", C.c_int32),
     ]
 
 
 class FA2:
     """The reference GPU path's iteration (CUDAForceAtlas2::doStep) restated on the CPU."""
 
-    def __init__(self, g: Graph, xy: np.ndarray, k_r: float, k_g: float, strong_gravity: bool):
+    def __init__(self, g: Graph, xy: np.ndarray, k_r: float, k_g: float, strong_gravity: bool,
+                 linlog: bool = False):
         self.g = g
         n = g.n
         self.xy = np.ascontiguousarray(xy, np.float32).reshape(-1).copy()
@@ -237,6 +240,7 @@ class FA2:
         s.f_ga_out = self.f_ga.ctypes.data
         s.f_tot_out = self.f_tot.ctypes.data
         s.maxdepth = 1
+        s.linlog = int(linlog)
         self.s = s
 
     def step(self, iters: int = 1):
@@ -299,6 +303,7 @@ def ref_cpu():
         L.refcpu_fa2_forces.argtypes = [vp, _f32p, _f32p]
         L.refcpu_fa2_set_forces.argtypes = [vp, _f32p, _f32p]
         L.refcpu_fa2_update_speeds.argtypes = [vp]
+        L.refcpu_fa2_set_linlog.argtypes = [vp, C.c_int]
         L.refcpu_fa2_write.argtypes = [vp, C.c_char_p, C.c_int]
         _ref_cpu = L
     return _ref_cpu
@@ -360,6 +365,9 @@ class RefCPUFA2:
 
     def step(self, iters: int = 1):
         ref_cpu().refcpu_fa2_step(self._p, iters)
+
+    def set_linlog(self, on: bool):
+        ref_cpu().refcpu_fa2_set_linlog(self._p, int(on))
 
     def forces(self):
         n = self.g.n

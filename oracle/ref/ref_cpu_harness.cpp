@@ -164,6 +164,9 @@ void refcpu_fa2_set_forces(void *p, const float *f, const float *f_prev) {
 
 void refcpu_fa2_update_speeds(void *p) { ((RefFa2 *)p)->fa2->updateSpeeds(); }
 
+/* ForceAtlas2::use_linlog, public in the reference (RPForceAtlas2.hpp:44). */
+void refcpu_fa2_set_linlog(void *p, int on) { ((RefFa2 *)p)->fa2->use_linlog = on != 0; }
+
 /* GraphLayout::writeToCSV / writeToBin (RPGraphLayout.cpp:209-250). */
 void refcpu_fa2_write(void *p, const char *path, int binary) {
     RefFa2 *r = (RefFa2 *)p;

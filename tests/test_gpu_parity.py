@@ -95,3 +95,43 @@ def test_walk_visits_match_oracle(ba3k):
     assert not ovf and visits > 0
     assert abs(st["visits"] - visits) <= 1e-3 * visits, (st["visits"], visits)
     assert 0 < st["interactions"] < st["visits"]
+
+
+@pytest.mark.parametrize("sg,k_r", [(True, 10.0), (False, 80.0)])
+def test_linlog_step_matches_oracle(ba3k, sg, k_r):
+    """Linear-log attraction (the reference's CPU use_linlog rule, pinned
+    against its own code on the CPU) on the GPU, at the tolerances of the
+    linear form."""
+    from gpugraphlayout_b200 import Engine
+    from oracle import oracle as O
+    g = ba3k
+    xy = O.random_positions(g.n, 2000, 2000, 1234)
+    e = Engine(g.n, g.sources, g.targets, strong_gravity=sg, gravity=1.0, scale=k_r, linlog=True)
+    e.set_positions(xy)
+    fo = O.FA2(g, xy, k_r, 1.0, sg, linlog=True)
+    e.step(1)
+    fo.step(1)
+    assert np.array_equal(e.sort_order(), fo.sortd.astype(np.uint32))
+    tot, ga = e.forces()
+    assert rel_rmse(ga, fo.f_ga.reshape(-1, 2)) <= GA_TOL
+    assert rel_rmse(tot, fo.f_tot.reshape(-1, 2)) <= TOT_TOL
+    assert rel_rmse(e.get_positions(), fo.positions) <= 1e-5
+
+
+def test_linlog_switches_between_steps(ba3k):
+    """fa2_set_linlog between steps: linear, then linear-log, then linear."""
+    from oracle import oracle as O
+    g = ba3k
+    xy = O.random_positions(g.n, 2000, 2000, 5)
+    e = _engine(g, xy, 10.0, 1.0, True)
+    fo = O.FA2(g, xy, 10.0, 1.0, True)
+    for linlog in (False, True, False):
+        e.set_linlog(linlog)
+        fo.s.linlog = int(linlog)
+        before = e.get_positions()
+        e.step(1)
+        fo.step(1)
+        _, ga = e.forces()
+        ga_ref = O.gravity_attraction(g, before, 1.0, True, linlog=linlog)
+        assert rel_rmse(ga, ga_ref) <= GA_TOL, linlog
+    assert rel_rmse(e.get_positions(), fo.positions) <= 1e-3

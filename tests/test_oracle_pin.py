@@ -241,6 +241,28 @@ def test_gravity_attraction_formulas_match_reference_cpu(tmp_path):
         del ref
 
 
+def test_linlog_attraction_matches_reference_cpu(tmp_path):
+    """The linear-log attraction of the reference's CPU path (use_linlog,
+    RPCPUForceAtlas2.cpp:59-67; the GPU path ignores the flag) against the
+    oracle's restatement, with gravity, on layouts whose edges span short and
+    long distances; summation order differs."""
+    from gpugraphlayout_b200 import synth
+    s, t = synth.ba_edges(1000, 3, seed=5)
+    path = str(tmp_path / "g.txt")
+    synth.write_edgelist(path, s, t)
+    rg = O.RefGraph(path)
+    og = O.Graph(s, t)
+    for sg, width in ((True, 2000.0), (False, 3.0)):
+        ref = O.RefCPUFA2(rg, width, width, 1234, True, sg, 1.0, 10.0)
+        ref.set_linlog(True)
+        ga_ref, _ = ref.forces()
+        ga = O.gravity_attraction(og, ref.positions(), 1.0, sg, linlog=True)
+        lin = O.gravity_attraction(og, ref.positions(), 1.0, sg, linlog=False)
+        assert rel_rmse(ga, ga_ref) < 1e-6
+        assert rel_rmse(lin, ga_ref) > 1e-2  # the flag changes the forces
+        del ref
+
+
 def test_speed_rule_matches_reference_cpu(tmp_path):
     """The global-speed update (RPFA2Kernels.cu:177-219 = RPCPUForceAtlas2.cpp:144-197)."""
     g = O.Graph(np.array([0, 1], np.uint32), np.array([1, 2], np.uint32))
