@@ -49,7 +49,7 @@ struct fa2_ctx {
     size_t scratch_bytes = 0;
     float2 *stage_xy = nullptr;    // n, reference order
     uint32_t *stage_ids = nullptr; // n
-    int bbox_blocks = 0, trav_blocks = 0, attract_grid = 0;
+    int bbox_blocks = 0, trav_blocks = 0;
     cudaStream_t sA = nullptr, sB = nullptr;
     cudaEvent_t evFork = nullptr, evJoin = nullptr;
     // graphs
@@ -189,13 +189,13 @@ void enqueue_iteration(fa2_ctx *c, bool full, bool perturb_first, bool timed) {
     cudaMemsetAsync(c->scratch, 0, c->scratch_bytes, A);
     if (full && !c->overlap) {
         mark(S_ATTRACT, 0, A);
-        launch_attract(b, c->kp, c->plan, c->attract_grid, A);
+        launch_attract(b, c->kp, c->plan, A);
         mark(S_ATTRACT, 1, A);
     } else if (full) {
         cudaEventRecord(c->evFork, A);
         cudaStreamWaitEvent(B, c->evFork, 0);
         mark(S_ATTRACT, 0, B);
-        launch_attract(b, c->kp, c->plan, c->attract_grid, B);
+        launch_attract(b, c->kp, c->plan, B);
         mark(S_ATTRACT, 1, B);
         cudaEventRecord(c->evJoin, B);
     }
@@ -468,7 +468,6 @@ fa2_ctx *fa2_create(const fa2_graph_desc *g, const fa2_params *prm, int *status)
         if (cudaEventCreate(&e) != cudaSuccess) return fail(FA2_ERR_CUDA);
     sort_set_smem_attr();
     c->trav_blocks = c->nsm * traverse_blocks_per_sm();
-    c->attract_grid = attract_grid((int)n, c->nsm);
 
     cudaStream_t A = c->sA;
     if (cudaMemcpyAsync(d_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice, A) ||

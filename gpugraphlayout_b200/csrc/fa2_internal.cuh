@@ -54,8 +54,7 @@ struct IterCounters {
     unsigned trav_ticket;
     unsigned trav_done;
     unsigned disp_done;
-    unsigned attract_ticket;
-    unsigned pad[2];
+    unsigned pad[3];
     unsigned hist[8][256];  // per-pass digit histograms of the sort keys
 };
 
@@ -94,8 +93,6 @@ struct AttractBucket {
 };
 constexpr int kMaxBuckets = 8;
 constexpr int kAttractBatch = 4;  // row groups per warp in short-row buckets
-constexpr int kHubNodes = 6144;   // highest-degree nodes whose positions the attraction
-                                  // keeps in shared memory (48 KB)
 struct AttractPlan {
     AttractBucket b[kMaxBuckets];
     int nbuckets;
@@ -161,9 +158,7 @@ void launch_emit(const Buffers &b, int nsm, cudaStream_t s);
 void launch_traverse(const Buffers &b, const Params &p, int nblocks, cudaStream_t s);
 void launch_displace(const Buffers &b, int nsm, cudaStream_t s);
 void launch_count_interactions(const Buffers &b, const Params &p, int nblocks, cudaStream_t s);
-void launch_attract(const Buffers &b, const Params &p, const AttractPlan &plan, int grid,
-                    cudaStream_t s);
-int attract_grid(int n, int nsm);
+void launch_attract(const Buffers &b, const Params &p, const AttractPlan &plan, cudaStream_t s);
 void launch_scatter_xy(int n, const uint32_t *ref_of, const float2 *src_ref, float2 *dst_int,
                        cudaStream_t s);
 void launch_gather_xy(int n, const uint32_t *ref_of, const float2 *src_int, float2 *dst_ref,

@@ -412,16 +412,13 @@ __device__ __forceinline__ float2 pull(float2 q, float2 p) {
     return make_float2(dx, dy);
 }
 
-// Neighbour-position gathers: the first hub_n internal ids, the nodes of
-// highest degree, come from a copy in shared memory (at R-MAT scale 20 the top
-// 6,144 take 40 % of all gathers); the rest through L1/L2.
+// Neighbour-position gathers go through L1, which keeps the positions of the
+// hubs (the first internal ids, gathered most often).  A copy of the hubs in
+// shared memory measured slower: its carve-out took the L1 that the other
+// gathers hit.
 struct Gather {
     const float2 *__restrict pos;
-    const float2 *hub;
-    int hub_n;
-    __device__ __forceinline__ float2 operator()(int c) const {
-        return c < hub_n ? hub[c] : __ldg(&pos[c]);
-    }
+    __device__ __forceinline__ float2 operator()(int c) const { return __ldg(&pos[c]); }
 };
 
 template <bool LINLOG>
@@ -502,21 +499,23 @@ __device__ __forceinline__ void attract_long_row(uint32_t b, uint32_t e, int fir
     for (; q < e; q += STRIDE) add_four<LINLOG>(__ldcs(&col4[q]), p, g, ax, ay);
 }
 
-// One work block of the attraction plan (a row for the block-per-row
-// bucket, 8 rows for the warp-per-row bucket, batches of short rows).
+// The attraction pass: one block per work block of the plan (a row for the
+// block-per-row bucket, 8 rows for the warp-per-row bucket, batches of short
+// rows).
 template <bool LINLOG>
-__device__ __forceinline__ void attract_block(int vb, const AttractPlan &plan, const Gather &g,
-                                              const float *__restrict mass,
-                                              const uint32_t *__restrict off,
-                                              const int4 *__restrict col4,
-                                              float2 *__restrict fag, const Params &prm,
-                                              float2 *s_red) {
+__global__ void __launch_bounds__(256) k_attract(AttractPlan plan, const float2 *__restrict pos,
+                                                 const float *__restrict mass,
+                                                 const uint32_t *__restrict off,
+                                                 const int4 *__restrict col4,
+                                                 float2 *__restrict fag, Params prm) {
+    __shared__ float2 s_red[256 / kWarp];
+    const Gather g{pos};
     int bi = 0;
 #pragma unroll 1
     for (int q = 1; q < plan.nbuckets; ++q)
-        if (vb >= plan.b[q].block_begin) bi = q;
+        if ((int)blockIdx.x >= plan.b[q].block_begin) bi = q;
     const AttractBucket bk = plan.b[bi];
-    const int blk = vb - bk.block_begin;
+    const int blk = blockIdx.x - bk.block_begin;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (bk.lanes == 256) {
         // one row per block
@@ -566,31 +565,6 @@ __device__ __forceinline__ void attract_block(int vb, const AttractPlan &plan, c
         case 4: attract_short_rows<4, LINLOG>(row0, bk.row_end, g, mass, off, col4, fag, prm, lane); break;
         case 2: attract_short_rows<2, LINLOG>(row0, bk.row_end, g, mass, off, col4, fag, prm, lane); break;
         default: attract_short_rows<1, LINLOG>(row0, bk.row_end, g, mass, off, col4, fag, prm, lane); break;
-    }
-}
-
-// The attraction pass: a grid that fills the GPU once, each block copying
-// the hub positions into shared memory and then taking work blocks of the
-// plan from a ticket until none are left.
-template <bool LINLOG>
-__global__ void __launch_bounds__(256) k_attract(AttractPlan plan, const float2 *__restrict pos,
-                                                 const float *__restrict mass,
-                                                 const uint32_t *__restrict off,
-                                                 const int4 *__restrict col4,
-                                                 float2 *__restrict fag, Params prm,
-                                                 unsigned *ticket, int hub_n) {
-    extern __shared__ float2 s_hub[];
-    __shared__ float2 s_red[256 / kWarp];
-    __shared__ int s_vb;
-    for (int i = threadIdx.x; i < hub_n; i += blockDim.x) s_hub[i] = pos[i];
-    const Gather g{pos, s_hub, hub_n};
-    for (;;) {
-        if (threadIdx.x == 0) s_vb = (int)atomicAdd(ticket, 1u);
-        __syncthreads();  // the ticket, and on the first round the hub copy
-        const int vb = s_vb;
-        if (vb >= plan.nblocks) break;
-        attract_block<LINLOG>(vb, plan, g, mass, off, col4, fag, prm, s_red);
-        __syncthreads();  // s_vb and s_red are reused
     }
 }
 
@@ -652,31 +626,14 @@ void launch_count_interactions(const Buffers &b, const Params &p, int nblocks, c
     k_count_interactions<<<nblocks, kTravThreads, 0, s>>>(b.n, b.nodes, b.body_node, b.st, p);
 }
 
-int attract_hub_nodes(int n) { return n < kHubNodes ? n : kHubNodes; }
-
-int attract_grid(int n, int nsm) {
-    const size_t smem = sizeof(float2) * (size_t)attract_hub_nodes(n);
-    int bl = 0, bl2 = 0;
-    cudaFuncSetAttribute(k_attract<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_attract<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bl, k_attract<false>, 256, smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bl2, k_attract<true>, 256, smem);
-    bl = bl2 < bl ? bl2 : bl;
-    return nsm * (bl < 1 ? 1 : bl);
-}
-
-void launch_attract(const Buffers &b, const Params &p, const AttractPlan &plan, int grid,
-                    cudaStream_t s) {
+void launch_attract(const Buffers &b, const Params &p, const AttractPlan &plan, cudaStream_t s) {
     if (plan.nblocks == 0) return;
-    const int hub_n = attract_hub_nodes(b.n);
-    const size_t smem = sizeof(float2) * (size_t)hub_n;
-    if (grid > plan.nblocks) grid = plan.nblocks;
     if (p.linlog)
-        k_attract<true><<<grid, 256, smem, s>>>(plan, b.pos, b.mass, b.csr_off, b.csr_col4, b.fag,
-                                                p, &b.ctr->attract_ticket, hub_n);
+        k_attract<true><<<plan.nblocks, 256, 0, s>>>(plan, b.pos, b.mass, b.csr_off, b.csr_col4,
+                                                     b.fag, p);
     else
-        k_attract<false><<<grid, 256, smem, s>>>(plan, b.pos, b.mass, b.csr_off, b.csr_col4, b.fag,
-                                                 p, &b.ctr->attract_ticket, hub_n);
+        k_attract<false><<<plan.nblocks, 256, 0, s>>>(plan, b.pos, b.mass, b.csr_off, b.csr_col4,
+                                                      b.fag, p);
 }
 
 void launch_scatter_xy(int n, const uint32_t *ref_of, const float2 *src_ref, float2 *dst_int,
