@@ -296,6 +296,121 @@ def run_ours(args, world, rank, local):
     print(json.dumps(out))
 
 
+# ---------------------------------------------------------------- batched --
+
+BATCH_GRAPHS = 4096
+BATCH_METRIC = ("FA2 batch iters/s: 4096 SBM graphs (nodes log-uniform 50-20000) "
+                "laid out together")
+
+
+def batch_config(graphs, world):
+    n = sum(g[0] for g in graphs)
+    m = sum(len(g[1]) for g in graphs)
+    return {"workload": f"{len(graphs)} stochastic block models, nodes log-uniform in "
+                        "[50, 20000], 2-32 equal blocks, p_in 0.05, p_out 0.002, mean degree "
+                        "capped at 40 (seed 0); positions U[-5000,5000]^2 (srandom per graph); "
+                        "weak gravity, scale 2, gravity 1, theta 1",
+            "graphs": len(graphs), "nodes": n, "edges": m,
+            "l2": f"per-iteration working set ({(16 * n + 8 * m) / 1e6:.0f} MB) larger than L2",
+            "parallelism": f"graphs sharded over {world} rank(s), no collective"}
+
+
+def batch_cpu_baseline(graphs, sample_ids):
+    """The reference's CPU ForceAtlas2 on a sample of the batch's graphs, 2
+    iterations each after 1 untimed; the batch's time per iteration is
+    extrapolated from the sample by seconds per node (the sample spans the
+    size range)."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        return None
+    t_sum, n_sum = 0.0, 0
+    for i in sample_ids:
+        n, lo, hi = graphs[i]
+        g = O.Graph(lo, hi)
+        ref = O.RefCPUFA2(O.RefGraph(graph=g), 10000.0, 10000.0, 1234, True, False, 1.0, 2.0)
+        ref.step(1)
+        t0 = time.perf_counter()
+        ref.step(2)
+        t_sum += (time.perf_counter() - t0) / 2
+        n_sum += g.n
+        del ref
+    total_n = sum(g[0] for g in graphs)
+    per_iter = t_sum / n_sum * total_n
+    return {"value": 1.0 / per_iter, "unit": "batch iters/s", "cores": 1, "kind": "reference",
+            "sample": f"2 iterations of CPUForceAtlas2::doStep (1 thread) on {len(sample_ids)} of "
+                      f"the graphs ({n_sum} nodes), extrapolated by seconds per node to all "
+                      f"{total_n} nodes"}
+
+
+def run_batched(args, world, rank, local):
+    import torch
+    from gpugraphlayout_b200 import BatchEngine, random_positions, shard, synth
+    graphs = synth.sbm_batch(BATCH_GRAPHS, seed=0)
+    parts = shard.partition(shard.graph_costs(graphs), world)
+    mine = parts[rank]
+    eng = BatchEngine([graphs[i] for i in mine], strong_gravity=False, gravity=1.0, scale=2.0,
+                      device=local)
+    xy = np.concatenate([random_positions(graphs[i][0], 10000.0, 10000.0, 1234 + i)
+                         for i in mine]) if mine else np.zeros((0, 2), np.float32)
+    eng.set_positions(xy)
+    torch.cuda.set_device(local)
+    eng.step(max(args.warmup, 3))
+    clk_path = os.path.join(tempfile.gettempdir(), f"fa2_clocks_b{rank}.csv")
+    sampler = clocks_sampler(local, clk_path)
+    time.sleep(0.3)
+    barrier(world)
+    torch.cuda.synchronize()
+    ms = eng.step_timed(args.steps)
+    torch.cuda.synchronize()
+    barrier(world)
+    if sampler:
+        sampler.terminate()
+        sampler.wait()
+    ms_max = barrier_max(world, ms)
+    value = args.steps / (ms_max / 1000.0)
+
+    # end to end through the C ABI: positions in, one iteration, positions out
+    host = np.ascontiguousarray(eng.get_positions())
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        eng.set_positions(host)
+        eng.step(1)
+        host = eng.get_positions()
+    e2e = args.steps / barrier_max(world, time.perf_counter() - t0)
+    if rank != 0:
+        return
+    pk, pk_kind = peaks()
+    hbm = float(pk["hbm_gbs"])
+    n_all = sum(g[0] for g in graphs)
+    m_all = sum(len(g[1]) for g in graphs)
+    # compulsory bytes of one iteration of every graph: CSR ids (2 per edge),
+    # offsets, positions and previous forces read and written, mass
+    bytes_iter = 8 * m_all + 4 * n_all + 16 * n_all + 16 * n_all + 4 * n_all
+    achieved = bytes_iter * value / 1e9
+    out = {
+        "metric": BATCH_METRIC, "value": value, "unit": "batch iters/s", "n_gpus": world,
+        "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": batch_config(graphs, world),
+        "graph_iters_per_s": value * len(graphs),
+        "clocks": clocks_summary(clk_path),
+        "gpu_launches": args.steps,
+        "e2e": {"value": e2e, "unit": "batch iters/s", "h2d_bytes_per_step": 8 * n_all // world,
+                "d2h_bytes_per_step": 8 * n_all // world},
+        "roofline": {"kernel": "batch", "bound": "hbm", "achieved": achieved, "peak": hbm,
+                     "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                     "note": f"peak = {pk_kind} HBM copy bandwidth; achieved = compulsory bytes "
+                             "of one iteration of every graph / time; the per-graph pipeline is "
+                             "latency-bound (one CTA per graph), so this is a lower bound"},
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        sizes = np.array([g[0] for g in graphs])
+        sample = [int(i) for i in np.argsort(sizes)[:: len(graphs) // 8][:8]]
+        out["cpu_baseline"] = batch_cpu_baseline(graphs, sample)
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -303,10 +418,20 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="rmat20", choices=["rmat20", "batched"],
+                    help="rmat20: the R-MAT scale-20 graph (default); batched: 4096 SBM graphs")
     args = ap.parse_args()
     world, rank, local = dist_setup(args.gpus)
     try:
-        if args.impl == "reference":
+        if args.workload == "batched":
+            if args.impl == "reference":
+                if rank == 0:
+                    print(json.dumps({"impl": "reference", "unavailable": "the batched workload "
+                                      "has no reference arm; its cpu_baseline is in the "
+                                      "default arm's line"}))
+            else:
+                run_batched(args, world, rank, local)
+        elif args.impl == "reference":
             run_reference(args, world, rank)
         else:
             run_ours(args, world, rank, local)

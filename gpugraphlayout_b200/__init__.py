@@ -23,7 +23,7 @@ import numpy as np
 
 from ._native import Fa2Error, GraphDesc, Params, Stats, check, lib
 
-__all__ = ["Engine", "UGraph", "GraphLayout", "CUDAForceAtlas2", "Fa2Error", "kernel_names",
+__all__ = ["Engine", "BatchEngine", "UGraph", "GraphLayout", "CUDAForceAtlas2", "Fa2Error", "kernel_names",
            "random_positions"]
 
 
@@ -157,6 +157,86 @@ class Engine:
         fp = None if f_prev is None else np.ascontiguousarray(f_prev, np.float32).reshape(self.n, 2)
         check(lib().fa2_set_speed_state(self._ctx, global_speed, speed_efficiency, _ptr(fp)),
               "fa2_set_speed_state")
+
+
+class BatchEngine:
+    """One fa2_batch: many independent graphs laid out together, each with the
+    FA2 iteration of Engine and its own quadtree and speed state.
+
+    ``graphs`` is a sequence of (num_nodes, sources, targets) with graph-local
+    ids.  Positions and forces are (total nodes, 2) arrays, graph after graph."""
+
+    def __init__(self, graphs, *, strong_gravity: bool = False, gravity: float = 1.0,
+                 scale: float = 1.0, theta: float = 1.0, epssq: float = 0.05 * 0.05,
+                 device: int = 0, linlog: bool = False):
+        L = lib()
+        self._keep = []
+        descs = (GraphDesc * max(1, len(graphs)))()
+        self.sizes = []
+        for i, (n, s, t) in enumerate(graphs):
+            s = np.ascontiguousarray(s, np.uint32)
+            t = np.ascontiguousarray(t, np.uint32)
+            self._keep += [s, t]
+            descs[i] = GraphDesc(int(n), len(s), _ptr(s), _ptr(t))
+            self.sizes.append(int(n))
+        p = Params()
+        L.fa2_default_params(C.byref(p))
+        p.strong_gravity = int(strong_gravity)
+        p.gravity, p.scale, p.theta, p.epssq, p.device = gravity, scale, theta, epssq, device
+        p.linlog = int(linlog)
+        st = C.c_int(0)
+        self._b = L.fa2_batch_create(len(graphs), descs, C.byref(p), C.byref(st))
+        check(st.value, "fa2_batch_create")
+        self.num_graphs = len(graphs)
+        self.offsets = np.concatenate([[0], np.cumsum(self.sizes)]).astype(np.int64)
+        self.n = int(self.offsets[-1])
+
+    def close(self):
+        if getattr(self, "_b", None):
+            lib().fa2_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        self.close()
+
+    def set_positions(self, xy) -> None:
+        a = np.ascontiguousarray(xy, np.float32).reshape(self.n, 2)
+        check(lib().fa2_batch_set_positions(self._b, _ptr(a)), "fa2_batch_set_positions")
+
+    def get_positions(self) -> np.ndarray:
+        out = np.zeros((self.n, 2), np.float32)
+        check(lib().fa2_batch_get_positions(self._b, _ptr(out)), "fa2_batch_get_positions")
+        return out
+
+    def step(self, n_iters: int = 1) -> None:
+        check(lib().fa2_batch_step(self._b, int(n_iters)), "fa2_batch_step")
+
+    def step_timed(self, n_iters: int) -> float:
+        ms = C.c_float(0.0)
+        check(lib().fa2_batch_step_timed(self._b, int(n_iters), C.byref(ms)),
+              "fa2_batch_step_timed")
+        return ms.value
+
+    def forces(self):
+        tot = np.zeros((self.n, 2), np.float32)
+        ga = np.zeros((self.n, 2), np.float32)
+        check(lib().fa2_batch_get_forces(self._b, _ptr(tot), _ptr(ga)), "fa2_batch_get_forces")
+        return tot, ga
+
+    def sort_order(self) -> np.ndarray:
+        out = np.zeros(max(1, self.n), np.uint32)
+        check(lib().fa2_batch_get_sort_order(self._b, _ptr(out)), "fa2_batch_get_sort_order")
+        return out[: self.n]
+
+    def speeds(self):
+        gs = np.zeros(max(1, self.num_graphs), np.float32)
+        se = np.zeros(max(1, self.num_graphs), np.float32)
+        check(lib().fa2_batch_get_speed(self._b, _ptr(gs), _ptr(se)), "fa2_batch_get_speed")
+        return gs[: self.num_graphs], se[: self.num_graphs]
+
+    def part(self, a, g: int):
+        """Rows of graph g in a batch-ordered array."""
+        return a[self.offsets[g]:self.offsets[g + 1]]
 
 
 class UGraph:

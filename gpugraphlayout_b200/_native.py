@@ -17,7 +17,10 @@ EXPORTS = (
     "fa2_default_params", "fa2_create", "fa2_destroy", "fa2_set_positions",
     "fa2_get_positions", "fa2_step", "fa2_step_timed", "fa2_kernel_name",
     "fa2_get_stats", "fa2_get_forces", "fa2_get_sort_order", "fa2_set_speed_state",
-    "fa2_get_speed_state", "fa2_set_force_params", "fa2_set_linlog", "fa2_set_overlap", "fa2_repulsion_noalloc", "fa2_ugraph_load",
+    "fa2_get_speed_state", "fa2_set_force_params", "fa2_set_linlog", "fa2_set_overlap",
+    "fa2_batch_create", "fa2_batch_destroy", "fa2_batch_set_positions", "fa2_batch_get_positions",
+    "fa2_batch_step", "fa2_batch_step_timed", "fa2_batch_get_forces", "fa2_batch_get_sort_order",
+    "fa2_batch_get_speed", "fa2_repulsion_noalloc", "fa2_ugraph_load",
     "fa2_ugraph_from_pairs", "fa2_ugraph_free", "fa2_ugraph_num_nodes",
     "fa2_ugraph_num_edges", "fa2_ugraph_node_map_r", "fa2_ugraph_degrees",
     "fa2_ugraph_edges", "fa2_random_positions", "fa2_write_layout",
@@ -26,6 +29,7 @@ EXPORTS = (
 
 FA2_OK = 0
 FA2_NOALLOC_MAX_BODIES = 8192  # include/fa2b200.h
+FA2_BATCH_MAX_NODES = 65536    # include/fa2b200.h
 STATUS_NAMES = {
     0: "FA2_OK", 1: "FA2_ERR_INVALID_ARGUMENT", 2: "FA2_ERR_NO_DEVICE", 3: "FA2_ERR_CUDA",
     4: "FA2_ERR_OUT_OF_MEMORY", 5: "FA2_ERR_DEVICE_LIMIT", 6: "FA2_ERR_TOO_LARGE",
@@ -96,6 +100,16 @@ def lib():
     L.fa2_set_force_params.argtypes = [vp, C.c_float, C.c_float]
     L.fa2_set_overlap.argtypes = [vp, C.c_int32]
     L.fa2_set_linlog.argtypes = [vp, C.c_int32]
+    L.fa2_batch_create.restype = vp
+    L.fa2_batch_create.argtypes = [C.c_uint32, vp, C.POINTER(Params), ip]
+    L.fa2_batch_destroy.argtypes = [vp]
+    L.fa2_batch_set_positions.argtypes = [vp, vp]
+    L.fa2_batch_get_positions.argtypes = [vp, vp]
+    L.fa2_batch_step.argtypes = [vp, C.c_int32]
+    L.fa2_batch_step_timed.argtypes = [vp, C.c_int32, f32p]
+    L.fa2_batch_get_forces.argtypes = [vp, vp, vp]
+    L.fa2_batch_get_sort_order.argtypes = [vp, vp]
+    L.fa2_batch_get_speed.argtypes = [vp, vp, vp]
     L.fa2_repulsion_noalloc.argtypes = [vp, vp, C.c_uint32, C.POINTER(Params), vp, vp]
     L.fa2_ugraph_load.restype = vp
     L.fa2_ugraph_load.argtypes = [C.c_char_p, ip]

@@ -1,0 +1,986 @@
+// fa2_batch.cu -- many independent graphs laid out in one persistent launch.
+//
+// Each graph is small next to the GPU (tens to tens of thousands of nodes),
+// so one CTA runs the whole ForceAtlas2 iteration of one graph: gravity and
+// attraction, bounding box, Morton keys, a block-level radix sort, the tree
+// (counts, prefix sums, nodes), the warp-vote traversal, the speed rule and
+// the displacement -- the same arithmetic as the single-graph kernels, with
+// every reduction and scan inside the block.  No CTA waits on another.  The
+// CTAs of a grid that fills the GPU take graphs from a queue, largest first,
+// and run `iters` iterations of a graph before taking the next, so a graph's
+// working set stays in L2 across its iterations.  Per-CTA scratch lives in
+// one slot per CTA, sized for the largest graph of the batch.
+//
+// The reference has no batched mode: it lays out one graph per process, with
+// its speed and tree state in device statics (src/RPFA2Kernels.cu:29-33,
+// src/RPBHKernels.cu:54-62), so a batch is a sequence of separate runs.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <numeric>
+#include <vector>
+
+#include "../../include/fa2b200.h"
+#include "fa2_device.cuh"
+
+namespace fa2 {
+
+namespace {
+
+constexpr int kBThreads = 1024;
+constexpr int kBWarps = kBThreads / kWarp;
+constexpr int kBRounds = 4;                       // keys per thread in a sort chunk
+constexpr int kBChunk = kBThreads * kBRounds;     // keys per sort chunk
+constexpr uint32_t kBatchMaxNodes = FA2_BATCH_MAX_NODES;  // nodes per graph
+constexpr int kErrPoisonRounds = 1 << 9;          // coincident bodies kept reappearing
+
+struct BatchGraph {
+    uint32_t node_base;  // first node of the graph in the batch arrays
+    uint32_t n;          // nodes
+};
+
+struct BatchSpeed {
+    float global_speed, speed_efficiency;
+    int err;             // kErr* bits of this graph; its iterations stop
+    int perturb_rounds;  // .99 re-insertion rounds of its last iteration
+};
+
+// Offsets of one CTA's scratch slot, in bytes, each 256-byte aligned.
+struct SlotLayout {
+    size_t keys0, keys1, vals0, vals1, lcp, group, body_node, owner, nodes, pm, pxy, fa, f, gpart;
+    size_t bytes;
+    uint32_t cap;  // tree nodes a slot holds
+};
+
+struct BatchArgs {
+    const BatchGraph *graphs;
+    const uint32_t *order;  // graphs, largest first
+    int num_graphs;
+    float2 *pos, *fprev;
+    const float *mass;
+    const uint32_t *off, *col;  // CSR over batch node ids
+    BatchSpeed *speed;
+    float2 *f_tot, *f_ag;       // last iteration's forces (diagnostics)
+    uint32_t *sortd;            // last iteration's body order, graph-local ids
+    unsigned *queue;
+    char *slots;
+    SlotLayout L;
+    Params prm;
+    float jitter_tolerance, k_s_max;
+    int iters;
+};
+
+struct NodeSums {
+    uint32_t g;
+    long long m;
+    i128 x, y;
+};
+
+__device__ __forceinline__ void sums_add(NodeSums &a, const NodeSums &b) {
+    a.g += b.g;
+    a.m += b.m;
+    a.x += b.x;
+    a.y += b.y;
+}
+
+__device__ __forceinline__ NodeSums shfl_up_sums(const NodeSums &v, int o) {
+    NodeSums t;
+    t.g = __shfl_up_sync(kFullMask, v.g, o);
+    t.m = __shfl_up_sync(kFullMask, v.m, o);
+    t.x = shfl_up_i128(v.x, o);
+    t.y = shfl_up_i128(v.y, o);
+    return t;
+}
+
+// Shared memory of the batch kernel (static part; sort histograms included).
+struct BatchSmem {
+    uint32_t whist[kBWarps][256];
+    uint32_t qsum[4][256];
+    uint32_t base[256];
+    uint32_t coff[256];
+    NodeSums wsum[kBWarps];
+    NodeSums carry;
+    float4 wbox[kBWarps];
+    float dq[64];
+    float2 wred[kBWarps];
+    float rx, ry, radius;
+    uint32_t total_nodes;
+    int ticket;
+    int graph;
+    int err, poison;
+    float gs, se;
+};
+
+// Block-wide exclusive scan of NodeSums; *total receives the block's sum.
+// Every thread of the block calls it.
+__device__ NodeSums block_scan(NodeSums v, BatchSmem &S, NodeSums *total) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    NodeSums inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const NodeSums t = shfl_up_sums(inc, o);
+        if (lane >= o) sums_add(inc, t);
+    }
+    if (lane == 31) S.wsum[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+        NodeSums w = S.wsum[lane], wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const NodeSums t = shfl_up_sums(wi, o);
+            if (lane >= o) sums_add(wi, t);
+        }
+        NodeSums ex = wi;  // exclusive = inclusive - own
+        ex.g -= w.g;
+        ex.m -= w.m;
+        ex.x -= w.x;
+        ex.y -= w.y;
+        S.wsum[lane] = ex;
+        if (lane == 31) S.carry = wi;  // block total, read below before reuse
+    }
+    __syncthreads();
+    NodeSums out = S.wsum[wid];
+    out.g += inc.g - v.g;
+    out.m += inc.m - v.m;
+    out.x += inc.x - v.x;
+    out.y += inc.y - v.y;
+    *total = S.carry;
+    __syncthreads();
+    return out;
+}
+
+template <typename T>
+__device__ __forceinline__ T *slot_ptr(char *slot, size_t off) {
+    return reinterpret_cast<T *>(slot + off);
+}
+
+// --------------------------------------------------------------- phases --
+
+// Gravity + attraction of the graph's nodes (8 lanes per row), into fa.
+template <bool LINLOG>
+__device__ void phase_attract(const BatchArgs &A, uint32_t base, uint32_t n, float2 *fa) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int sub = lane >> 3, l8 = lane & 7;
+    for (uint32_t r0 = (uint32_t)wid * 4; r0 < n; r0 += kBWarps * 4) {
+        const uint32_t row = r0 + (uint32_t)sub;
+        const bool valid = row < n;
+        float ax = 0.0f, ay = 0.0f;
+        float2 p = make_float2(0.0f, 0.0f);
+        if (valid) {
+            p = A.pos[base + row];
+            const uint32_t e1 = A.off[base + row + 1];
+            for (uint32_t e = A.off[base + row] + (uint32_t)l8; e < e1; e += 8) {
+                const float2 q = pull<LINLOG>(A.pos[A.col[e]], p);
+                ax += q.x;
+                ay += q.y;
+            }
+        }
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1) {
+            ax += __shfl_xor_sync(kFullMask, ax, o);
+            ay += __shfl_xor_sync(kFullMask, ay, o);
+        }
+        if (valid && l8 == 0) {
+            const float2 g = with_gravity(p, A.mass[base + row], ax, ay, A.prm);
+            fa[row] = g;
+            A.f_ag[base + row] = g;
+        }
+    }
+}
+
+// Bounding box and root cell of the graph (BoundingBoxKernel,
+// src/RPBHKernels.cu:70-157), into S.rx, S.ry, S.radius.
+__device__ void phase_bbox(const BatchArgs &A, uint32_t base, uint32_t n, BatchSmem &S) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    float4 a = make_float4(FLT_MAX, -FLT_MAX, FLT_MAX, -FLT_MAX);
+    for (uint32_t i = threadIdx.x; i < n; i += kBThreads) {
+        const float2 p = A.pos[base + i];
+        a = make_float4(fminf(a.x, p.x), fmaxf(a.y, p.x), fminf(a.z, p.y), fmaxf(a.w, p.y));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a.x = fminf(a.x, __shfl_xor_sync(kFullMask, a.x, o));
+        a.y = fmaxf(a.y, __shfl_xor_sync(kFullMask, a.y, o));
+        a.z = fminf(a.z, __shfl_xor_sync(kFullMask, a.z, o));
+        a.w = fmaxf(a.w, __shfl_xor_sync(kFullMask, a.w, o));
+    }
+    if (lane == 0) S.wbox[wid] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float4 b = S.wbox[0];
+        for (int w = 1; w < kBWarps; ++w) {
+            const float4 c = S.wbox[w];
+            b = make_float4(fminf(b.x, c.x), fmaxf(b.y, c.y), fminf(b.z, c.z), fmaxf(b.w, c.w));
+        }
+        S.radius = fmaxf(b.y - b.x, b.w - b.z) * 0.5f;
+        S.rx = (b.x + b.y) * 0.5f;
+        S.ry = (b.z + b.w) * 0.5f;
+    }
+    __syncthreads();
+}
+
+// One stable LSD pass over the graph's n keys in chunks of kBChunk: digit
+// histogram, bases, then per chunk a ballot ranking per warp and offsets
+// across warps.
+__device__ void sort_pass(int pass, uint32_t n, const uint64_t *kin, const uint32_t *vin,
+                          uint64_t *kout, uint32_t *vout, BatchSmem &S) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int shift = 8 * pass;
+    const unsigned lt = (1u << lane) - 1u;
+    if (threadIdx.x < 256) S.base[threadIdx.x] = 0;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < n; i += kBThreads)
+        atomicAdd(&S.base[(uint32_t)(kin[i] >> shift) & 255u], 1u);
+    __syncthreads();
+    if (threadIdx.x < 256) {  // exclusive scan of the 256 counts (warps 0..7)
+        const uint32_t c = S.base[threadIdx.x];
+        uint32_t inc = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(kFullMask, inc, o);
+            if (lane >= o) inc += t;
+        }
+        if (lane == 31) S.coff[wid] = inc;
+        __syncwarp();
+        S.qsum[0][threadIdx.x] = inc - c;
+    }
+    __syncthreads();
+    if (threadIdx.x < 256) {
+        uint32_t b = 0;
+        for (int w = 0; w < wid; ++w) b += S.coff[w];
+        S.base[threadIdx.x] = S.qsum[0][threadIdx.x] + b;
+    }
+    __syncthreads();
+    for (uint32_t c0 = 0; c0 < n; c0 += kBChunk) {
+        const uint32_t w0 = c0 + (uint32_t)wid * (kBChunk / kBWarps);
+        uint64_t k[kBRounds];
+        uint32_t v[kBRounds], rank[kBRounds];
+#pragma unroll
+        for (int r = 0; r < kBRounds; ++r) {
+            const uint32_t idx = w0 + (uint32_t)(r * 32 + lane);
+            k[r] = idx < n ? kin[idx] : 0ull;
+            v[r] = idx < n ? vin[idx] : 0u;
+        }
+        for (int j = threadIdx.x; j < kBWarps * 256; j += kBThreads) (&S.whist[0][0])[j] = 0;
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < kBRounds; ++r) {
+            const bool valid = w0 + (uint32_t)(r * 32 + lane) < n;
+            const uint32_t d = (uint32_t)(k[r] >> shift) & 255u;
+            unsigned peers = __ballot_sync(kFullMask, valid);
+            if (!valid) peers = ~peers;
+#pragma unroll
+            for (int b = 0; b < 8; ++b) {
+                const bool bit = (d >> b) & 1u;
+                const unsigned m = __ballot_sync(kFullMask, bit);
+                peers &= bit ? m : ~m;
+            }
+            uint32_t before = 0;
+            if (valid) before = S.whist[wid][d];
+            rank[r] = before + __popc(peers & lt);
+            __syncwarp();
+            if (valid && (peers & lt) == 0) S.whist[wid][d] = before + __popc(peers);
+            __syncwarp();
+        }
+        __syncthreads();
+        // per digit: exclusive offsets across the 32 warps, 4 threads per digit
+        const int dg = threadIdx.x & 255, qt = threadIdx.x >> 8;
+        {
+            uint32_t q = 0;
+#pragma unroll
+            for (int w = 0; w < 8; ++w) q += S.whist[qt * 8 + w][dg];
+            S.qsum[qt][dg] = q;
+        }
+        __syncthreads();
+        {
+            uint32_t run = 0, tot = 0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t c = S.qsum[q][dg];
+                if (q < qt) run += c;
+                tot += c;
+            }
+            run += S.base[dg];
+#pragma unroll
+            for (int w = 0; w < 8; ++w) {
+                const uint32_t c = S.whist[qt * 8 + w][dg];
+                S.whist[qt * 8 + w][dg] = run;
+                run += c;
+            }
+            if (qt == 0) S.coff[dg] = tot;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < kBRounds; ++r) {
+            if (w0 + (uint32_t)(r * 32 + lane) < n) {
+                const uint32_t d = (uint32_t)(k[r] >> shift) & 255u;
+                const uint32_t out = S.whist[wid][d] + rank[r];
+                kout[out] = k[r];
+                vout[out] = v[r];
+            }
+        }
+        if (threadIdx.x < 256) S.base[threadIdx.x] += S.coff[threadIdx.x];
+        __syncthreads();
+    }
+}
+
+// Keys from the positions, the 8 sort passes (ending in keys0/vals0) and the
+// ordering of equal-key runs; returns with S.poison set if exactly
+// coincident bodies were found (perturb = 0) or after scaling them (1).
+__device__ void phase_keys_sort(const BatchArgs &A, uint32_t base, uint32_t n, char *slot,
+                                BatchSmem &S, int perturb) {
+    uint64_t *k0 = slot_ptr<uint64_t>(slot, A.L.keys0), *k1 = slot_ptr<uint64_t>(slot, A.L.keys1);
+    uint32_t *v0 = slot_ptr<uint32_t>(slot, A.L.vals0), *v1 = slot_ptr<uint32_t>(slot, A.L.vals1);
+    const float rx = S.rx, ry = S.ry, rr = S.radius;
+    for (uint32_t i = threadIdx.x; i < n; i += kBThreads) {
+        const float2 p = A.pos[base + i];
+        k0[i] = morton_key(p.x, p.y, rx, ry, rr);
+        v0[i] = i;
+    }
+    __syncthreads();
+    for (int pass = 0; pass < 8; pass += 2) {
+        sort_pass(pass, n, k0, v0, k1, v1, S);
+        sort_pass(pass + 1, n, k1, v1, k0, v0, S);
+    }
+    for (uint32_t k = threadIdx.x; k + 1 < n; k += kBThreads) {
+        if (k0[k + 1] != k0[k] || (k > 0 && k0[k - 1] == k0[k])) continue;
+        fix_run((int)k, (int)n, k0, v0, A.pos + base, nullptr, rx, ry, rr, &S.err, &S.poison,
+                perturb);
+    }
+    __syncthreads();
+}
+
+// Tree count: L[k], preorder indices, owners and the exact prefix sums.
+__device__ void phase_count(const BatchArgs &A, uint32_t base, uint32_t n, char *slot,
+                            BatchSmem &S) {
+    const uint64_t *keys = slot_ptr<uint64_t>(slot, A.L.keys0);
+    const uint32_t *vals = slot_ptr<uint32_t>(slot, A.L.vals0);
+    int8_t *lcp = slot_ptr<int8_t>(slot, A.L.lcp);
+    uint32_t *group = slot_ptr<uint32_t>(slot, A.L.group);
+    uint32_t *owner = slot_ptr<uint32_t>(slot, A.L.owner);
+    long long *pm = slot_ptr<long long>(slot, A.L.pm);
+    i128 *pxy = slot_ptr<i128>(slot, A.L.pxy);
+    const double scale = S.radius > 0.0f ? kFixedScale / (double)S.radius : 1.0;
+    const float rx = S.rx, ry = S.ry;
+    const uint32_t cap = A.L.cap;
+    NodeSums carry{0, 0, 0, 0};
+    for (uint32_t c0 = 0; c0 < n; c0 += kBThreads) {
+        const uint32_t k = c0 + threadIdx.x;
+        NodeSums v{0, 0, 0, 0};
+        long long im = 0, qx = 0, qy = 0;
+        int c = 0;
+        if (k < n) {
+            const int Lk = lcp_at(keys, (int)n, (int)k), Lkm1 = lcp_at(keys, (int)n, (int)k - 1);
+            lcp[k] = (int8_t)Lk;
+            c = cells_at((int)k, Lk, Lkm1);
+            const uint32_t i = vals[k];
+            const float2 p = A.pos[base + i];
+            im = (long long)A.mass[base + i];
+            qx = fixed_offset(p.x, rx, scale);
+            qy = fixed_offset(p.y, ry, scale);
+            v.g = (uint32_t)c + 1u;
+            v.m = im;
+            v.x = (i128)im * qx;
+            v.y = (i128)im * qy;
+        }
+        NodeSums total;
+        NodeSums ex = block_scan(v, S, &total);
+        sums_add(ex, carry);
+        if (k < n) {
+            group[k] = ex.g;
+            pm[k] = ex.m;
+            pxy[2 * (size_t)k] = ex.x;
+            pxy[2 * (size_t)k + 1] = ex.y;
+            for (uint32_t q = 0; q <= (uint32_t)c; ++q) {
+                const uint32_t idx = ex.g + q;
+                if (idx < cap) owner[idx] = (k << 6) | (q < (uint32_t)c ? q : 63u);
+            }
+        }
+        sums_add(carry, total);
+    }
+    if (threadIdx.x == 0) {
+        pm[n] = carry.m;
+        pxy[2 * (size_t)n] = carry.x;
+        pxy[2 * (size_t)n + 1] = carry.y;
+        S.total_nodes = carry.g;
+        if (carry.g > cap) S.err |= kErrTreeTooLarge;
+    }
+    __syncthreads();
+}
+
+// Every node of the tree once (k_emit's rule, one thread per node).
+__device__ void phase_emit(const BatchArgs &A, uint32_t base, uint32_t n, char *slot,
+                           BatchSmem &S) {
+    const uint64_t *keys = slot_ptr<uint64_t>(slot, A.L.keys0);
+    const uint32_t *vals = slot_ptr<uint32_t>(slot, A.L.vals0);
+    const int8_t *lcp = slot_ptr<int8_t>(slot, A.L.lcp);
+    const uint32_t *group = slot_ptr<uint32_t>(slot, A.L.group);
+    const uint32_t *owner = slot_ptr<uint32_t>(slot, A.L.owner);
+    const long long *pm = slot_ptr<long long>(slot, A.L.pm);
+    const i128 *pxy = slot_ptr<i128>(slot, A.L.pxy);
+    float4 *nodes = slot_ptr<float4>(slot, A.L.nodes);
+    uint32_t *body_node = slot_ptr<uint32_t>(slot, A.L.body_node);
+    const double inv_scale = S.radius > 0.0f ? (double)S.radius / kFixedScale : 1.0;
+    const double rx = S.rx, ry = S.ry;
+    const uint32_t total = S.total_nodes;
+    for (uint32_t g = threadIdx.x; g < total; g += kBThreads) {
+        const uint32_t w = owner[g];
+        const int k = (int)(w >> 6), q = (int)(w & 63u);
+        if (q == 63) {
+            const uint32_t i = vals[k];
+            const float2 p = A.pos[base + i];
+            nodes[g] = make_float4(p.x, p.y, A.mass[base + i], make_meta(g + 1, kBodyLevel));
+            body_node[k] = g;
+            continue;
+        }
+        const int lvl = (k == 0 ? 0 : load_lcp(lcp, (int)n, k - 1) + 1) + q;
+        const int b = lvl == 0 ? (int)n - 1 : find_end(keys, lcp, (int)n, k, lvl);
+        const uint32_t next = body_index(lcp, group, (int)n, b) + 1;
+        const double cm = (double)(pm[b + 1] - pm[k]);
+        const double sx = i128_to_double(pxy[2 * (size_t)(b + 1)] - pxy[2 * (size_t)k]);
+        const double sy = i128_to_double(pxy[2 * (size_t)(b + 1) + 1] - pxy[2 * (size_t)k + 1]);
+        nodes[g] = make_float4((float)(rx + sx / cm * inv_scale), (float)(ry + sy / cm * inv_scale),
+                               (float)cm, make_meta(next, lvl));
+    }
+    __syncthreads();
+}
+
+// The warp-vote walk of k_traverse over this graph's tree, the total force,
+// swing and traction per group of 32 bodies, then (thread 0) the speed rule.
+__device__ void phase_traverse(const BatchArgs &A, uint32_t base, uint32_t n, char *slot,
+                               BatchSmem &S) {
+    const float4 *nodes = slot_ptr<float4>(slot, A.L.nodes);
+    const uint32_t *body_node = slot_ptr<uint32_t>(slot, A.L.body_node);
+    const uint32_t *vals = slot_ptr<uint32_t>(slot, A.L.vals0);
+    const float2 *fa = slot_ptr<float2>(slot, A.L.fa);
+    float2 *f = slot_ptr<float2>(slot, A.L.f);
+    float2 *gpart = slot_ptr<float2>(slot, A.L.gpart);
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        // src/RPBHKernels.cu:579-592
+        float tmp = S.radius * 2;
+        float dq = tmp * tmp * A.prm.itolsq;
+        S.dq[0] = 0.0f;
+        for (int l = 1; l <= kLevels; ++l) {
+            S.dq[l] = dq + A.prm.epssq;
+            dq = dq * 0.25f;
+        }
+        for (int l = kLevels + 1; l < 64; ++l) S.dq[l] = 0.0f;
+        S.ticket = 0;
+    }
+    __syncthreads();
+    const uint32_t end = S.total_nodes;
+    const int ngroups = (int)((n + 31) >> 5);
+    for (;;) {
+        int w = 0;
+        if (lane == 0) w = atomicAdd(&S.ticket, 1);
+        w = __shfl_sync(kFullMask, w, 0);
+        if (w >= ngroups) break;
+        const int k = w * 32 + lane;
+        const bool active = k < (int)n;
+        const float4 me = nodes[body_node[active ? k : (int)n - 1]];
+        const float px = active ? me.x : 1e30f, py = active ? me.y : 1e30f;
+        float ax = 0.0f, ay = 0.0f;
+        uint32_t node = 1;
+        if (node < end) {
+            for (;;) {
+                const float4 r = nodes[node];
+                const int meta = __float_as_int(r.w);
+                const float dx = px - r.x, dy = py - r.y;
+                const float d2 = dx * dx + dy * dy + A.prm.epssq;
+                if (__all_sync(kFullMask, d2 >= S.dq[meta_level(meta)])) {
+                    const float c = __fdividef(r.z, d2);
+                    ax = fmaf(dx, c, ax);
+                    ay = fmaf(dy, c, ay);
+                    node = meta_next(meta);
+                    if (node >= end) break;
+                } else {
+                    ++node;
+                }
+            }
+        }
+        const float kmi = A.prm.k_r * me.z;
+        ax *= kmi;
+        ay *= kmi;
+        float sw = 0.0f, tr = 0.0f;
+        if (active) {
+            const uint32_t i = vals[k];
+            const float2 g = fa[i], fp = A.fprev[base + i];
+            const float fx = g.x + ax, fy = g.y + ay;
+            f[i] = make_float2(fx, fy);
+            A.f_tot[base + i] = make_float2(fx, fy);
+            float dx = fx - fp.x, dy = fy - fp.y;
+            sw = me.z * sqrtf(dx * dx + dy * dy);
+            dx = fx + fp.x;
+            dy = fy + fp.y;
+            tr = me.z * (float)(sqrtf(dx * dx + dy * dy) / 2.0);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            sw += __shfl_xor_sync(kFullMask, sw, o);
+            tr += __shfl_xor_sync(kFullMask, tr, o);
+        }
+        if (lane == 0) gpart[w] = make_float2(sw, tr);
+    }
+    __syncthreads();
+    // fixed-order sum of the group partials, then the speed rule
+    if (threadIdx.x < 32) {
+        float sw = 0.0f, tr = 0.0f;
+        for (int w = lane; w < ngroups; w += 32) {
+            const float2 v = gpart[w];
+            sw += v.x;
+            tr += v.y;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            sw += __shfl_xor_sync(kFullMask, sw, o);
+            tr += __shfl_xor_sync(kFullMask, tr, o);
+        }
+        if (lane == 0) {
+            float se = S.se, gs = S.gs;
+            speed_update(sw, tr, (int)n, A.jitter_tolerance, A.k_s_max, se, gs);
+            S.se = se;
+            S.gs = gs;
+        }
+    }
+    __syncthreads();
+}
+
+// Displacement (DisplacementKernel, src/RPFA2Kernels.cu:223-251).
+__device__ void phase_displace(const BatchArgs &A, uint32_t base, uint32_t n, char *slot,
+                               BatchSmem &S) {
+    const float2 *f = slot_ptr<float2>(slot, A.L.f);
+    const float gs = S.gs;
+    for (uint32_t i = threadIdx.x; i < n; i += kBThreads) {
+        const float2 fi = f[i], fp = A.fprev[base + i];
+        const float factor = displacement_factor(fi, fp, gs);
+        float2 p = A.pos[base + i];
+        p.x += fi.x * factor;
+        p.y += fi.y * factor;
+        A.pos[base + i] = p;
+        A.fprev[base + i] = fi;
+    }
+    __syncthreads();
+}
+
+template <bool LINLOG>
+__global__ void __launch_bounds__(kBThreads, 1) k_batch(BatchArgs A) {
+    __shared__ BatchSmem S;
+    char *slot = A.slots + (size_t)blockIdx.x * A.L.bytes;
+    float2 *fa = slot_ptr<float2>(slot, A.L.fa);
+    for (;;) {
+        if (threadIdx.x == 0) S.graph = (int)atomicAdd(A.queue, 1u);
+        __syncthreads();
+        const int qi = S.graph;
+        if (qi >= A.num_graphs) break;
+        const int gi = (int)A.order[qi];
+        const BatchGraph G = A.graphs[gi];
+        const uint32_t base = G.node_base, n = G.n;
+        if (threadIdx.x == 0) {
+            const BatchSpeed sp = A.speed[gi];
+            S.gs = sp.global_speed;
+            S.se = sp.speed_efficiency;
+            S.err = sp.err;
+            S.poison = 0;
+        }
+        __syncthreads();
+        int rounds = 0;
+        for (int it = 0; it < A.iters && n > 0; ++it) {
+            if (S.err) break;
+            phase_attract<LINLOG>(A, base, n, fa);
+            phase_bbox(A, base, n, S);
+            phase_keys_sort(A, base, n, slot, S, 0);
+            // Exactly coincident bodies: scale the later ones by .99 (the
+            // reference's re-insertion, src/RPBHKernels.cu:271-278) and build
+            // again, keeping gravity, attraction and the box of before.
+            rounds = 0;
+            while (S.poison && !S.err) {
+                if (++rounds > 64) {
+                    if (threadIdx.x == 0) S.err |= kErrPoisonRounds;
+                    __syncthreads();
+                    break;
+                }
+                __syncthreads();
+                if (threadIdx.x == 0) S.poison = 0;
+                phase_keys_sort(A, base, n, slot, S, 1);  // scales, poison stays 0
+                phase_keys_sort(A, base, n, slot, S, 0);  // sorts the scaled positions
+            }
+            if (S.err) break;
+            phase_count(A, base, n, slot, S);
+            if (S.err) break;
+            phase_emit(A, base, n, slot, S);
+            phase_traverse(A, base, n, slot, S);
+            phase_displace(A, base, n, slot, S);
+        }
+        // the body order of the last iteration, graph-local ids
+        const uint32_t *vals = slot_ptr<uint32_t>(slot, A.L.vals0);
+        for (uint32_t k = threadIdx.x; k < n; k += kBThreads) A.sortd[base + k] = vals[k];
+        if (threadIdx.x == 0) {
+            BatchSpeed sp;
+            sp.global_speed = S.gs;
+            sp.speed_efficiency = S.se;
+            sp.err = S.err;
+            sp.perturb_rounds = rounds;
+            A.speed[gi] = sp;
+        }
+        __syncthreads();
+    }
+}
+
+size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+SlotLayout make_layout(uint32_t nmax) {
+    SlotLayout L;
+    const uint64_t cap64 = 33ull * nmax + 64;
+    L.cap = (uint32_t)cap64;
+    size_t o = 0;
+    auto take = [&](size_t bytes) {
+        const size_t at = o;
+        o = up256(o + bytes);
+        return at;
+    };
+    L.keys0 = take(8ull * nmax);
+    L.keys1 = take(8ull * nmax);
+    L.vals0 = take(4ull * nmax);
+    L.vals1 = take(4ull * nmax);
+    L.lcp = take(1ull * nmax);
+    L.group = take(4ull * nmax);
+    L.body_node = take(4ull * nmax);
+    L.owner = take(4ull * cap64);
+    L.nodes = take(16ull * (cap64 + 1));
+    L.pm = take(8ull * (nmax + 1));
+    L.pxy = take(32ull * (nmax + 1));
+    L.fa = take(8ull * nmax);
+    L.f = take(8ull * nmax);
+    L.gpart = take(8ull * ((nmax + 31) / 32));
+    L.bytes = o;
+    return L;
+}
+
+}  // namespace
+
+}  // namespace fa2
+
+using namespace fa2;
+
+struct fa2_batch {
+    int device = 0;
+    int nsm = 0;
+    uint32_t num_graphs = 0;
+    uint64_t total_nodes = 0;
+    fa2_params prm{};
+    Params kp{};
+    std::vector<uint32_t> base;  // node base per graph
+    std::vector<uint32_t> count; // nodes per graph
+    std::vector<void *> allocs;
+    BatchArgs args{};
+    int grid = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+int cuda_status_b(cudaError_t e) {
+    if (e == cudaSuccess) return FA2_OK;
+    if (e == cudaErrorMemoryAllocation) return FA2_ERR_OUT_OF_MEMORY;
+    return FA2_ERR_CUDA;
+}
+
+#define BCK(x)                                       \
+    do {                                             \
+        cudaError_t e_ = (x);                        \
+        if (e_ != cudaSuccess) return cuda_status_b(e_); \
+    } while (0)
+
+template <typename T>
+int balloc(fa2_batch *b, T **p, size_t count) {
+    void *q = nullptr;
+    BCK(cudaMalloc(&q, count * sizeof(T) + 16));
+    b->allocs.push_back(q);
+    *p = static_cast<T *>(q);
+    return FA2_OK;
+}
+
+void bfree(fa2_batch *b) {
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    for (void *p : b->allocs) cudaFree(p);
+    b->allocs.clear();
+}
+
+int launch_batch(fa2_batch *b, int iters) {
+    b->args.iters = iters;
+    BCK(cudaMemsetAsync(b->args.queue, 0, sizeof(unsigned), b->stream));
+    if (b->kp.linlog)
+        k_batch<true><<<b->grid, kBThreads, 0, b->stream>>>(b->args);
+    else
+        k_batch<false><<<b->grid, kBThreads, 0, b->stream>>>(b->args);
+    BCK(cudaGetLastError());
+    return FA2_OK;
+}
+
+int check_errors(fa2_batch *b) {
+    std::vector<BatchSpeed> sp(b->num_graphs);
+    BCK(cudaMemcpyAsync(sp.data(), b->args.speed, sp.size() * sizeof(BatchSpeed),
+                        cudaMemcpyDeviceToHost, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+    for (const BatchSpeed &s : sp)
+        if (s.err) return FA2_ERR_DEVICE_LIMIT;
+    return FA2_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+fa2_batch *fa2_batch_create(uint32_t num_graphs, const fa2_graph_desc *graphs,
+                            const fa2_params *prm, int *status) {
+    int dummy;
+    if (!status) status = &dummy;
+    *status = FA2_ERR_INVALID_ARGUMENT;
+    if (!prm || (num_graphs && !graphs)) return nullptr;
+    if (!prm->use_barneshut) {
+        *status = FA2_ERR_UNSUPPORTED;
+        return nullptr;
+    }
+    if (!(prm->theta > 0.0f)) return nullptr;
+    uint64_t total_n = 0, total_m = 0;
+    uint32_t nmax = 1;
+    for (uint32_t g = 0; g < num_graphs; ++g) {
+        const fa2_graph_desc &d = graphs[g];
+        if (d.num_edges && (!d.sources || !d.targets)) return nullptr;
+        for (uint64_t e = 0; e < d.num_edges; ++e)
+            if (d.sources[e] >= d.num_nodes || d.targets[e] >= d.num_nodes ||
+                d.sources[e] == d.targets[e])
+                return nullptr;
+        if (d.num_nodes > kBatchMaxNodes) {
+            *status = FA2_ERR_TOO_LARGE;
+            return nullptr;
+        }
+        total_n += d.num_nodes;
+        total_m += d.num_edges;
+        nmax = std::max(nmax, d.num_nodes);
+    }
+    if (total_n >= (1ull << 31) || 2 * total_m >= (1ull << 32)) {
+        *status = FA2_ERR_TOO_LARGE;
+        return nullptr;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || prm->device < 0 || prm->device >= ndev) {
+        *status = FA2_ERR_NO_DEVICE;
+        return nullptr;
+    }
+    cudaDeviceProp dp;
+    if (cudaGetDeviceProperties(&dp, prm->device) != cudaSuccess || dp.major < 10) {
+        *status = FA2_ERR_NO_DEVICE;
+        return nullptr;
+    }
+    if (cudaSetDevice(prm->device) != cudaSuccess) {
+        *status = FA2_ERR_CUDA;
+        return nullptr;
+    }
+    fa2_batch *b = new fa2_batch();
+    auto fail = [&](int s) {
+        *status = s;
+        bfree(b);
+        delete b;
+        return (fa2_batch *)nullptr;
+    };
+    b->device = prm->device;
+    b->nsm = dp.multiProcessorCount;
+    b->num_graphs = num_graphs;
+    b->total_nodes = total_n;
+    b->prm = *prm;
+    b->kp.k_r = prm->scale;
+    b->kp.k_g = prm->gravity;
+    b->kp.itolsq = 1.0f / (prm->theta * prm->theta);  // src/RPForceAtlas2.cpp:47
+    b->kp.epssq = prm->epssq;
+    b->kp.strong_gravity = prm->strong_gravity;
+    b->kp.linlog = prm->linlog != 0;
+    b->kp.nsm = b->nsm;
+
+    // host layout: graphs back to back, each graph's nodes in id order;
+    // symmetric CSR over batch ids; mass = degree + 1 (src/RPForceAtlas2.cpp:74-77)
+    const size_t N = (size_t)total_n;
+    b->base.resize(num_graphs);
+    b->count.resize(num_graphs);
+    std::vector<BatchGraph> hg(num_graphs);
+    std::vector<uint32_t> deg(N, 0);
+    uint64_t nb = 0;
+    for (uint32_t g = 0; g < num_graphs; ++g) {
+        b->base[g] = (uint32_t)nb;
+        b->count[g] = graphs[g].num_nodes;
+        hg[g] = BatchGraph{(uint32_t)nb, graphs[g].num_nodes};
+        for (uint64_t e = 0; e < graphs[g].num_edges; ++e) {
+            deg[nb + graphs[g].sources[e]]++;
+            deg[nb + graphs[g].targets[e]]++;
+        }
+        nb += graphs[g].num_nodes;
+    }
+    std::vector<uint32_t> off(N + 1, 0);
+    for (size_t i = 0; i < N; ++i) off[i + 1] = off[i] + deg[i];
+    std::vector<uint32_t> col(std::max<size_t>(off[N], 1));
+    std::vector<uint32_t> fill(off.begin(), off.end() - 1);
+    for (uint32_t g = 0; g < num_graphs; ++g) {
+        const uint32_t bs = b->base[g];
+        for (uint64_t e = 0; e < graphs[g].num_edges; ++e) {
+            const uint32_t s = bs + graphs[g].sources[e], t = bs + graphs[g].targets[e];
+            col[fill[s]++] = t;
+            col[fill[t]++] = s;
+        }
+    }
+    std::vector<float> mass(N);
+    for (size_t i = 0; i < N; ++i) mass[i] = (float)deg[i] + 1.0f;
+    // largest first (nodes + edges), so the long graphs start early
+    std::vector<uint32_t> order(num_graphs);
+    std::iota(order.begin(), order.end(), 0u);
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t c) {
+        return (uint64_t)graphs[a].num_nodes + graphs[a].num_edges >
+               (uint64_t)graphs[c].num_nodes + graphs[c].num_edges;
+    });
+
+    BatchArgs &A = b->args;
+    A.L = make_layout(nmax);
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<false>, kBThreads, 0);
+    int occ2 = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k_batch<true>, kBThreads, 0);
+    occ = std::max(1, std::min(occ, occ2));
+    b->grid = std::max(1, std::min<int>(b->nsm * occ, (int)std::max<uint32_t>(num_graphs, 1)));
+
+    BatchGraph *d_graphs = nullptr;
+    uint32_t *d_order = nullptr, *d_off = nullptr, *d_col = nullptr;
+    float *d_mass = nullptr;
+    int s = FA2_OK;
+    if ((s = balloc(b, &d_graphs, std::max<size_t>(num_graphs, 1))) ||
+        (s = balloc(b, &d_order, std::max<size_t>(num_graphs, 1))) ||
+        (s = balloc(b, &A.pos, std::max<size_t>(N, 1))) ||
+        (s = balloc(b, &A.fprev, std::max<size_t>(N, 1))) ||
+        (s = balloc(b, &d_mass, std::max<size_t>(N, 1))) || (s = balloc(b, &d_off, N + 1)) ||
+        (s = balloc(b, &d_col, col.size())) ||
+        (s = balloc(b, &A.speed, std::max<size_t>(num_graphs, 1))) ||
+        (s = balloc(b, &A.f_tot, std::max<size_t>(N, 1))) ||
+        (s = balloc(b, &A.f_ag, std::max<size_t>(N, 1))) ||
+        (s = balloc(b, &A.sortd, std::max<size_t>(N, 1))) || (s = balloc(b, &A.queue, 1)) ||
+        (s = balloc(b, &A.slots, A.L.bytes * (size_t)b->grid)))
+        return fail(s);
+    A.graphs = d_graphs;
+    A.order = d_order;
+    A.num_graphs = (int)num_graphs;
+    A.mass = d_mass;
+    A.off = d_off;
+    A.col = d_col;
+    A.prm = b->kp;
+    A.jitter_tolerance = prm->jitter_tolerance;
+    A.k_s_max = prm->k_s_max;
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess)
+        return fail(FA2_ERR_CUDA);
+    std::vector<BatchSpeed> sp(num_graphs);
+    for (auto &x : sp) x = BatchSpeed{1.0f, 1.0f, 0, 0};  // src/RPFA2Kernels.cu:30-31
+    cudaStream_t st = b->stream;
+    if (cudaMemcpyAsync(d_graphs, hg.data(), hg.size() * sizeof(BatchGraph), cudaMemcpyHostToDevice, st) ||
+        cudaMemcpyAsync(d_order, order.data(), order.size() * 4, cudaMemcpyHostToDevice, st) ||
+        cudaMemcpyAsync(d_mass, mass.data(), N * 4, cudaMemcpyHostToDevice, st) ||
+        cudaMemcpyAsync(d_off, off.data(), (N + 1) * 4, cudaMemcpyHostToDevice, st) ||
+        cudaMemcpyAsync(d_col, col.data(), col.size() * 4, cudaMemcpyHostToDevice, st) ||
+        cudaMemcpyAsync(A.speed, sp.data(), sp.size() * sizeof(BatchSpeed), cudaMemcpyHostToDevice, st) ||
+        cudaMemsetAsync(A.pos, 0, N * 8, st) || cudaMemsetAsync(A.fprev, 0, N * 8, st) ||
+        cudaMemsetAsync(A.f_tot, 0, N * 8, st) || cudaMemsetAsync(A.f_ag, 0, N * 8, st) ||
+        cudaMemsetAsync(A.sortd, 0, N * 4, st) || cudaStreamSynchronize(st))
+        return fail(FA2_ERR_CUDA);
+    *status = FA2_OK;
+    return b;
+}
+
+void fa2_batch_destroy(fa2_batch *b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    bfree(b);
+    delete b;
+}
+
+int fa2_batch_set_positions(fa2_batch *b, const float *xy) {
+    if (!b || (!xy && b->total_nodes)) return FA2_ERR_INVALID_ARGUMENT;
+    BCK(cudaSetDevice(b->device));
+    if (!b->total_nodes) return FA2_OK;
+    BCK(cudaMemcpyAsync(b->args.pos, xy, b->total_nodes * 8, cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+    return FA2_OK;
+}
+
+int fa2_batch_get_positions(fa2_batch *b, float *xy) {
+    if (!b || (!xy && b->total_nodes)) return FA2_ERR_INVALID_ARGUMENT;
+    BCK(cudaSetDevice(b->device));
+    if (!b->total_nodes) return FA2_OK;
+    BCK(cudaMemcpyAsync(xy, b->args.pos, b->total_nodes * 8, cudaMemcpyDeviceToHost, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+    return FA2_OK;
+}
+
+int fa2_batch_step(fa2_batch *b, int32_t n_iters) {
+    if (!b || n_iters < 0) return FA2_ERR_INVALID_ARGUMENT;
+    BCK(cudaSetDevice(b->device));
+    if (!n_iters || !b->num_graphs) return FA2_OK;
+    int s = launch_batch(b, n_iters);
+    if (s) return s;
+    return check_errors(b);
+}
+
+int fa2_batch_step_timed(fa2_batch *b, int32_t n_iters, float *ms) {
+    if (!b || n_iters < 0 || !ms) return FA2_ERR_INVALID_ARGUMENT;
+    BCK(cudaSetDevice(b->device));
+    *ms = 0.0f;
+    if (!n_iters || !b->num_graphs) return FA2_OK;
+    BCK(cudaEventRecord(b->ev0, b->stream));
+    int s = launch_batch(b, n_iters);
+    if (s) return s;
+    BCK(cudaEventRecord(b->ev1, b->stream));
+    BCK(cudaEventSynchronize(b->ev1));
+    BCK(cudaEventElapsedTime(ms, b->ev0, b->ev1));
+    return check_errors(b);
+}
+
+int fa2_batch_get_forces(fa2_batch *b, float *f_total, float *f_attr_grav) {
+    if (!b) return FA2_ERR_INVALID_ARGUMENT;
+    BCK(cudaSetDevice(b->device));
+    const size_t bytes = b->total_nodes * 8;
+    if (f_total && bytes)
+        BCK(cudaMemcpyAsync(f_total, b->args.f_tot, bytes, cudaMemcpyDeviceToHost, b->stream));
+    if (f_attr_grav && bytes)
+        BCK(cudaMemcpyAsync(f_attr_grav, b->args.f_ag, bytes, cudaMemcpyDeviceToHost, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+    return FA2_OK;
+}
+
+int fa2_batch_get_sort_order(fa2_batch *b, uint32_t *order) {
+    if (!b || (!order && b->total_nodes)) return FA2_ERR_INVALID_ARGUMENT;
+    BCK(cudaSetDevice(b->device));
+    if (!b->total_nodes) return FA2_OK;
+    BCK(cudaMemcpyAsync(order, b->args.sortd, b->total_nodes * 4, cudaMemcpyDeviceToHost,
+                        b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+    return FA2_OK;
+}
+
+int fa2_batch_get_speed(fa2_batch *b, float *global_speed, float *speed_efficiency) {
+    if (!b) return FA2_ERR_INVALID_ARGUMENT;
+    BCK(cudaSetDevice(b->device));
+    std::vector<BatchSpeed> sp(b->num_graphs);
+    if (!sp.empty()) {
+        BCK(cudaMemcpyAsync(sp.data(), b->args.speed, sp.size() * sizeof(BatchSpeed),
+                            cudaMemcpyDeviceToHost, b->stream));
+        BCK(cudaStreamSynchronize(b->stream));
+    }
+    for (size_t g = 0; g < sp.size(); ++g) {
+        if (global_speed) global_speed[g] = sp[g].global_speed;
+        if (speed_efficiency) speed_efficiency[g] = sp[g].speed_efficiency;
+    }
+    return FA2_OK;
+}
+
+}  // extern "C"

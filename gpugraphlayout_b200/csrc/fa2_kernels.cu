@@ -19,32 +19,6 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 
-// Quadrant digits of (px, py) under the root cell, computed the way
-// TreeBuildingKernel walks down (src/RPBHKernels.cu:217-241): the child
-// centre is the parent centre +/- r, r halving per level; a coordinate
-// equal to the centre goes to the low side.
-__device__ __forceinline__ uint64_t morton_key(float px, float py, float x, float y, float r) {
-    uint64_t key = 0;
-#pragma unroll 8
-    for (int lvl = 0; lvl < kLevels; ++lvl) {
-        r *= 0.5f;
-        int j = 0;
-        float dx = -r, dy = -r;
-        if (x < px) {
-            j = 1;
-            dx = r;
-        }
-        if (y < py) {
-            j |= 2;
-            dy = r;
-        }
-        x = __fadd_rn(x, dx);
-        y = __fadd_rn(y, dy);
-        key = (key << 2) | (uint64_t)j;
-    }
-    return key;
-}
-
 // ------------------------------------------------------------------- bbox --
 
 __device__ __forceinline__ float4 bbox_merge(float4 a, float4 b) {
@@ -279,26 +253,8 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
         }
         st->swg_sum = swg;
         st->etra_sum = etra;
-        // src/RPFA2Kernels.cu:243-275
-        float estimated_optimal_jitter_tollerance = 0.05 * sqrtf((float)n);
-        float minJT = sqrtf(estimated_optimal_jitter_tollerance);
-        float jt = st->jitter_tolerance *
-                   fmaxf(minJT, fminf(st->k_s_max, estimated_optimal_jitter_tollerance * etra /
-                                                       powf((float)n, 2.0f)));
-        float min_speed_efficiency = 0.05f;
         float se = st->speed_efficiency, gs = st->global_speed;
-        if (swg / etra > 2.0) {
-            if (se > min_speed_efficiency) se *= 0.5;
-            jt = fmaxf(jt, st->jitter_tolerance);
-        }
-        float targetSpeed = jt * se * etra / swg;
-        if (swg > jt * etra) {
-            if (se > min_speed_efficiency) se *= 0.7;
-        } else if (gs < 1000) {
-            se *= 1.3;
-        }
-        float max_rise = 0.5f;
-        gs += fminf(targetSpeed - gs, max_rise * gs);
+        speed_update(swg, etra, n, st->jitter_tolerance, st->k_s_max, se, gs);
         st->speed_efficiency = se;
         st->global_speed = gs;
     }
@@ -372,9 +328,7 @@ __global__ void __launch_bounds__(kDispThreads) k_displace(int n, float2 *__rest
     float4 a = make_float4(FLT_MAX, -FLT_MAX, FLT_MAX, -FLT_MAX);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float2 fi = f[i], fp = fprev[i];
-        const float dx = fi.x - fp.x, dy = fi.y - fp.y;
-        const float swg = sqrtf(dx * dx + dy * dy);
-        const float factor = global_speed / (1.0 + sqrtf(global_speed * swg));
+        const float factor = displacement_factor(fi, fp, global_speed);
         float2 p = pos[i];
         p.x += fi.x * factor;
         p.y += fi.y * factor;
@@ -395,27 +349,10 @@ __global__ void __launch_bounds__(kDispThreads) k_displace(int n, float2 *__rest
 // ids with one 16-byte load.  `lanes` lanes share a row and reduce with
 // shuffles; heavy rows take a whole block.  To keep many loads in flight a
 // warp of a short-row bucket works on kAttractBatch groups of rows at once:
-// all column loads first, then all position gathers.
-// One neighbour's pull: p_j - p_i, or with linear-log attraction (use_linlog
-// of the reference's CPU path, RPCPUForceAtlas2.cpp:59-67) that vector times
-// log(1 + d) / d, d = 0 taken as FLT_MAX (padding ids give the zero vector).
-template <bool LINLOG>
-__device__ __forceinline__ float2 pull(float2 q, float2 p) {
-    float dx = q.x - p.x, dy = q.y - p.y;
-    if (LINLOG) {
-        const float ex = p.x - q.x, ey = p.y - q.y;
-        const float dist = sqrtf(ex * ex + ey * ey);
-        const float w = dist == 0.0f ? FLT_MAX : logf(1 + dist) / dist;
-        dx *= w;
-        dy *= w;
-    }
-    return make_float2(dx, dy);
-}
-
-// Neighbour-position gathers go through L1, which keeps the positions of the
-// hubs (the first internal ids, gathered most often).  A copy of the hubs in
-// shared memory measured slower: its carve-out took the L1 that the other
-// gathers hit.
+// all column loads first, then all position gathers.  Neighbour-position
+// gathers go through L1, which keeps the positions of the hubs (the first
+// internal ids, gathered most often); a copy of the hubs in shared memory
+// measured slower, its carve-out taking the L1 that the other gathers hit.
 struct Gather {
     const float2 *__restrict pos;
     __device__ __forceinline__ float2 operator()(int c) const { return __ldg(&pos[c]); }
@@ -428,18 +365,6 @@ __device__ __forceinline__ void add_four(const int4 c, const float2 p, const Gat
     const float2 q2 = pull<LINLOG>(g(c.z), p), q3 = pull<LINLOG>(g(c.w), p);
     ax += q0.x + q1.x + (q2.x + q3.x);
     ay += q0.y + q1.y + (q2.y + q3.y);
-}
-
-__device__ __forceinline__ float2 with_gravity(float2 p, float m, float ax, float ay,
-                                               const Params &prm) {
-    float f_g;
-    if (prm.strong_gravity)
-        f_g = prm.k_g * m;
-    else if (p.x != 0.0f || p.y != 0.0f)
-        f_g = prm.k_g * m * rsqrtf(p.x * p.x + p.y * p.y);
-    else
-        f_g = 0.0f;
-    return make_float2(-p.x * f_g + ax, -p.y * f_g + ay);
 }
 
 // Rows of at most LANES int4 chunks (LANES <= 16): one chunk per lane.

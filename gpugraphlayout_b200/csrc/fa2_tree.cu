@@ -39,79 +39,6 @@ constexpr unsigned kFull = kFullMask;
 
 // ------------------------------------------------------------------- runs --
 
-// Replays the cell centre of a 32-digit key path.
-__device__ __forceinline__ void key_centre(uint64_t key, float rx, float ry, float rr, float &x,
-                                           float &y, float &r) {
-    x = rx;
-    y = ry;
-    r = rr;
-    for (int lvl = 0; lvl < kLevels; ++lvl) {
-        r *= 0.5f;
-        const int j = (int)(key >> (2 * (kLevels - 1 - lvl))) & 3;
-        x = __fadd_rn(x, (j & 1) ? r : -r);
-        y = __fadd_rn(y, (j & 2) ? r : -r);
-    }
-}
-
-// Orders two bodies that share all 32 digits by the digits below level 32
-// (the reference keeps splitting: src/RPBHKernels.cu:282-313), then by
-// reference id.  Returns true if a goes first.
-__device__ bool deep_less(float2 pa, float2 pb, uint32_t ida, uint32_t idb, float x, float y,
-                          float r) {
-    for (int lvl = 0; lvl < kDeepLevels; ++lvl) {
-        r *= 0.5f;
-        const int ja = (x < pa.x ? 1 : 0) | (y < pa.y ? 2 : 0);
-        const int jb = (x < pb.x ? 1 : 0) | (y < pb.y ? 2 : 0);
-        if (ja != jb) return ja < jb;
-        x = __fadd_rn(x, (ja & 1) ? r : -r);
-        y = __fadd_rn(y, (ja & 2) ? r : -r);
-    }
-    return ida < idb;
-}
-
-// The run of equal keys that starts at sorted body k: order it, then either
-// flag exactly coincident bodies (perturb == 0) or scale every body that sits
-// on an earlier one (lower reference id) by .99, as the reference's insertion
-// does for the later-inserted body (src/RPBHKernels.cu:271-278).
-__device__ void fix_run(int k, int n, const uint64_t *__restrict keys, uint32_t *__restrict vals,
-                        float2 *__restrict pos, const uint32_t *__restrict ref_of, DevState *st,
-                        int perturb) {
-    const uint64_t key = keys[k];
-    int len = 2;
-    while (k + len < n && keys[k + len] == key && len <= kMaxRun) ++len;
-    if (len > kMaxRun) {
-        atomicOr(&st->err, kErrRunTooLong);
-        return;
-    }
-    float cx, cy, cr;
-    key_centre(key, st->rootx, st->rooty, st->radius, cx, cy, cr);
-    uint32_t *v = vals + k;
-    for (int a = 1; a < len; ++a) {  // insertion sort, stable
-        const uint32_t va = v[a];
-        const float2 pa = pos[va];
-        int b = a - 1;
-        while (b >= 0) {
-            const uint32_t vb = v[b];
-            if (!deep_less(pa, pos[vb], ref_of[va], ref_of[vb], cx, cy, cr)) break;
-            v[b + 1] = vb;
-            --b;
-        }
-        v[b + 1] = va;
-    }
-    // coincident neighbours (equal positions are adjacent after ordering)
-    bool any = false;
-    float2 prev = pos[v[0]];
-    for (int a = 1; a < len; ++a) {
-        const float2 p = pos[v[a]];
-        const bool same = p.x == prev.x && p.y == prev.y;
-        prev = p;
-        if (!same) continue;
-        any = true;
-        if (perturb) pos[v[a]] = make_float2((float)((double)p.x * .99), (float)((double)p.y * .99));
-    }
-    if (any && !perturb) atomicAdd(&st->poison, 1);
-}
-
 // Replay path: the runs of the last sort, with the .99 scaling applied.
 __global__ void __launch_bounds__(256) k_runs(int n, const uint64_t *__restrict keys,
                                               uint32_t *__restrict vals, float2 *__restrict pos,
@@ -120,61 +47,12 @@ __global__ void __launch_bounds__(256) k_runs(int n, const uint64_t *__restrict 
     if (st->err || st->poison) return;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k + 1 < n; k += gridDim.x * blockDim.x) {
         if (keys[k + 1] != keys[k] || (k > 0 && keys[k - 1] == keys[k])) continue;
-        fix_run(k, n, keys, vals, pos, ref_of, st, perturb);
+        fix_run(k, n, keys, vals, pos, ref_of, st->rootx, st->rooty, st->radius, &st->err,
+                &st->poison, perturb);
     }
 }
 
 // ------------------------------------------------------------- tree count --
-
-__device__ __forceinline__ int lcp_at(const uint64_t *__restrict keys, int n, int k) {
-    return (k < 0 || k >= n - 1) ? -1 : lcp_digits(keys[k], keys[k + 1]);
-}
-
-// cells that start at sorted body k
-__device__ __forceinline__ int cells_at(int k, int Lk, int Lkm1) {
-    return k == 0 ? max(Lk, 0) + 1 : max(0, Lk - Lkm1);
-}
-
-typedef __int128 i128;
-
-__device__ __forceinline__ i128 shfl_up_i128(i128 v, int o) {
-    const unsigned long long lo = (unsigned long long)v;
-    const long long hi = (long long)(v >> 64);
-    const unsigned long long lo2 = __shfl_up_sync(kFull, lo, o);
-    const long long hi2 = __shfl_up_sync(kFull, hi, o);
-    return ((i128)hi2 << 64) | (i128)lo2;
-}
-
-__device__ __forceinline__ i128 shfl_xor_i128(i128 v, int o) {
-    const unsigned long long lo = (unsigned long long)v;
-    const long long hi = (long long)(v >> 64);
-    const unsigned long long lo2 = __shfl_xor_sync(kFull, lo, o);
-    const long long hi2 = __shfl_xor_sync(kFull, hi, o);
-    return ((i128)hi2 << 64) | (i128)lo2;
-}
-
-// 128-bit load that bypasses L1 (the value was written by another block)
-__device__ __forceinline__ i128 ldcg_i128(const i128 *p) {
-    const longlong2 v = __ldcg(reinterpret_cast<const longlong2 *>(p));
-    return ((i128)v.y << 64) | (i128)(unsigned long long)v.x;
-}
-
-__device__ __forceinline__ double i128_to_double(i128 v) {
-    const long long hi = (long long)(v >> 64);
-    const unsigned long long lo = (unsigned long long)v;
-    return (double)hi * 18446744073709551616.0 + (double)lo;
-}
-
-// Fixed-point offset from the root centre, in 2^-48 root radii (finer than a
-// float32 ulp of any coordinate but the tiniest), kept within +-2^55 (a body
-// scaled by .99 may sit outside the box); mass (< 2^24) x offset is formed in
-// 128 bits and a sum over 2^25 bodies stays below 2^105.
-constexpr double kFixedScale = 281474976710656.0;  // 2^48
-__device__ __forceinline__ long long fixed_offset(float p, float root, double scale) {
-    double q = ((double)p - (double)root) * scale;
-    q = fmin(fmax(q, -36028797018963968.0), 36028797018963968.0);
-    return __double2ll_rn(q);
-}
 
 struct NodeSums {
     uint32_t g;  // nodes (cells + body)
@@ -375,61 +253,11 @@ __global__ void __launch_bounds__(kCountThreads) k_tree_count(
     // after this tile's offsets are published, so a long run delays no one
 #pragma unroll
     for (int e = 0; e < kCountItems; ++e)
-        if (run_starts & (1u << e)) fix_run(base + e, n, keys, vals, pos, ref_of, st, 0);
+        if (run_starts & (1u << e)) fix_run(base + e, n, keys, vals, pos, ref_of, st->rootx, st->rooty, st->radius,
+                    &st->err, &st->poison, 0);
 }
 
 // ------------------------------------------------------------------- emit --
-
-__device__ __forceinline__ int load_lcp(const int8_t *__restrict lcp, int n, int k) {
-    return (k < 0 || k >= n - 1) ? -1 : (int)lcp[k];
-}
-
-// preorder index of sorted body b
-__device__ __forceinline__ uint32_t body_index(const int8_t *__restrict lcp,
-                                               const uint32_t *__restrict group, int n, int b) {
-    const int Lb = load_lcp(lcp, n, b), Lbm1 = load_lcp(lcp, n, b - 1);
-    return group[b] + (uint32_t)cells_at(b, Lb, Lbm1);
-}
-
-// Last body of the cell at level lvl that starts at sorted body k: the first
-// j >= k with L[j] < lvl.  Small cells end within a few bodies (a short scan
-// of L); larger ones are found by exponential + binary search over the keys
-// (LCP(K_k, K_j) falls as j grows).
-__device__ int find_end(const uint64_t *__restrict keys, const int8_t *__restrict lcp, int n,
-                        int k, int lvl) {
-    constexpr int kScan = 8;
-    int L[kScan];
-#pragma unroll
-    for (int s = 0; s < kScan; ++s) L[s] = load_lcp(lcp, n, k + s);
-#pragma unroll
-    for (int s = 0; s < kScan; ++s)
-        if (L[s] < lvl) return k + s;
-    const uint64_t kk = keys[k];
-    int ok = k + kScan - 1, step = 1, bad = n;
-    for (;;) {
-        const int j = ok + step;
-        if (j >= n) {
-            bad = n;
-            break;
-        }
-        if (lcp_digits(keys[j], kk) >= lvl) {
-            ok = j;
-            step <<= 1;
-        } else {
-            bad = j;
-            break;
-        }
-    }
-    int lo = ok, hi = bad - 1;  // largest j with LCP(K_k, K_j) >= lvl, in [ok, bad)
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (lcp_digits(keys[mid], kk) >= lvl)
-            lo = mid;
-        else
-            hi = mid - 1;
-    }
-    return lo;
-}
 
 // One thread per tree node (grid-stride over the preorder index): a body
 // writes its own record; a cell finds its last body, then forms its mass and

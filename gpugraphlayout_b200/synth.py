@@ -95,15 +95,20 @@ def sbm_edges(n: int, blocks: int, p_in: float, p_out: float, max_mean_degree: f
             j = idx + i + 1 - nb * (nb - 1) // 2 + (nb - i) * ((nb - i) - 1) // 2
             los.append(b0 + i)
             his.append(b0 + j)
-    # between blocks
-    for bi in range(blocks):
-        for bj in range(bi + 1, blocks):
-            pairs = sizes[bi] * sizes[bj]
-            k = rng.binomial(pairs, p_out)
-            if k:
-                idx = np.unique(rng.integers(0, pairs, size=k))
-                los.append(bounds[bi] + idx // sizes[bj])
-                his.append(bounds[bj] + idx % sizes[bj])
+    # between blocks: a binomial count per block pair, all pairs at once
+    bi, bj = np.triu_indices(blocks, 1)
+    if len(bi):
+        pairs = sizes[bi] * sizes[bj]
+        k = rng.binomial(pairs, p_out)
+        which = np.repeat(np.arange(len(bi)), k)
+        if len(which):
+            idx = (rng.random(len(which)) * pairs[which]).astype(np.int64)
+            idx = np.minimum(idx, pairs[which] - 1)
+            key = np.unique(which * (int(pairs.max()) + 1) + idx)
+            which = key // (int(pairs.max()) + 1)
+            idx = key % (int(pairs.max()) + 1)
+            los.append(bounds[bi][which] + idx // sizes[bj][which])
+            his.append(bounds[bj][which] + idx % sizes[bj][which])
     if not los:
         return np.zeros(0, np.uint32), np.zeros(0, np.uint32)
     lo = np.concatenate(los)
@@ -132,3 +137,39 @@ def write_edgelist(path: str, src: np.ndarray, dst: np.ndarray) -> None:
             v //= 10
     with open(path, "wb") as f:
         f.write(buf.tobytes())
+
+
+def _sbm_batch_part(args):
+    out = []
+    for n, b, s in args:
+        lo, hi = sbm_edges(int(n), int(b), 0.05, 0.002, 40.0, seed=int(s))
+        out.append((int(n), lo, hi))
+    return out
+
+
+def sbm_batch(num_graphs: int = 4096, n_min: int = 50, n_max: int = 20000, seed: int = 0,
+              workers: int | None = None):
+    """The batched workload: num_graphs stochastic block models with node
+    counts log-uniform in [n_min, n_max], 2-32 equal blocks, p_in 0.05,
+    p_out 0.002, mean degree capped at 40.  Returns (n, lo, hi) per graph.
+    Graph i depends only on (seed, i); `workers` processes (spawned, default
+    the CPU count) generate them."""
+    import os
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(n_min), np.log(n_max), num_graphs)).round().astype(np.int64)
+    blocks = rng.integers(2, 33, num_graphs)
+    jobs = [(int(sizes[i]), int(min(blocks[i], sizes[i])), seed * 100003 + i)
+            for i in range(num_graphs)]
+    workers = workers or min(32, os.cpu_count() or 1)
+    if workers <= 1 or num_graphs < 64:
+        return _sbm_batch_part(jobs)
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    chunks = [jobs[w::workers] for w in range(workers)]
+    with ProcessPoolExecutor(workers, mp_context=mp.get_context("spawn")) as ex:
+        parts = list(ex.map(_sbm_batch_part, chunks))
+    out = [None] * num_graphs
+    for w, part in enumerate(parts):
+        for j, g in enumerate(part):
+            out[w + j * workers] = g
+    return out

@@ -160,6 +160,46 @@ int fa2_set_linlog(fa2_ctx *ctx, int32_t enable);
 int fa2_set_overlap(fa2_ctx *ctx, int32_t enable);
 
 /* ------------------------------------------------------------------------
+ * Batched layout: many independent graphs in one persistent launch.  No
+ * counterpart in the reference, which lays out one graph per process (its
+ * speed and tree state are device statics, src/RPFA2Kernels.cu:29-33,
+ * src/RPBHKernels.cu:54-62).  Every graph gets the FA2 iteration of
+ * fa2_step with its own quadtree, speed state and bounding box; one CTA runs
+ * a graph's iterations, taking graphs largest first from a queue.
+ * ---------------------------------------------------------------------- */
+
+typedef struct fa2_batch fa2_batch;
+
+/* Largest graph (nodes) the batched path takes; larger ones -> FA2_ERR_TOO_LARGE. */
+#define FA2_BATCH_MAX_NODES 65536
+
+/* num_graphs graphs, each as fa2_create takes one (ids local to the graph);
+ * the parameters apply to every graph.  Positions start at zero. */
+fa2_batch *fa2_batch_create(uint32_t num_graphs, const fa2_graph_desc *graphs,
+                            const fa2_params *params, int *status);
+void fa2_batch_destroy(fa2_batch *batch);
+
+/* Positions of all graphs, graph after graph, each graph's nodes in id order
+ * (2 floats per node; host memory). */
+int fa2_batch_set_positions(fa2_batch *batch, const float *xy);
+int fa2_batch_get_positions(fa2_batch *batch, float *xy);
+
+/* n_iters iterations of every graph in one launch; returns when done.
+ * FA2_ERR_DEVICE_LIMIT if a graph hit a device bound (its iterations stop). */
+int fa2_batch_step(fa2_batch *batch, int32_t n_iters);
+
+/* fa2_batch_step with *ms = CUDA-event time of the launch. */
+int fa2_batch_step_timed(fa2_batch *batch, int32_t n_iters, float *ms);
+
+/* Test hooks, last iteration: total and gravity + attraction forces (2 floats
+ * per node, same order as the positions); the body order of each graph's
+ * quadtree (graph-local ids, the reference's sortd); the adaptive speed and
+ * speed efficiency per graph. */
+int fa2_batch_get_forces(fa2_batch *batch, float *f_total, float *f_attr_grav);
+int fa2_batch_get_sort_order(fa2_batch *batch, uint32_t *order);
+int fa2_batch_get_speed(fa2_batch *batch, float *global_speed, float *speed_efficiency);
+
+/* ------------------------------------------------------------------------
  * Repulsion without allocation.  No counterpart in the reference: there the
  * repulsion runs only inside CUDAForceAtlas2::doStep, on buffers that the
  * constructor allocated (src/RPGPUForceAtlas2.cu:109-149).

@@ -175,3 +175,24 @@ def test_cli_argument_checks(tmp_path):
     assert r.returncode != 0 and "No output folder" in r.stderr
     r = _cli("cpu", "5", "1", "sg", "1", "1", "approximate", str(p), str(tmp_path), "bin")
     assert r.returncode != 0 and "GPU" in r.stderr
+
+
+def test_batch_create_checks_arguments_before_the_device():
+    """fa2_batch_create refuses bad graphs and graphs past FA2_BATCH_MAX_NODES
+    with a status, before it looks for a device."""
+    import ctypes as C
+    from gpugraphlayout_b200 import _native as N
+    L = N.lib()
+    p = N.Params()
+    L.fa2_default_params(C.byref(p))
+    s = np.array([0, 1], np.uint32)
+    t = np.array([1, 1], np.uint32)  # a self-loop
+    d = (N.GraphDesc * 1)()
+    d[0] = N.GraphDesc(3, 2, s.ctypes.data, t.ctypes.data)
+    st = C.c_int(-1)
+    assert not L.fa2_batch_create(1, d, C.byref(p), C.byref(st))
+    assert st.value == 1  # FA2_ERR_INVALID_ARGUMENT
+    t2 = np.array([1, 2], np.uint32)
+    d[0] = N.GraphDesc(N.FA2_BATCH_MAX_NODES + 1, 2, s.ctypes.data, t2.ctypes.data)
+    assert not L.fa2_batch_create(1, d, C.byref(p), C.byref(st))
+    assert st.value == 6  # FA2_ERR_TOO_LARGE
