@@ -24,7 +24,7 @@ import numpy as np
 from ._native import Fa2Error, GraphDesc, Params, Stats, check, lib
 
 __all__ = ["Engine", "BatchEngine", "UGraph", "GraphLayout", "CUDAForceAtlas2", "Fa2Error", "kernel_names",
-           "random_positions"]
+           "random_positions", "render_rgb", "write_png"]
 
 
 def _ptr(a: np.ndarray):
@@ -334,6 +334,32 @@ class GraphLayout:
 
     def writeToBin(self, path: str):
         self._write(path, 1)
+
+    def writeToPNG(self, image_w: int, image_h: int, path: str):
+        """The reference's picture of the layout, rendered on the GPU."""
+        check(lib().fa2_write_png(self.graph._h, _ptr(np.ascontiguousarray(self.xy)),
+                                  int(image_w), int(image_h), str(path).encode()),
+              f"write {path}")
+
+
+def render_rgb(num_nodes: int, sources, targets, xy, image_w: int, image_h: int,
+               device: int = 0) -> np.ndarray:
+    """GraphLayout::writeToPNG's picture as an (image_h, image_w, 3) uint8
+    array, top row first, rendered on the GPU."""
+    s = np.ascontiguousarray(sources, np.uint32)
+    t = np.ascontiguousarray(targets, np.uint32)
+    p = np.ascontiguousarray(xy, np.float32).reshape(-1, 2)
+    out = np.zeros((image_h, image_w, 3), np.uint8)
+    check(lib().fa2_render_rgb(int(num_nodes), len(s), _ptr(s), _ptr(t), _ptr(p), int(image_w),
+                               int(image_h), int(device), _ptr(out)), "fa2_render_rgb")
+    return out
+
+
+def write_png(rgb, path: str) -> None:
+    """An 8-bit RGB PNG of an (h, w, 3) uint8 array."""
+    a = np.ascontiguousarray(rgb, np.uint8)
+    check(lib().fa2_png_encode(_ptr(a), a.shape[1], a.shape[0], str(path).encode()),
+          f"write {path}")
 
 
 class CUDAForceAtlas2:

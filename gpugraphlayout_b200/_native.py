@@ -20,7 +20,7 @@ EXPORTS = (
     "fa2_get_speed_state", "fa2_set_force_params", "fa2_set_linlog", "fa2_set_overlap",
     "fa2_batch_create", "fa2_batch_destroy", "fa2_batch_set_positions", "fa2_batch_get_positions",
     "fa2_batch_step", "fa2_batch_step_timed", "fa2_batch_get_forces", "fa2_batch_get_sort_order",
-    "fa2_batch_get_speed", "fa2_repulsion_noalloc", "fa2_ugraph_load",
+    "fa2_batch_get_speed", "fa2_render_rgb", "fa2_png_encode", "fa2_write_png", "fa2_repulsion_noalloc", "fa2_ugraph_load",
     "fa2_ugraph_from_pairs", "fa2_ugraph_free", "fa2_ugraph_num_nodes",
     "fa2_ugraph_num_edges", "fa2_ugraph_node_map_r", "fa2_ugraph_degrees",
     "fa2_ugraph_edges", "fa2_random_positions", "fa2_write_layout",
@@ -100,6 +100,10 @@ def lib():
     L.fa2_set_force_params.argtypes = [vp, C.c_float, C.c_float]
     L.fa2_set_overlap.argtypes = [vp, C.c_int32]
     L.fa2_set_linlog.argtypes = [vp, C.c_int32]
+    L.fa2_render_rgb.argtypes = [C.c_uint32, C.c_uint64, vp, vp, vp, C.c_int32, C.c_int32,
+                                 C.c_int32, vp]
+    L.fa2_png_encode.argtypes = [vp, C.c_int32, C.c_int32, C.c_char_p]
+    L.fa2_write_png.argtypes = [vp, vp, C.c_int32, C.c_int32, C.c_char_p]
     L.fa2_batch_create.restype = vp
     L.fa2_batch_create.argtypes = [C.c_uint32, vp, C.POINTER(Params), ip]
     L.fa2_batch_destroy.argtypes = [vp]

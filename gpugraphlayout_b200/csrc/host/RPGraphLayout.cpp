@@ -1,10 +1,12 @@
 // RPGraphLayout.cpp -- include/RPGraphLayout.hpp.
 #include "RPGraphLayout.hpp"
+#include "fa2b200.h"
 
 #include <stdio.h>
 #include <stdlib.h>
 
 #include <cmath>
+#include <algorithm>
 #include <fstream>
 #include <limits>
 
@@ -104,11 +106,23 @@ namespace RPGraph
         setY(node_id, c.y);
     }
 
-    void GraphLayout::writeToPNG(const int, const int, std::string path)
+    // src/RPGraphLayout.cpp:170-207: rendered on the GPU (fa2_render_rgb) and
+    // written by this library's PNG encoder; errors print and exit, as the
+    // reference's library calls do.
+    void GraphLayout::writeToPNG(const int image_w, const int image_h, std::string path)
     {
-        fprintf(stderr, "error: PNG output (%s) needs libpng, which this build does not use; "
-                        "use csv or bin.\n", path.c_str());
-        exit(EXIT_FAILURE);
+        std::vector<nid_t> s, t;
+        graph.edges(s, t);
+        std::vector<uint32_t> su(s.begin(), s.end()), tu(t.begin(), t.end());
+        std::vector<uint8_t> rgb((size_t)std::max(image_w, 0) * (size_t)std::max(image_h, 0) * 3);
+        int st = fa2_render_rgb(graph.num_nodes(), su.size(), su.data(), tu.data(), data(),
+                                image_w, image_h, 0, rgb.data());
+        if (st == FA2_OK) st = fa2_png_encode(rgb.data(), image_w, image_h, path.c_str());
+        if (st != FA2_OK)
+        {
+            fprintf(stderr, "error: writing %s: %s\n", path.c_str(), fa2_status_string(st));
+            exit(EXIT_FAILURE);
+        }
     }
 
     void GraphLayout::writeToCSV(std::string path)

@@ -2,6 +2,7 @@
 // GraphLayout behind plain C, for FFI callers (ctypes, cgo, JNI).
 #include <stdlib.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "RPGraphLayout.hpp"
@@ -93,6 +94,19 @@ int fa2_write_layout(const fa2_ugraph *h, const float *xy, const char *path, int
     else
         layout.writeToCSV(path);
     return is_file_exists(path) ? FA2_OK : FA2_ERR_IO;
+}
+
+int fa2_write_png(const fa2_ugraph *h, const float *xy, int32_t image_w, int32_t image_h,
+                  const char *path) {
+    if (!h || !path || (!xy && h->g->num_nodes())) return FA2_ERR_INVALID_ARGUMENT;
+    std::vector<RPGraph::nid_t> s, t;
+    h->g->edges(s, t);
+    std::vector<uint32_t> su(s.begin(), s.end()), tu(t.begin(), t.end());
+    std::vector<uint8_t> rgb((size_t)std::max(image_w, 0) * (size_t)std::max(image_h, 0) * 3);
+    int st = fa2_render_rgb(h->g->num_nodes(), su.size(), su.data(), tu.data(), xy, image_w,
+                            image_h, 0, rgb.data());
+    if (st) return st;
+    return fa2_png_encode(rgb.data(), image_w, image_h, path);
 }
 
 }  // extern "C"

@@ -7,8 +7,8 @@
 // Same arguments, checks, output names (<edgelist basename>_<iter>.<fmt>) and
 // progress lines.  Differences: this build provides the GPU path only, so
 // `cpu` is refused with a message; with exactly ten arguments the format
-// defaults to png (the reference reads argv[10] past the end there); png
-// output is refused because libpng is not used.
+// defaults to png (the reference reads argv[10] past the end there).  png
+// output is rendered on the GPU and written by this library's PNG encoder.
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>

@@ -2,8 +2,10 @@
  * RPGraphLayout.hpp -- 2-D positions of a UGraph's nodes (drop-in for the
  * reference's src/RPGraphLayout.hpp:31-67).  Writers produce the reference's
  * formats: CSV "id,x,y" and binary {uint32 id, float x, float y} per node, in
- * UGraph id order with edge-list ids.  PNG output needs libpng, which this
- * build does not use: writeToPNG reports that and exits.
+ * UGraph id order with edge-list ids.  writeToPNG renders the reference's
+ * picture (node discs and edge lines blended black on white) on the GPU and
+ * writes it with this library's own PNG encoder (fa2_render_rgb,
+ * fa2_png_encode in fa2b200.h): pngwriter and libpng are not used.
  */
 #ifndef RPGraphLayout_hpp
 #define RPGraphLayout_hpp

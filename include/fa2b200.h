@@ -278,6 +278,34 @@ void fa2_random_positions(uint32_t n, float width, float height, uint32_t seed, 
  * positions xy for graph g.  Refuses (FA2_ERR_IO) an existing file. */
 int fa2_write_layout(const fa2_ugraph *g, const float *xy, const char *path, int binary);
 
+/* ------------------------------------------------------------------------
+ * Headless rendering: the picture of GraphLayout::writeToPNG
+ * (src/RPGraphLayout.cpp:170-207) drawn on the GPU.  Every node is a filled
+ * disc of radius 3 px blended black at opacity 10000 / num_nodes, every edge
+ * a line blended black at opacity 100000 / num_edges, on white, the layout's
+ * bounding box scaled to the image.  Blending black scales a pixel by
+ * (1 - opacity), so the image is a product over the plots covering each
+ * pixel, independent of drawing order.  pngwriter, which the reference draws
+ * with, is not part of its sources; the pixel rules are: positions truncated
+ * to int as the reference computes them, pixel (x, y) 1-based with y up; a
+ * disc is every pixel within distance 3; a line the Bresenham pixels between
+ * its integer end points.
+ * ---------------------------------------------------------------------- */
+
+/* Renders into rgb (image_w * image_h * 3 bytes, top row first) on CUDA device
+ * `device`.  Edges as fa2_ugraph_edges lists them, each once. */
+int fa2_render_rgb(uint32_t num_nodes, uint64_t num_edges, const uint32_t *sources,
+                   const uint32_t *targets, const float *xy, int32_t image_w, int32_t image_h,
+                   int32_t device, uint8_t *rgb);
+
+/* Writes an 8-bit RGB PNG of rgb (image_w * image_h * 3 bytes, top row first). */
+int fa2_png_encode(const uint8_t *rgb, int32_t image_w, int32_t image_h, const char *path);
+
+/* GraphLayout::writeToPNG of positions xy for graph g, rendered on device 0;
+ * like the reference it overwrites an existing file. */
+int fa2_write_png(const fa2_ugraph *g, const float *xy, int32_t image_w, int32_t image_h,
+                  const char *path);
+
 /* Human-readable text of a status code. */
 const char *fa2_status_string(int status);
 

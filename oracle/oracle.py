@@ -472,3 +472,61 @@ class RefGPUEmu:
         if getattr(self, "_h", None):
             ref_gpuemu().refgpu_destroy(self._h)
             self._h = None
+
+
+# -------------------------------------------------------------- rendering --
+
+def render(n: int, sources, targets, xy, image_w: int, image_h: int) -> np.ndarray:
+    """The layout picture of GraphLayout::writeToPNG (src/RPGraphLayout.cpp:
+    170-207) restated with the pixel rules of the engine's renderer: frame in
+    the reference's float/double arithmetic, positions truncated to int,
+    1-based pixels with y up; discs of radius 3; Bresenham lines; each pixel
+    white times (1 - a_node)^discs (1 - a_edge)^lines, black once a plot with
+    opacity >= 1 covers it.  Returns (h, w, 3) uint8, top row first."""
+    f32 = np.float32
+    xy = np.asarray(xy, f32).reshape(-1, 2)
+    s = np.asarray(sources, np.int64)
+    t = np.asarray(targets, np.int64)
+    mnx, mxx = f32(xy[:, 0].min()), f32(xy[:, 0].max())
+    mny, mxy = f32(xy[:, 1].min()), f32(xy[:, 1].max())
+    x_range, y_range = f32(mxx - mnx), f32(mxy - mny)
+    x_center = f32(np.float64(mnx) + np.float64(x_range) / 2.0)
+    y_center = f32(np.float64(mny) + np.float64(y_range) / 2.0)
+    minx = f32(np.float64(x_center) - np.float64(x_range) / 2.0)
+    miny = f32(np.float64(y_center) - np.float64(y_range) / 2.0)
+    with np.errstate(divide="ignore"):
+        xs, ys = f32(f32(image_w) / x_range), f32(f32(image_h) / y_range)
+    a_node = f32(10000.0 / n)
+    a_edge = f32(100000.0 / len(s)) if len(s) else f32(np.inf)
+    px = np.trunc(f32(xy[:, 0] - minx) * xs).astype(np.int64)
+    py = np.trunc(f32(xy[:, 1] - miny) * ys).astype(np.int64)
+    cn = np.zeros((image_h, image_w), np.int64)
+    ce = np.zeros((image_h, image_w), np.int64)
+
+    def plot(cnt, x, y):
+        ok = (x >= 1) & (x <= image_w) & (y >= 1) & (y <= image_h)
+        np.add.at(cnt, (image_h - y[ok], x[ok] - 1), 1)
+
+    for dy in range(-3, 4):
+        for dx in range(-3, 4):
+            if dx * dx + dy * dy <= 9:
+                plot(cn, px + dx, py + dy)
+    if len(s):
+        x1, y1, x2, y2 = px[s], py[s], px[t], py[t]
+        ax, ay = np.abs(x2 - x1), np.abs(y2 - y1)
+        sx, sy = np.where(x2 >= x1, 1, -1), np.where(y2 >= y1, 1, -1)
+        xmajor = ax >= ay
+        D, d = np.where(xmajor, ax, ay), np.where(xmajor, ay, ax)
+        steps = D + 1
+        e = np.repeat(np.arange(len(s)), steps)
+        tt = np.arange(steps.sum()) - np.repeat(np.cumsum(steps) - steps, steps)
+        De, de = D[e], d[e]
+        mi = np.where(De > 0, (2 * tt * de + De) // np.maximum(2 * De, 1), 0)
+        x = np.where(xmajor[e], x1[e] + sx[e] * tt, x1[e] + sx[e] * mi)
+        y = np.where(xmajor[e], y1[e] + sy[e] * mi, y1[e] + sy[e] * tt)
+        plot(ce, x, y)
+    with np.errstate(over="ignore", invalid="ignore"):
+        v = np.power(1.0 - np.float64(a_node), cn) * np.power(1.0 - np.float64(a_edge), ce)
+    v = np.where(((cn > 0) & (a_node >= 1)) | ((ce > 0) & (a_edge >= 1)), 0.0, v)
+    c = np.minimum(255.0, np.floor(v * 255.0 + 0.5)).astype(np.uint8)
+    return np.repeat(c[:, :, None], 3, axis=2)

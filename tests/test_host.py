@@ -196,3 +196,38 @@ def test_batch_create_checks_arguments_before_the_device():
     d[0] = N.GraphDesc(N.FA2_BATCH_MAX_NODES + 1, 2, s.ctypes.data, t2.ctypes.data)
     assert not L.fa2_batch_create(1, d, C.byref(p), C.byref(st))
     assert st.value == 6  # FA2_ERR_TOO_LARGE
+
+
+def _read_png(path):
+    """Minimal PNG reader for 8-bit RGB, filter-0 files (what the engine writes):
+    checks the signature and every chunk's CRC, returns an (h, w, 3) array."""
+    import struct
+    import zlib
+    data = open(path, "rb").read()
+    assert data[:8] == b"\x89PNG\r\n\x1a\n"
+    pos, idat, w = 8, b"", None
+    while pos < len(data):
+        (n,) = struct.unpack(">I", data[pos:pos + 4])
+        kind = data[pos + 4:pos + 8]
+        body = data[pos + 8:pos + 8 + n]
+        (crc,) = struct.unpack(">I", data[pos + 8 + n:pos + 12 + n])
+        assert zlib.crc32(kind + body) == crc
+        if kind == b"IHDR":
+            w, h, depth, ctype, comp, filt, inter = struct.unpack(">IIBBBBB", body)
+            assert (depth, ctype, comp, filt, inter) == (8, 2, 0, 0, 0)
+        elif kind == b"IDAT":
+            idat += body
+        pos += 12 + n
+    raw = np.frombuffer(zlib.decompress(idat), np.uint8).reshape(h, 1 + 3 * w)
+    assert (raw[:, 0] == 0).all()
+    return raw[:, 1:].reshape(h, w, 3)
+
+
+def test_png_encoder_round_trip(tmp_path):
+    from gpugraphlayout_b200 import write_png
+    rng = np.random.default_rng(0)
+    for h, w in ((5, 7), (1, 1), (300, 257)):  # the last needs several stored blocks
+        img = rng.integers(0, 256, (h, w, 3), dtype=np.uint8)
+        path = str(tmp_path / f"x{h}_{w}.png")
+        write_png(img, path)
+        assert np.array_equal(_read_png(path), img)
