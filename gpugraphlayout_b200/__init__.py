@@ -57,7 +57,7 @@ class Engine:
     def __init__(self, num_nodes: int, sources, targets, *, strong_gravity: bool = False,
                  gravity: float = 1.0, scale: float = 1.0, theta: float = 1.0,
                  epssq: float = 0.05 * 0.05, device: int = 0, use_barneshut: bool = True,
-                 linlog: bool = False):
+                 linlog: bool = False, multipole: int = 1):
         L = lib()
         self._src = np.ascontiguousarray(sources, np.uint32)
         self._dst = np.ascontiguousarray(targets, np.uint32)
@@ -68,6 +68,7 @@ class Engine:
         p.strong_gravity = int(strong_gravity)
         p.gravity, p.scale, p.theta, p.epssq, p.device = gravity, scale, theta, epssq, device
         p.linlog = int(linlog)
+        p.multipole = int(multipole)
         st = C.c_int(0)
         self._ctx = L.fa2_create(C.byref(g), C.byref(p), C.byref(st))
         check(st.value, "fa2_create")
@@ -123,6 +124,22 @@ class Engine:
     def set_linlog(self, enable: bool) -> None:
         """Linear-log (True) or linear (False) attraction from the next step on."""
         check(lib().fa2_set_linlog(self._ctx, 1 if enable else 0), "fa2_set_linlog")
+
+    def set_approximation(self, theta: float, multipole: int = 1) -> None:
+        """Barnes-Hut opening parameter and far-field order from the next step
+        on: multipole 1 treats accepted cells as point masses (the reference),
+        2 adds each cell's quadrupole term."""
+        check(lib().fa2_set_approximation(self._ctx, float(theta), int(multipole)),
+              "fa2_set_approximation")
+
+    def exact_repulsion(self, samples) -> np.ndarray:
+        """Exact all-pairs repulsion (float64, computed on the GPU) of the
+        nodes ``samples`` (reference ids) at the current positions, (k, 2)."""
+        ids = np.ascontiguousarray(samples, np.uint32)
+        out = np.zeros((len(ids), 2), np.float64)
+        check(lib().fa2_exact_repulsion(self._ctx, len(ids), _ptr(ids), _ptr(out)),
+              "fa2_exact_repulsion")
+        return out
 
     def set_overlap(self, enable: bool) -> None:
         """Attraction beside the tree build (default) or alone before it."""

@@ -18,6 +18,7 @@ EXPORTS = (
     "fa2_get_positions", "fa2_step", "fa2_step_timed", "fa2_kernel_name",
     "fa2_get_stats", "fa2_get_forces", "fa2_get_sort_order", "fa2_set_speed_state",
     "fa2_get_speed_state", "fa2_set_force_params", "fa2_set_linlog", "fa2_set_overlap",
+    "fa2_set_approximation", "fa2_exact_repulsion", "fa2_last_cuda_error",
     "fa2_batch_create", "fa2_batch_destroy", "fa2_batch_set_positions", "fa2_batch_get_positions",
     "fa2_batch_step", "fa2_batch_step_timed", "fa2_batch_get_forces", "fa2_batch_get_sort_order",
     "fa2_batch_get_speed", "fa2_render_rgb", "fa2_png_encode", "fa2_write_png", "fa2_repulsion_noalloc", "fa2_ugraph_load",
@@ -46,7 +47,7 @@ class Params(C.Structure):
     _fields_ = [("use_barneshut", C.c_int32), ("strong_gravity", C.c_int32),
                 ("gravity", C.c_float), ("scale", C.c_float), ("theta", C.c_float),
                 ("epssq", C.c_float), ("jitter_tolerance", C.c_float), ("k_s_max", C.c_float),
-                ("device", C.c_int32), ("linlog", C.c_int32)]
+                ("device", C.c_int32), ("linlog", C.c_int32), ("multipole", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -64,6 +65,10 @@ class Fa2Error(RuntimeError):
         self.status = status
         name = STATUS_NAMES.get(status, str(status))
         text = _lib.fa2_status_string(status).decode() if _lib else name
+        if _lib and status == 3:  # FA2_ERR_CUDA: the runtime's own error and where
+            detail = _lib.fa2_last_cuda_error().decode()
+            if detail:
+                text = f"{text}: {detail}"
         super().__init__(f"{what}: {name} ({text})" if what else f"{name} ({text})")
 
 
@@ -100,6 +105,10 @@ def lib():
     L.fa2_set_force_params.argtypes = [vp, C.c_float, C.c_float]
     L.fa2_set_overlap.argtypes = [vp, C.c_int32]
     L.fa2_set_linlog.argtypes = [vp, C.c_int32]
+    L.fa2_set_approximation.argtypes = [vp, C.c_float, C.c_int32]
+    L.fa2_exact_repulsion.argtypes = [vp, C.c_int32, vp, vp]
+    L.fa2_last_cuda_error.restype = C.c_char_p
+    L.fa2_last_cuda_error.argtypes = []
     L.fa2_render_rgb.argtypes = [C.c_uint32, C.c_uint64, vp, vp, vp, C.c_int32, C.c_int32,
                                  C.c_int32, vp]
     L.fa2_png_encode.argtypes = [vp, C.c_int32, C.c_int32, C.c_char_p]

@@ -195,10 +195,14 @@ __device__ void phase_attract(const BatchArgs &A, uint32_t base, uint32_t n, flo
 __device__ void phase_bbox(const BatchArgs &A, uint32_t base, uint32_t n, BatchSmem &S) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     float4 a = make_float4(FLT_MAX, -FLT_MAX, FLT_MAX, -FLT_MAX);
+    bool bad = false;
     for (uint32_t i = threadIdx.x; i < n; i += kBThreads) {
         const float2 p = A.pos[base + i];
         a = make_float4(fminf(a.x, p.x), fmaxf(a.y, p.x), fminf(a.z, p.y), fmaxf(a.w, p.y));
+        bad |= !(isfinite(p.x) && isfinite(p.y));
     }
+    // a NaN or infinite position stops this graph's iterations
+    if (__any_sync(kFullMask, bad) && lane == 0) atomicOr(&S.err, kErrNonFinite);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         a.x = fminf(a.x, __shfl_xor_sync(kFullMask, a.x, o));
@@ -490,7 +494,8 @@ __device__ void phase_traverse(const BatchArgs &A, uint32_t base, uint32_t n, ch
                 const int meta = __float_as_int(r.w);
                 const float dx = px - r.x, dy = py - r.y;
                 const float d2 = dx * dx + dy * dy + A.prm.epssq;
-                if (__all_sync(kFullMask, d2 >= S.dq[meta_level(meta)])) {
+                // !(d2 < dq): a NaN distance accepts, so the walk still ends
+                if (__all_sync(kFullMask, !(d2 < S.dq[meta_level(meta)]))) {
                     const float c = __fdividef(r.z, d2);
                     ax = fmaf(dx, c, ax);
                     ay = fmaf(dy, c, ay);
@@ -591,6 +596,7 @@ __global__ void __launch_bounds__(kBThreads, 1) k_batch(BatchArgs A) {
             if (S.err) break;
             phase_attract<LINLOG>(A, base, n, fa);
             phase_bbox(A, base, n, S);
+            if (S.err) break;
             phase_keys_sort(A, base, n, slot, S, 0);
             // Exactly coincident bodies: scale the later ones by .99 (the
             // reference's re-insertion, src/RPBHKernels.cu:271-278) and build
@@ -743,7 +749,8 @@ fa2_batch *fa2_batch_create(uint32_t num_graphs, const fa2_graph_desc *graphs,
     if (!status) status = &dummy;
     *status = FA2_ERR_INVALID_ARGUMENT;
     if (!prm || (num_graphs && !graphs)) return nullptr;
-    if (!prm->use_barneshut) {
+    // the batched walk uses cells as point masses only
+    if (!prm->use_barneshut || prm->multipole > 1) {
         *status = FA2_ERR_UNSUPPORTED;
         return nullptr;
     }
@@ -801,6 +808,7 @@ fa2_batch *fa2_batch_create(uint32_t num_graphs, const fa2_graph_desc *graphs,
     b->kp.epssq = prm->epssq;
     b->kp.strong_gravity = prm->strong_gravity;
     b->kp.linlog = prm->linlog != 0;
+    b->kp.multipole = 1;
     b->kp.nsm = b->nsm;
 
     // host layout: graphs back to back, each graph's nodes in id order;
@@ -909,6 +917,14 @@ int fa2_batch_set_positions(fa2_batch *b, const float *xy) {
     BCK(cudaSetDevice(b->device));
     if (!b->total_nodes) return FA2_OK;
     BCK(cudaMemcpyAsync(b->args.pos, xy, b->total_nodes * 8, cudaMemcpyHostToDevice, b->stream));
+    // new positions clear the graphs' device errors, which depend on them
+    std::vector<BatchSpeed> sp(b->num_graphs);
+    BCK(cudaMemcpyAsync(sp.data(), b->args.speed, sp.size() * sizeof(BatchSpeed),
+                        cudaMemcpyDeviceToHost, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+    for (BatchSpeed &x : sp) x.err = 0;
+    BCK(cudaMemcpyAsync(b->args.speed, sp.data(), sp.size() * sizeof(BatchSpeed),
+                        cudaMemcpyHostToDevice, b->stream));
     BCK(cudaStreamSynchronize(b->stream));
     return FA2_OK;
 }

@@ -23,10 +23,15 @@ using namespace fa2;
 
 namespace {
 
-constexpr int kNumSlots = 7;
-const char *const kSlotNames[kNumSlots] = {"attract", "keys",     "sort",    "tree_count",
-                                           "emit",    "traverse", "displace"};
-enum Slot { S_ATTRACT, S_KEYS, S_SORT, S_COUNT, S_EMIT, S_TRAV, S_DISP };
+constexpr int kNumSlots = 9;
+const char *const kSlotNames[kNumSlots] = {"attract",  "keys",     "sort",    "tree_count",
+                                           "emit",     "traverse", "displace", "moments",
+                                           "quadrupole"};
+enum Slot { S_ATTRACT, S_KEYS, S_SORT, S_COUNT, S_EMIT, S_TRAV, S_DISP, S_MOM, S_QUAD };
+
+// The last CUDA error a call of this thread met, with the source line that saw
+// it (fa2_last_cuda_error).
+thread_local char g_last_cuda_error[192] = "";
 
 constexpr int kMaxReplayRounds = 64;
 
@@ -51,7 +56,7 @@ struct fa2_ctx {
     uint32_t *stage_ids = nullptr; // n
     int bbox_blocks = 0, trav_blocks = 0;
     cudaStream_t sA = nullptr, sB = nullptr;
-    cudaEvent_t evFork = nullptr, evJoin = nullptr;
+    cudaEvent_t evFork = nullptr, evJoin = nullptr, evCounted = nullptr;
     // graphs
     cudaGraphExec_t exec = nullptr;
     cudaGraphExec_t exec_timed = nullptr;
@@ -74,11 +79,14 @@ void drop_graphs(fa2_ctx *c) {
     c->graph_timed = nullptr;
 }
 
-int cuda_status(cudaError_t e) {
+int cuda_status_at(cudaError_t e, int line) {
     if (e == cudaSuccess) return FA2_OK;
+    snprintf(g_last_cuda_error, sizeof(g_last_cuda_error), "%s (%s) at fa2_capi.cu:%d",
+             cudaGetErrorName(e), cudaGetErrorString(e), line);
     if (e == cudaErrorMemoryAllocation) return FA2_ERR_OUT_OF_MEMORY;
     return FA2_ERR_CUDA;
 }
+#define cuda_status(e) cuda_status_at((e), __LINE__)
 
 #define CK(call)                                   \
     do {                                           \
@@ -96,6 +104,19 @@ int dalloc(fa2_ctx *c, T **p, size_t count) {
     return FA2_OK;
 }
 
+// Buffers of the quadrupole option, allocated when it is first selected.
+int ensure_quad_buffers(fa2_ctx *c) {
+    Buffers &b = c->b;
+    int s = FA2_OK;
+    if ((!b.quad && (s = dalloc(c, &b.quad, b.capacity))) ||
+        (!b.pmom && (s = dalloc(c, &b.pmom, (size_t)b.n + 1))) ||
+        (!b.mom_lb && (s = dalloc(c, &b.mom_lb, (size_t)mom_tiles(b.n)))) ||
+        (!b.mom_m && (s = dalloc(c, &b.mom_m, (size_t)b.n))) ||
+        (!b.mom_q && (s = dalloc(c, &b.mom_q, (size_t)b.n))))
+        return s;
+    return FA2_OK;
+}
+
 void free_all(fa2_ctx *c) {
     if (c->exec) cudaGraphExecDestroy(c->exec);
     if (c->exec_timed) cudaGraphExecDestroy(c->exec_timed);
@@ -106,6 +127,7 @@ void free_all(fa2_ctx *c) {
     c->allocs.clear();
     if (c->evFork) cudaEventDestroy(c->evFork);
     if (c->evJoin) cudaEventDestroy(c->evJoin);
+    if (c->evCounted) cudaEventDestroy(c->evCounted);
     if (c->sA) cudaStreamDestroy(c->sA);
     if (c->sB) cudaStreamDestroy(c->sB);
 }
@@ -186,6 +208,8 @@ void enqueue_iteration(fa2_ctx *c, bool full, bool perturb_first, bool timed) {
         if (timed)
             cudaEventRecordWithFlags(c->slot_events[slot * 2 + end], s, cudaEventRecordExternal);
     };
+    const bool quad = c->kp.multipole >= 2;
+    const bool side = full && c->overlap;  // stream B carries the attraction
     cudaMemsetAsync(c->scratch, 0, c->scratch_bytes, A);
     if (full && !c->overlap) {
         mark(S_ATTRACT, 0, A);
@@ -197,7 +221,7 @@ void enqueue_iteration(fa2_ctx *c, bool full, bool perturb_first, bool timed) {
         mark(S_ATTRACT, 0, B);
         launch_attract(b, c->kp, c->plan, B);
         mark(S_ATTRACT, 1, B);
-        cudaEventRecord(c->evJoin, B);
+        if (!quad) cudaEventRecord(c->evJoin, B);
     }
     if (perturb_first) launch_runs(b, 1, c->nsm, A);
     mark(S_KEYS, 0, A);
@@ -207,12 +231,30 @@ void enqueue_iteration(fa2_ctx *c, bool full, bool perturb_first, bool timed) {
     launch_sort(b, A);
     mark(S_SORT, 1, A);
     mark(S_COUNT, 0, A);
-    launch_tree_count(b, A);
+    launch_tree_count(b, quad, A);
     mark(S_COUNT, 1, A);
+    // The tree count leaves the sorted bodies' grid offsets and masses for the
+    // moment scan; with stream B in use the scan runs there, beside the emit.
+    if (quad) {
+        cudaStream_t M = side ? B : A;
+        if (side) {
+            cudaEventRecord(c->evCounted, A);
+            cudaStreamWaitEvent(B, c->evCounted, 0);
+        }
+        mark(S_MOM, 0, M);
+        launch_moments(b, M);
+        mark(S_MOM, 1, M);
+        if (side) cudaEventRecord(c->evJoin, B);
+    }
     mark(S_EMIT, 0, A);
     launch_emit(b, c->nsm, A);
     mark(S_EMIT, 1, A);
-    if (full && c->overlap) cudaStreamWaitEvent(A, c->evJoin, 0);
+    if (side) cudaStreamWaitEvent(A, c->evJoin, 0);
+    if (quad) {
+        mark(S_QUAD, 0, A);
+        launch_quad_cells(b, c->nsm, A);
+        mark(S_QUAD, 1, A);
+    }
     mark(S_TRAV, 0, A);
     launch_traverse(b, c->kp, c->trav_blocks, A);
     mark(S_TRAV, 1, A);
@@ -349,6 +391,7 @@ void fa2_default_params(fa2_params *p) {
     p->k_s_max = 10.0f;
     p->device = 0;
     p->linlog = 0;
+    p->multipole = 1;
 }
 
 fa2_ctx *fa2_create(const fa2_graph_desc *g, const fa2_params *prm, int *status) {
@@ -397,6 +440,7 @@ fa2_ctx *fa2_create(const fa2_graph_desc *g, const fa2_params *prm, int *status)
     c->kp.epssq = prm->epssq;
     c->kp.strong_gravity = prm->strong_gravity;
     c->kp.linlog = prm->linlog != 0;
+    c->kp.multipole = prm->multipole >= 2 ? 2 : 1;
 
     std::vector<uint32_t> off;
     std::vector<int32_t> col;
@@ -432,6 +476,7 @@ fa2_ctx *fa2_create(const fa2_graph_desc *g, const fa2_params *prm, int *status)
         (s = dalloc(c, &b.st, 1)) || (s = dalloc(c, &c->stage_xy, n)) ||
         (s = dalloc(c, &c->stage_ids, n)))
         return fail(s);
+    if (c->kp.multipole >= 2 && (s = ensure_quad_buffers(c))) return fail(s);
     c->bbox_blocks = c->nsm * 2;
     // partial boxes of k_bbox (bbox_blocks) and of k_displace (up to 4 per SM)
     if ((s = dalloc(c, &b.bbox_partial, (size_t)c->nsm * 4))) return fail(s);
@@ -444,13 +489,15 @@ fa2_ctx *fa2_create(const fa2_graph_desc *g, const fa2_params *prm, int *status)
     b.sort_rounds = sort_rounds((int)n, c->nsm);
     const size_t sort_counts = (size_t)8 * sort_tiles_max((int)n) * 256;
     const size_t count_status = (size_t)count_tiles((int)n);
-    c->scratch_bytes = sizeof(IterCounters) + 4 * (sort_counts + count_status);
+    const size_t mom_status = (size_t)mom_tiles((int)n);
+    c->scratch_bytes = sizeof(IterCounters) + 4 * (sort_counts + count_status + mom_status);
     char *scr = nullptr;
     if ((s = dalloc(c, &scr, c->scratch_bytes))) return fail(s);
     c->scratch = scr;
     b.ctr = (IterCounters *)scr;
     b.sort_counts = (uint32_t *)(scr + sizeof(IterCounters));
     b.count_status = b.sort_counts + sort_counts;
+    b.mom_status = b.count_status + count_status;
 
     // The tree chain (stream A) is the critical path; the attraction (stream B)
     // only has to finish before the traversal.  With A at the higher priority
@@ -461,7 +508,8 @@ fa2_ctx *fa2_create(const fa2_graph_desc *g, const fa2_params *prm, int *status)
     if (cudaStreamCreateWithPriority(&c->sA, cudaStreamNonBlocking, prio_high) != cudaSuccess ||
         cudaStreamCreateWithPriority(&c->sB, cudaStreamNonBlocking, prio_low) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->evFork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->evJoin, cudaEventDisableTiming) != cudaSuccess)
+        cudaEventCreateWithFlags(&c->evJoin, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->evCounted, cudaEventDisableTiming) != cudaSuccess)
         return fail(FA2_ERR_CUDA);
     c->slot_events.resize(kNumSlots * 2);
     for (auto &e : c->slot_events)
@@ -507,8 +555,10 @@ int fa2_set_positions(fa2_ctx *c, const float *xy) {
     const size_t bytes = (size_t)c->n * 8;
     CK(cudaMemcpyAsync(c->stage_xy, xy, bytes, cudaMemcpyHostToDevice, c->sA));
     launch_scatter_xy((int)c->n, c->b.ref_of, c->stage_xy, c->b.pos, c->sA);
-    // the root cell of the next tree comes from these positions
+    // the root cell of the next tree comes from these positions; device
+    // errors of earlier positions are cleared (k_bbox flags non-finite ones)
     CK(cudaMemsetAsync(c->scratch, 0, c->scratch_bytes, c->sA));
+    CK(cudaMemsetAsync(&c->b.st->err, 0, sizeof(int), c->sA));
     launch_bbox(c->b, c->bbox_blocks, c->sA);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(c->sA));
@@ -676,6 +726,60 @@ int fa2_set_linlog(fa2_ctx *c, int32_t enable) {
     drop_graphs(c);
     return FA2_OK;
 }
+
+int fa2_set_approximation(fa2_ctx *c, float theta, int32_t multipole) {
+    if (!c || !(theta > 0.0f) || multipole < 1 || multipole > 2) return FA2_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(c->device));
+    const float itolsq = 1.0f / (theta * theta);  // src/RPForceAtlas2.cpp:47
+    if (c->kp.itolsq == itolsq && c->kp.multipole == multipole) {
+        c->prm.theta = theta;
+        return FA2_OK;
+    }
+    CK(cudaStreamSynchronize(c->sA));
+    if (multipole >= 2) {
+        const int s = ensure_quad_buffers(c);
+        if (s) return s;
+    }
+    c->kp.itolsq = itolsq;
+    c->kp.multipole = multipole;
+    c->prm.theta = theta;
+    c->prm.multipole = multipole;
+    drop_graphs(c);  // theta and the walk variant are captured in the graphs
+    return FA2_OK;
+}
+
+int fa2_exact_repulsion(fa2_ctx *c, int32_t n_samples, const uint32_t *samples, double *out) {
+    if (!c || n_samples < 0 || (n_samples && (!samples || !out))) return FA2_ERR_INVALID_ARGUMENT;
+    if (n_samples == 0) return FA2_OK;
+    std::vector<uint32_t> internal(c->n);
+    for (uint32_t k = 0; k < c->n; ++k) internal[c->ref_of[k]] = k;
+    std::vector<uint32_t> ids((size_t)n_samples);
+    for (int32_t s = 0; s < n_samples; ++s) {
+        if (samples[s] >= c->n) return FA2_ERR_INVALID_ARGUMENT;
+        ids[s] = internal[samples[s]];
+    }
+    CK(cudaSetDevice(c->device));
+    uint32_t *d_ids = nullptr;
+    double2 *d_out = nullptr;
+    cudaError_t e = cudaMalloc(&d_ids, ids.size() * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&d_out, ids.size() * sizeof(double2));
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_ids, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, c->sA);
+    if (e == cudaSuccess) {
+        launch_exact_f64(c->b, c->kp, d_ids, n_samples, d_out, c->sA);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out, d_out, ids.size() * sizeof(double2), cudaMemcpyDeviceToHost,
+                            c->sA);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->sA);
+    const int s = cuda_status(e);
+    cudaFree(d_ids);
+    cudaFree(d_out);
+    return s;
+}
+
+const char *fa2_last_cuda_error(void) { return g_last_cuda_error; }
 
 int fa2_set_overlap(fa2_ctx *c, int32_t enable) {
     if (!c) return FA2_ERR_INVALID_ARGUMENT;

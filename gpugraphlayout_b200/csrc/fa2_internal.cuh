@@ -27,6 +27,7 @@ enum : int {
     kErrScanWait = 2,      // a tree-count tile waited too long
     kErrRunTooLong = 4,    // more than kMaxRun bodies share a 64-bit key
     kErrTreeTooLarge = 8,  // the quadtree needs more nodes than allocated
+    kErrNonFinite = 16,    // a position is NaN or infinite
 };
 
 // Scalars that live on the device for the whole run.
@@ -54,7 +55,8 @@ struct IterCounters {
     unsigned trav_ticket;
     unsigned trav_done;
     unsigned disp_done;
-    unsigned pad[3];
+    unsigned mom_ticket;
+    unsigned pad[2];
     unsigned hist[8][256];  // per-pass digit histograms of the sort keys
 };
 
@@ -84,6 +86,11 @@ inline int sort_rounds(int n, int nsm) {
 }
 inline int count_tiles(int n) { return (n + kCountTile - 1) / kCountTile; }
 
+// Moment scan (quadrupole option): bodies per tile and tiles.
+constexpr int kMomThreads = 256;
+constexpr int kMomTile = kMomThreads * 4;
+inline int mom_tiles(int n) { return (n + kMomTile - 1) / kMomTile; }
+
 // Attraction work split: rows (nodes in degree-descending order) with the
 // same number of lanes per row form one contiguous bucket.
 struct AttractBucket {
@@ -106,6 +113,20 @@ struct LookbackSums {
     __int128 agg_x, agg_y, incl_x, incl_y;
 };
 
+// Exact moments of a run of sorted bodies on the fixed-point grid of 2^-44
+// root radii (q = offset from the root centre): sum m q_x, sum m q_y,
+// sum m (q_x^2 - q_y^2), sum m q_x q_y.  With the total mass below 2^32 and
+// |q| <= 2^45 every sum stays below 2^123.
+struct Moments {
+    __int128 x, y, re, im;
+};
+
+// Look-back sums of one moment tile: its own total and, once known, the
+// total of every body up to its end.
+struct MomLookback {
+    Moments agg, incl;
+};
+
 struct Buffers {
     int n;
     // per node, internal (degree-descending) order
@@ -122,6 +143,12 @@ struct Buffers {
     uint32_t *group;          // n: first preorder node of body k's group
     uint32_t *body_node;      // n: preorder node of sorted body k
     uint32_t *owner;          // capacity: per node, sorted body k << 6 | cell offset (63: body)
+    float2 *quad;             // capacity: per cell, complex 2nd moment about its centre of mass
+    Moments *pmom;            // n + 1: exclusive prefix of the body moments (quadrupole only)
+    longlong2 *mom_q;         // n: sorted bodies' offsets on the 2^-44 grid (null: not kept)
+    uint32_t *mom_m;          // n: sorted bodies' masses
+    MomLookback *mom_lb;      // moment tiles: look-back sums
+    uint32_t *mom_status;     // [moment tiles]: look-back flags (in the cleared scratch)
     float4 *nodes;            // capacity + 1: x, y, mass, meta
     uint32_t capacity;
     long long *pm;            // n + 1: exclusive prefix of mass over sorted bodies
@@ -140,7 +167,8 @@ struct Buffers {
 struct Params {
     float k_r, k_g, itolsq, epssq;
     int strong_gravity;
-    int linlog;  // linear-log attraction
+    int linlog;     // linear-log attraction
+    int multipole;  // 1: monopole cells (the reference); 2: + quadrupole term
     int nsm;
 };
 
@@ -153,11 +181,15 @@ void launch_bbox(const Buffers &b, int nblocks, cudaStream_t s);
 void launch_keys(const Buffers &b, int nsm, cudaStream_t s);
 void launch_sort(const Buffers &b, cudaStream_t s);
 void launch_runs(const Buffers &b, int perturb, int nsm, cudaStream_t s);
-void launch_tree_count(const Buffers &b, cudaStream_t s);
+void launch_tree_count(const Buffers &b, bool keep_moments, cudaStream_t s);
+void launch_moments(const Buffers &b, cudaStream_t s);
 void launch_emit(const Buffers &b, int nsm, cudaStream_t s);
+void launch_quad_cells(const Buffers &b, int nsm, cudaStream_t s);
 void launch_traverse(const Buffers &b, const Params &p, int nblocks, cudaStream_t s);
 void launch_displace(const Buffers &b, int nsm, cudaStream_t s);
 void launch_count_interactions(const Buffers &b, const Params &p, int nblocks, cudaStream_t s);
+void launch_exact_f64(const Buffers &b, const Params &p, const uint32_t *ids, int n_ids,
+                      double2 *out, cudaStream_t s);
 void launch_attract(const Buffers &b, const Params &p, const AttractPlan &plan, cudaStream_t s);
 void launch_scatter_xy(int n, const uint32_t *ref_of, const float2 *src_ref, float2 *dst_int,
                        cudaStream_t s);

@@ -41,12 +41,16 @@ __device__ __forceinline__ float4 warp_bbox(float4 a) {
 // Block bounding box (minx, maxx, miny, maxy) of the thread values; the
 // last block to finish merges all block results and sets the root cell the
 // way BoundingBoxKernel does (src/RPBHKernels.cu:128-148).  Every thread of
-// the block must call it.
+// the block must call it.  A thread that saw a NaN or infinite position
+// passes bad: the next iteration then stops with kErrNonFinite instead of
+// building a tree from it.
 template <int THREADS>
-__device__ void bbox_finish(float4 a, float4 *__restrict partial, unsigned *done, DevState *st) {
+__device__ void bbox_finish(float4 a, bool bad, float4 *__restrict partial, unsigned *done,
+                            DevState *st) {
     __shared__ float4 s_w[THREADS / kWarp];
     __shared__ bool s_last;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (__any_sync(kFull, bad) && lane == 0) atomicOr(&st->err, kErrNonFinite);
     a = warp_bbox(a);
     if (lane == 0) s_w[wid] = a;
     __syncthreads();
@@ -84,11 +88,13 @@ __global__ void __launch_bounds__(kBBoxThreads) k_bbox(int n, const float2 *__re
                                                        float4 *__restrict partial,
                                                        DevState *st, IterCounters *ctr) {
     float4 a = make_float4(FLT_MAX, -FLT_MAX, FLT_MAX, -FLT_MAX);
+    bool bad = false;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float2 p = pos[i];
         a = bbox_merge(a, make_float4(p.x, p.x, p.y, p.y));
+        bad |= !(isfinite(p.x) && isfinite(p.y));
     }
-    bbox_finish<kBBoxThreads>(a, partial, &ctr->bbox_done, st);
+    bbox_finish<kBBoxThreads>(a, bad, partial, &ctr->bbox_done, st);
 }
 
 // ------------------------------------------------------------------- keys --
@@ -134,8 +140,15 @@ __global__ void __launch_bounds__(1024) k_keys(int n, int tile, const float2 *__
 // The tail adds gravity + attraction, forms the swing and traction sums
 // (SpeedKernel, src/RPFA2Kernels.cu:111-202) and, in the last block to
 // finish, updates the adaptive speed (:204-219).
+//
+// QUAD adds, for every accepted cell, the quadrupole term of its far field,
+// conj(a2 / w^3) = conj(a2) u^3 with w = z - Z, u = w / |w|^2 and the softened
+// |w|^2 = d^2 + eps; a2 is the cell's complex second moment (k_quad_up).  No
+// reference counterpart: it is the option fa2_set_approximation selects.
+template <bool QUAD>
 __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
-    int n, const float4 *__restrict nodes, const uint32_t *__restrict body_node,
+    int n, const float4 *__restrict nodes, const float2 *__restrict quad,
+    const uint32_t *__restrict body_node,
     const uint32_t *__restrict vals, const float2 *__restrict fag,
     const float2 *__restrict fprev, float2 *__restrict f, float2 *__restrict warp_partial,
     DevState *st, IterCounters *ctr, Params prm) {
@@ -181,13 +194,15 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
         uint32_t node = 1;
         // An opened cell's first child is node + 1 and always exists, so only
         // a jump to "next" can end the walk.
-        if (node < end) {
+        if (!QUAD && node < end) {
             for (;;) {
                 const float4 r = __ldg(&nodes[node]);
                 const int meta = __float_as_int(r.w);
                 const float dx = px - r.x, dy = py - r.y;
                 const float d2 = dx * dx + dy * dy + prm.epssq;
-                if (__all_sync(kFull, d2 >= s_dq[meta_level(meta)])) {
+                // written as !(d2 < dq): a NaN distance accepts, so a warp
+                // with a non-finite lane still ends its walk
+                if (__all_sync(kFull, !(d2 < s_dq[meta_level(meta)]))) {
                     const float c = __fdividef(r.z, d2);
                     ax = fmaf(dx, c, ax);
                     ay = fmaf(dy, c, ay);
@@ -195,6 +210,45 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
                     if (node >= end) break;
                 } else {
                     ++node;
+                }
+            }
+        }
+        if (QUAD && node < end) {
+            float4 r = __ldg(&nodes[node]);
+            for (;;) {
+                const int meta = __float_as_int(r.w);
+                const int lvl = meta_level(meta);
+                const float m = r.z;
+                const float dx = px - r.x, dy = py - r.y;
+                const float d2 = dx * dx + dy * dy + prm.epssq;
+                if (__all_sync(kFull, !(d2 < s_dq[lvl]))) {
+                    const uint32_t next = meta_next(meta);
+                    // the loads of the next node (and of this cell's second
+                    // moment) go out before this node's sums, so the warp
+                    // does not wait on them one after the other
+                    float2 q = make_float2(0.0f, 0.0f);
+                    if (lvl != kBodyLevel) q = __ldg(&quad[node]);
+                    if (next < end) r = __ldg(&nodes[next]);
+                    const float inv = __fdividef(1.0f, d2);
+                    const float c = m * inv;
+                    ax = fmaf(dx, c, ax);
+                    ay = fmaf(dy, c, ay);
+                    if (lvl != kBodyLevel) {
+                        // conj(a2) u^3 with u = 1 / conj(w) = w / |w|^2: |u| <= 1 / sqrt(eps)
+                        // and |a2 u^3| is below the monopole term's size, so nothing
+                        // overflows however far apart the bodies are
+                        const float ux = dx * inv, uy = dy * inv;
+                        const float xx = ux * ux, yy = uy * uy;
+                        const float ur = ux * fmaf(-3.0f, yy, xx);
+                        const float ui = uy * fmaf(-3.0f, xx, yy);
+                        ax = fmaf(q.x, ur, fmaf(-q.y, ui, ax));
+                        ay = fmaf(-q.x, ui, fmaf(-q.y, ur, ay));
+                    }
+                    node = next;
+                    if (node >= end) break;
+                } else {
+                    ++node;
+                    r = __ldg(&nodes[node]);
                 }
             }
         }
@@ -298,7 +352,7 @@ __global__ void __launch_bounds__(kTravThreads) k_count_interactions(
             const float dx = px - r.x, dy = py - r.y;
             const float d2 = dx * dx + dy * dy + prm.epssq;
             ++steps;
-            if (__all_sync(kFull, d2 >= s_dq[meta_level(meta)])) {
+            if (__all_sync(kFull, !(d2 < s_dq[meta_level(meta)]))) {
                 ++acc;
                 node = meta_next(meta);
             } else {
@@ -318,6 +372,48 @@ __global__ void __launch_bounds__(kTravThreads) k_count_interactions(
 // DisplacementKernel (src/RPFA2Kernels.cu:223-251), fused with the bounding
 // box of the new positions, which the next iteration's tree needs
 // (BoundingBoxKernel, src/RPBHKernels.cu:70-157).
+// ------------------------------------------------------------ exact f64 --
+
+// The exact all-pairs repulsion of a few sampled bodies in double precision,
+// the yardstick for the tree's approximation error: one block per sampled
+// body i (an internal id), out[s] = k_r m_i sum_{j != i} m_j d / (d^2 + eps),
+// d = p_i - p_j.  Each thread sums a fixed stride of j and the block reduces
+// in a fixed order, so the result does not depend on timing.
+constexpr int kExactThreads = 256;
+
+__global__ void __launch_bounds__(kExactThreads) k_exact_f64(int n, const float2 *__restrict pos,
+                                                             const float *__restrict mass,
+                                                             const uint32_t *__restrict ids,
+                                                             double2 *__restrict out, Params prm) {
+    __shared__ double s_x[kExactThreads], s_y[kExactThreads];
+    const uint32_t i = ids[blockIdx.x];
+    double ax = 0.0, ay = 0.0;
+    if (i < (uint32_t)n) {
+        const double px = pos[i].x, py = pos[i].y;
+        for (int j = threadIdx.x; j < n; j += kExactThreads) {
+            if ((uint32_t)j == i) continue;
+            const double dx = px - pos[j].x, dy = py - pos[j].y;
+            const double c = (double)mass[j] / (dx * dx + dy * dy + (double)prm.epssq);
+            ax += dx * c;
+            ay += dy * c;
+        }
+    }
+    s_x[threadIdx.x] = ax;
+    s_y[threadIdx.x] = ay;
+    __syncthreads();
+    for (int o = kExactThreads / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            s_x[threadIdx.x] += s_x[threadIdx.x + o];
+            s_y[threadIdx.x] += s_y[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double kmi = i < (uint32_t)n ? (double)prm.k_r * mass[i] : 0.0;
+        out[blockIdx.x] = make_double2(kmi * s_x[0], kmi * s_y[0]);
+    }
+}
+
 __global__ void __launch_bounds__(kDispThreads) k_displace(int n, float2 *__restrict pos,
                                                            const float2 *__restrict f,
                                                            float2 *__restrict fprev,
@@ -326,6 +422,7 @@ __global__ void __launch_bounds__(kDispThreads) k_displace(int n, float2 *__rest
     if (st->err || st->poison) return;
     const float global_speed = st->global_speed;
     float4 a = make_float4(FLT_MAX, -FLT_MAX, FLT_MAX, -FLT_MAX);
+    bool bad = false;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float2 fi = f[i], fp = fprev[i];
         const float factor = displacement_factor(fi, fp, global_speed);
@@ -335,8 +432,9 @@ __global__ void __launch_bounds__(kDispThreads) k_displace(int n, float2 *__rest
         pos[i] = p;
         fprev[i] = fi;
         a = bbox_merge(a, make_float4(p.x, p.x, p.y, p.y));
+        bad |= !(isfinite(p.x) && isfinite(p.y));
     }
-    bbox_finish<kDispThreads>(a, partial, &ctr->disp_done, st);
+    bbox_finish<kDispThreads>(a, bad, partial, &ctr->disp_done, st);
     if (blockIdx.x == 0 && threadIdx.x == 0) st->iters_done += 1;
 }
 
@@ -538,8 +636,20 @@ void launch_keys(const Buffers &b, int nsm, cudaStream_t s) {
 
 
 void launch_traverse(const Buffers &b, const Params &p, int nblocks, cudaStream_t s) {
-    k_traverse<<<nblocks, kTravThreads, 0, s>>>(b.n, b.nodes, b.body_node, b.vals[0], b.fag,
-                                                b.fprev, b.f, b.warp_partial, b.st, b.ctr, p);
+    if (p.multipole >= 2)
+        k_traverse<true><<<nblocks, kTravThreads, 0, s>>>(b.n, b.nodes, b.quad, b.body_node,
+                                                          b.vals[0], b.fag, b.fprev, b.f,
+                                                          b.warp_partial, b.st, b.ctr, p);
+    else
+        k_traverse<false><<<nblocks, kTravThreads, 0, s>>>(b.n, b.nodes, b.quad, b.body_node,
+                                                           b.vals[0], b.fag, b.fprev, b.f,
+                                                           b.warp_partial, b.st, b.ctr, p);
+}
+
+void launch_exact_f64(const Buffers &b, const Params &p, const uint32_t *ids, int n_ids,
+                      double2 *out, cudaStream_t s) {
+    if (n_ids <= 0) return;
+    k_exact_f64<<<n_ids, kExactThreads, 0, s>>>(b.n, b.pos, b.mass, ids, out, p);
 }
 
 void launch_displace(const Buffers &b, int nsm, cudaStream_t s) {
@@ -578,9 +688,10 @@ void launch_sorted_ref_ids(int n, const uint32_t *ref_of, const uint32_t *vals, 
 
 int traverse_blocks_per_sm() {
     // the walk lives on L1 hits: give L1 the most of the SM's on-chip memory
-    cudaFuncSetAttribute(k_traverse, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+    cudaFuncSetAttribute(k_traverse<false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+    cudaFuncSetAttribute(k_traverse<true>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_traverse, kTravThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_traverse<false>, kTravThreads, 0);
     return nb < 1 ? 1 : nb;
 }
 

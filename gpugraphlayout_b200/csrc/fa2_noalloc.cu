@@ -159,6 +159,7 @@ int run(const float *d_xy, const float *d_mass, uint32_t n, const fa2_params *pr
     kp.epssq = prm->epssq;
     kp.strong_gravity = 0;
     kp.linlog = 0;
+    kp.multipole = 1;
     kp.nsm = d.nsm;
 
     // Must start at zero on every call: the counters, histograms, per-tile
@@ -173,7 +174,7 @@ int run(const float *d_xy, const float *d_mass, uint32_t n, const fa2_params *pr
     launch_bbox(b, d.nsm * 2, s);
     launch_keys(b, d.nsm, s);
     launch_sort(b, s);
-    launch_tree_count(b, s);
+    launch_tree_count(b, false, s);
     launch_emit(b, d.nsm, s);
     launch_traverse(b, kp, d.trav_blocks, s);
     cudaError_t e = cudaGetLastError();
@@ -184,7 +185,7 @@ int run(const float *d_xy, const float *d_mass, uint32_t n, const fa2_params *pr
     e = cudaMemcpyAsync(flags, &b.st->poison, sizeof(flags), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return status_of(e);
-    if (flags[1] & kErrMass) return FA2_ERR_INVALID_ARGUMENT;
+    if (flags[1] & (kErrMass | kErrNonFinite)) return FA2_ERR_INVALID_ARGUMENT;
     if (flags[1]) return FA2_ERR_DEVICE_LIMIT;
     if (flags[0]) return FA2_ERR_INVALID_ARGUMENT;  // coincident bodies
     return FA2_OK;
@@ -199,7 +200,7 @@ extern "C" int fa2_repulsion_noalloc(const float *d_xy, const float *d_mass, uin
     using namespace fa2;
     if (!prm) return FA2_ERR_INVALID_ARGUMENT;
     if (n > kMaxBodies) return FA2_ERR_TOO_LARGE;
-    if (!prm->use_barneshut) return FA2_ERR_UNSUPPORTED;
+    if (!prm->use_barneshut || prm->multipole > 1) return FA2_ERR_UNSUPPORTED;
     if (!(prm->theta > 0.0f)) return FA2_ERR_INVALID_ARGUMENT;
     if (n == 0) return FA2_OK;
     if (!d_xy || !d_mass || !d_force || ((uintptr_t)d_xy & 7) || ((uintptr_t)d_force & 7) ||

@@ -68,6 +68,10 @@ typedef struct {
                                  src/RPForceAtlas2.hpp:44; honoured by the reference's
                                  CPU path only, src/RPCPUForceAtlas2.cpp:59-67).  0 by
                                  default, as in the reference (src/RPForceAtlas2.cpp:52) */
+    int32_t multipole;        /* 1 (default): cells act as point masses at their centre
+                                 of mass, as in the reference (src/RPBHKernels.cu:661-668);
+                                 2: each accepted cell also adds its quadrupole term (no
+                                 reference counterpart; see fa2_set_approximation) */
 } fa2_params;
 
 /* Fills the reference defaults (weak gravity, gravity 1, scale 1). */
@@ -115,7 +119,12 @@ typedef struct {
     uint32_t tree_cells;
     int32_t max_level;          /* deepest cell level (root 0) */
     int32_t perturb_rounds;     /* .99 re-insertion rounds in the last step */
-    int32_t device_error;       /* bit set of device-side limit hits, 0 = none */
+    int32_t device_error;       /* bit set of device-side limit hits, 0 = none:
+                                   2 tree-count wait limit, 4 more than 1024 bodies on
+                                   one 64-bit key, 8 tree larger than its buffer,
+                                   16 a NaN or infinite position, 32 malformed tree
+                                   seen by the quadrupole sums.  Stepping stops while
+                                   one is set; fa2_set_positions clears them */
     uint64_t nnz_padded;        /* CSR entries incl. padding */
     float global_speed;         /* adaptive speed after the last step */
     float speed_efficiency;
@@ -152,6 +161,28 @@ int fa2_set_force_params(fa2_ctx *ctx, float scale, float gravity);
  * path, which ignores ForceAtlas2::use_linlog. */
 int fa2_set_linlog(fa2_ctx *ctx, int32_t enable);
 
+/* Far-field accuracy between steps, no reference counterpart (its theta is
+ * fixed at 1, src/RPForceAtlas2.cpp:45).  theta > 0 is the Barnes-Hut opening
+ * parameter (the acceptance test d^2 + eps >= (2 r)^2 / theta^2 + eps);
+ * multipole 1 uses each accepted cell as a point mass, as the reference does;
+ * multipole 2 adds the cell's quadrupole term conj(a2 / w^3), a2 = sum m (z - Z)^2
+ * over the cell's bodies about its centre of mass Z, w = p_i - Z with the
+ * softened |w|^2 = d^2 + eps.  The quadrupole at a larger theta reaches the
+ * monopole's error at theta = 1 with fewer node visits.  FA2_ERR_INVALID_ARGUMENT
+ * for theta <= 0 or multipole outside 1..2. */
+int fa2_set_approximation(fa2_ctx *ctx, float theta, int32_t multipole);
+
+/* Exact all-pairs repulsion of sampled nodes, in double precision on the GPU,
+ * at the current positions: out[2 s], out[2 s + 1] = k_r m_i sum_{j != i} m_j d /
+ * (d^2 + eps) for i = samples[s] (reference ids), d = p_i - p_j.  The yardstick
+ * for the tree's approximation error; no reference counterpart. */
+int fa2_exact_repulsion(fa2_ctx *ctx, int32_t n_samples, const uint32_t *samples, double *out);
+
+/* The last CUDA error a call of this thread met that returned FA2_ERR_CUDA or
+ * FA2_ERR_OUT_OF_MEMORY: its name, text and the source line that saw it; ""
+ * if none.  The string stays valid until this thread's next failing call. */
+const char *fa2_last_cuda_error(void);
+
 /* Measurement hook, no reference counterpart.  enable = 1 (the default) runs
  * the attraction on a second stream beside the tree build, the two sharing
  * the GPU; enable = 0 runs it alone before the tree build, so that the
@@ -175,6 +206,7 @@ typedef struct fa2_batch fa2_batch;
 
 /* num_graphs graphs, each as fa2_create takes one (ids local to the graph);
  * the parameters apply to every graph.  Positions start at zero. */
+/* params->multipole must be 1 (FA2_ERR_UNSUPPORTED otherwise). */
 fa2_batch *fa2_batch_create(uint32_t num_graphs, const fa2_graph_desc *graphs,
                             const fa2_params *params, int *status);
 void fa2_batch_destroy(fa2_batch *batch);
@@ -229,15 +261,16 @@ int fa2_batch_get_speed(fa2_batch *batch, float *global_speed, float *speed_effi
  *    any stream capture.
  *  - The work is enqueued on `stream` (a cudaStream_t; NULL is the default
  *    stream) and the call waits for that stream before it returns, then
- *    reports: coincident bodies, or a mass that is not a whole number in
- *    [0, 2^24) -> FA2_ERR_INVALID_ARGUMENT (fa2_step moves coincident bodies
+ *    reports: coincident bodies, a NaN or infinite position, or a mass that
+ *    is not a whole number in [0, 2^24) -> FA2_ERR_INVALID_ARGUMENT (fa2_step moves coincident bodies
  *    apart, and its masses are degree + 1; this call does neither), a
  *    device-side bound -> FA2_ERR_DEVICE_LIMIT.
  *  - There is one scratch array per device: calls that overlap on the same
  *    device (several host threads, or several streams) race on it and give
  *    wrong forces.  Serialise them.
  *  - d_xy and d_force 8-byte aligned, d_mass 4-byte aligned; d_force must not
- *    overlap d_xy or d_mass. */
+ *    overlap d_xy or d_mass.
+ *  - prm->multipole must be 1 (FA2_ERR_UNSUPPORTED otherwise). */
 int fa2_repulsion_noalloc(const float *d_xy, const float *d_mass, uint32_t n,
                           const fa2_params *prm, void *stream, float *d_force);
 

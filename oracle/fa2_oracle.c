@@ -535,10 +535,12 @@ void orc_tree_cells(const orc_tree *t, int32_t *level, float *mass, float *cx,
 
 #define ORC_MAXDEPTH 32 /* RPBHFA2LaunchParameters.cuh:62 */
 
-int32_t orc_tree_repulsion(const orc_tree *t, const float *xy, const float *mass,
-                           float k_r, float itolsq, float epssq, int32_t group,
-                           const int32_t *sortd, float *fx, float *fy,
-                           int64_t *n_visits) {
+/* The walk of ForceCalculationKernel (restated below); with a2r/a2i set, each
+ * accepted cell also adds its quadrupole term (orc_tree_repulsion_quad). */
+static int32_t tree_walk(const orc_tree *t, const float *xy, const float *mass, float k_r,
+                         float itolsq, float epssq, int32_t group, const int32_t *sortd,
+                         const double *a2r, const double *a2i, float *fx, float *fy,
+                         int64_t *n_visits) {
     const int32_t NB = t->n;
     if (n_visits) *n_visits = 0;
     if (t->maxdepth > ORC_MAXDEPTH) return 1; /* RPBHKernels.cu:595 */
@@ -607,6 +609,15 @@ int32_t orc_tree_repulsion(const orc_tree *t, const float *xy, const float *mass
                         const float d2 = dx * dx + dy * dy + epssq;
                         ax[l] += k_r * dx * mass[b] * nm / d2;
                         ay[l] += k_r * dy * mass[b] * nm / d2;
+                        if (a2r && n >= NB) {
+                            /* conj(a2 / w^3) = conj(a2 conj(w)^3) / |w|^6, |w|^2 = d2 */
+                            const double qr = a2r[n - NB], qi = a2i[n - NB];
+                            const double ur = (double)dx * ((double)dx * dx - 3.0 * dy * dy);
+                            const double ui = (double)dy * ((double)dy * dy - 3.0 * dx * dx);
+                            const double inv = 1.0 / ((double)d2 * d2 * d2);
+                            ax[l] += (float)(k_r * mass[b] * (qr * ur - qi * ui) * inv);
+                            ay[l] += (float)(-k_r * mass[b] * (qr * ui + qi * ur) * inv);
+                        }
                     }
                 } else {
                     stack_pd[depth] = pd;
@@ -628,6 +639,64 @@ int32_t orc_tree_repulsion(const orc_tree *t, const float *xy, const float *mass
     free(ay);
     if (n_visits) *n_visits = visits;
     return 0;
+}
+
+int32_t orc_tree_repulsion(const orc_tree *t, const float *xy, const float *mass,
+                           float k_r, float itolsq, float epssq, int32_t group,
+                           const int32_t *sortd, float *fx, float *fy,
+                           int64_t *n_visits) {
+    return tree_walk(t, xy, mass, k_r, itolsq, epssq, group, sortd, NULL, NULL, fx, fy,
+                     n_visits);
+}
+
+/* Quadrupole extension, no reference counterpart: the complex second moment
+ * a2 = sum m (z - Z)^2 of every cell about its centre of mass, bottom-up over
+ * the children with the parallel-axis rule. */
+static void cell_quadrupoles(const orc_tree *t, const float *xy, const float *mass, int32_t c,
+                             double *a2r, double *a2i) {
+    const int32_t NB = t->n;
+    double sr = 0.0, si = 0.0;
+    for (int q = 0; q < 4; ++q) {
+        const int32_t ch = t->child[4 * c + q];
+        if (ch < 0) continue;
+        double mx, my, m, cr = 0.0, ci = 0.0;
+        if (ch < NB) {
+            mx = xy[2 * ch];
+            my = xy[2 * ch + 1];
+            m = mass[ch];
+        } else {
+            cell_quadrupoles(t, xy, mass, ch - NB, a2r, a2i);
+            mx = t->cx[ch - NB];
+            my = t->cy[ch - NB];
+            m = t->mass[ch - NB];
+            cr = a2r[ch - NB];
+            ci = a2i[ch - NB];
+        }
+        const double dx = mx - t->cx[c], dy = my - t->cy[c];
+        sr += cr + m * (dx * dx - dy * dy);
+        si += ci + m * (2.0 * dx * dy);
+    }
+    a2r[c] = sr;
+    a2i[c] = si;
+}
+
+int32_t orc_tree_repulsion_quad(const orc_tree *t, const float *xy, const float *mass,
+                                float k_r, float itolsq, float epssq, int32_t group,
+                                const int32_t *sortd, float *fx, float *fy, int64_t *n_visits) {
+    if (t->maxdepth > ORC_MAXDEPTH) return 1;
+    double *a2r = (double *)calloc((size_t)t->ncells + 1, sizeof(double));
+    double *a2i = (double *)calloc((size_t)t->ncells + 1, sizeof(double));
+    if (!a2r || !a2i) {
+        free(a2r);
+        free(a2i);
+        return -1;
+    }
+    cell_quadrupoles(t, xy, mass, 0, a2r, a2i);
+    int32_t r = tree_walk(t, xy, mass, k_r, itolsq, epssq, group, sortd, a2r, a2i, fx, fy,
+                          n_visits);
+    free(a2r);
+    free(a2i);
+    return r;
 }
 
 typedef struct {

@@ -130,6 +130,12 @@ int32_t orc_tree_repulsion(const orc_tree *t, const float *xy, const float *mass
                            float k_r, float itolsq, float epssq, int32_t group,
                            const int32_t *sortd, float *fx, float *fy,
                            int64_t *n_visits);
+/* orc_tree_repulsion plus each accepted cell's quadrupole term conj(a2 / w^3)
+ * (a2: the cell's complex second moment about its centre of mass; w: the
+ * body's offset from it, |w|^2 softened).  No reference counterpart. */
+int32_t orc_tree_repulsion_quad(const orc_tree *t, const float *xy, const float *mass,
+                                float k_r, float itolsq, float epssq, int32_t group,
+                                const int32_t *sortd, float *fx, float *fy, int64_t *n_visits);
 
 /* Exact pairwise repulsion in double precision for the listed nodes:
  * F_i = sum_{j != i} k_r m_i m_j (p_i - p_j) / (|p_i - p_j|^2 + eps),

@@ -58,10 +58,12 @@ def lib():
         L.orc_tree_summarize.argtypes = [C.c_void_p, _f32p, _f32p]
         L.orc_tree_sort.argtypes = [C.c_void_p, _i32p]
         L.orc_tree_cells.argtypes = [C.c_void_p, _i32p, _f32p, _f32p, _f32p, _i32p]
+        walk_args = [C.c_void_p, _f32p, _f32p, C.c_float, C.c_float, C.c_float, C.c_int32,
+                     _i32p, _f32p, _f32p, C.POINTER(C.c_int64)]
         L.orc_tree_repulsion.restype = C.c_int32
-        L.orc_tree_repulsion.argtypes = [C.c_void_p, _f32p, _f32p, C.c_float, C.c_float,
-                                         C.c_float, C.c_int32, _i32p, _f32p, _f32p,
-                                         C.POINTER(C.c_int64)]
+        L.orc_tree_repulsion.argtypes = walk_args
+        L.orc_tree_repulsion_quad.restype = C.c_int32
+        L.orc_tree_repulsion_quad.argtypes = walk_args
         L.orc_exact_repulsion_f64.argtypes = [C.c_int32, _f32p, _f32p, C.c_double, C.c_double,
                                               C.c_int32, _i32p, _f64p, _f64p]
         L.orc_fa2_step.restype = C.c_int32
@@ -173,12 +175,13 @@ class Tree:
         return dict(level=level, mass=mass, cx=cx, cy=cy, count=count)
 
     def repulsion(self, k_r: float, itolsq: float = 1.0, epssq: float = 0.05 * 0.05,
-                  group: int = 32):
+                  group: int = 32, multipole: int = 1):
         fx = np.zeros(self.n, np.float32)
         fy = np.zeros(self.n, np.float32)
         visits = C.c_int64(0)
-        ovf = lib().orc_tree_repulsion(self._t, self.xy, self.mass, k_r, itolsq, np.float32(epssq),
-                                       group, self.sort(), fx, fy, C.byref(visits))
+        walk = lib().orc_tree_repulsion_quad if multipole >= 2 else lib().orc_tree_repulsion
+        ovf = walk(self._t, self.xy, self.mass, k_r, itolsq, np.float32(epssq),
+                   group, self.sort(), fx, fy, C.byref(visits))
         return np.stack([fx, fy], 1), bool(ovf), visits.value
 
 

@@ -97,3 +97,21 @@ def test_noalloc_reports_inputs_it_does_not_handle():
     assert _noalloc(torch.from_numpy(xy).cuda(), frac, out, prm) == 1
     assert _noalloc(torch.from_numpy(xy).cuda(), mass, out, prm) == 0
     assert bool(torch.isfinite(out).all())
+
+
+def test_noalloc_refuses_non_finite_positions():
+    """A NaN or infinite position is flagged by the bounding-box pass and
+    refused with FA2_ERR_INVALID_ARGUMENT before a tree is built."""
+    import torch
+    from oracle import oracle as O
+    n = 700
+    mass = torch.ones(n, dtype=torch.float32, device="cuda")
+    out = torch.zeros((n, 2), dtype=torch.float32, device="cuda")
+    prm = _params(1.0)
+    for bad in (np.nan, np.inf):
+        xy = O.random_positions(n, 100, 100, 3)
+        xy[100, 1] = bad
+        assert _noalloc(torch.from_numpy(xy).cuda(), mass, out, prm) == 1
+    xy = O.random_positions(n, 100, 100, 3)
+    assert _noalloc(torch.from_numpy(xy).cuda(), mass, out, prm) == 0
+    assert bool(torch.isfinite(out).all())
