@@ -141,6 +141,22 @@ class Engine:
               "fa2_exact_repulsion")
         return out
 
+    def set_accuracy_guard(self, every: int, n_samples: int = 1024) -> None:
+        """Every `every` steps, check the approximation against the FP64 sum
+        on n_samples bodies and fall back to the reference walk (theta 1,
+        monopole) when that is more accurate; 0 turns the guard off."""
+        check(lib().fa2_set_accuracy_guard(self._ctx, int(every), int(n_samples)),
+              "fa2_set_accuracy_guard")
+
+    def accuracy_guard(self) -> dict:
+        """The last check's relative RMSEs and the counts of checks and fallbacks."""
+        ec, ep = C.c_double(0.0), C.c_double(0.0)
+        ck, fb = C.c_int32(0), C.c_int32(0)
+        check(lib().fa2_get_accuracy_guard(self._ctx, C.byref(ec), C.byref(ep), C.byref(ck),
+                                           C.byref(fb)), "fa2_get_accuracy_guard")
+        return {"err_current": ec.value, "err_plain": ep.value, "checks": ck.value,
+                "fallbacks": fb.value}
+
     def set_overlap(self, enable: bool) -> None:
         """Attraction beside the tree build (default) or alone before it."""
         check(lib().fa2_set_overlap(self._ctx, 1 if enable else 0), "fa2_set_overlap")

@@ -19,6 +19,7 @@ EXPORTS = (
     "fa2_get_stats", "fa2_get_forces", "fa2_get_sort_order", "fa2_set_speed_state",
     "fa2_get_speed_state", "fa2_set_force_params", "fa2_set_linlog", "fa2_set_overlap",
     "fa2_set_approximation", "fa2_exact_repulsion", "fa2_last_cuda_error",
+    "fa2_set_accuracy_guard", "fa2_get_accuracy_guard",
     "fa2_batch_create", "fa2_batch_destroy", "fa2_batch_set_positions", "fa2_batch_get_positions",
     "fa2_batch_step", "fa2_batch_step_timed", "fa2_batch_get_forces", "fa2_batch_get_sort_order",
     "fa2_batch_get_speed", "fa2_render_rgb", "fa2_png_encode", "fa2_write_png", "fa2_repulsion_noalloc", "fa2_ugraph_load",
@@ -107,6 +108,8 @@ def lib():
     L.fa2_set_linlog.argtypes = [vp, C.c_int32]
     L.fa2_set_approximation.argtypes = [vp, C.c_float, C.c_int32]
     L.fa2_exact_repulsion.argtypes = [vp, C.c_int32, vp, vp]
+    L.fa2_set_accuracy_guard.argtypes = [vp, C.c_int32, C.c_int32]
+    L.fa2_get_accuracy_guard.argtypes = [vp, vp, vp, vp, vp]
     L.fa2_last_cuda_error.restype = C.c_char_p
     L.fa2_last_cuda_error.argtypes = []
     L.fa2_render_rgb.argtypes = [C.c_uint32, C.c_uint64, vp, vp, vp, C.c_int32, C.c_int32,

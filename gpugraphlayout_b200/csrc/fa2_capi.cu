@@ -13,6 +13,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <numeric>
 #include <vector>
 
@@ -66,6 +67,12 @@ struct fa2_ctx {
     std::vector<cudaEvent_t> event_pool;       // per (iteration, slot, start/end)
     int last_perturb_rounds = 0;
     bool overlap = true;  // attraction on stream B beside the tree build
+    // accuracy guard (fa2_set_accuracy_guard)
+    int guard_every = 0, guard_samples = 0, guard_cap = 0, guard_left = 0;
+    int guard_checks = 0, guard_fallbacks = 0;
+    double guard_err_cur = 0.0, guard_err_plain = 0.0;
+    double2 *guard_exact = nullptr;
+    float2 *guard_plain = nullptr, *guard_cur = nullptr;
 };
 
 namespace {
@@ -293,6 +300,51 @@ int capture(fa2_ctx *c, bool timed, cudaGraphExec_t *out) {
     return cuda_status(e);
 }
 
+// The guard checks only an approximation other than the reference's.
+bool guard_active(const fa2_ctx *c) {
+    return c->guard_every > 0 && (c->kp.multipole >= 2 || c->kp.itolsq != 1.0f);
+}
+
+// One check of the accuracy guard on the last iteration's tree: relative RMSE
+// of the applied repulsion and of the plain walk against the FP64 sum over
+// the sampled bodies; the plain walk takes over when it is the more accurate.
+int guard_check(fa2_ctx *c) {
+    const int ns = c->guard_samples;
+    launch_guard(c->b, c->kp, ns, c->guard_exact, c->guard_plain, c->guard_cur, c->sA);
+    CK(cudaGetLastError());
+    std::vector<double2> ex((size_t)ns);
+    std::vector<float2> pl((size_t)ns), cu((size_t)ns);
+    CK(cudaMemcpyAsync(ex.data(), c->guard_exact, ex.size() * sizeof(double2),
+                       cudaMemcpyDeviceToHost, c->sA));
+    CK(cudaMemcpyAsync(pl.data(), c->guard_plain, pl.size() * sizeof(float2),
+                       cudaMemcpyDeviceToHost, c->sA));
+    CK(cudaMemcpyAsync(cu.data(), c->guard_cur, cu.size() * sizeof(float2),
+                       cudaMemcpyDeviceToHost, c->sA));
+    CK(cudaStreamSynchronize(c->sA));
+    double e_cur = 0.0, e_plain = 0.0, norm = 0.0;
+    for (int s = 0; s < ns; ++s) {
+        const double ax = cu[s].x - ex[s].x, ay = cu[s].y - ex[s].y;
+        const double bx = pl[s].x - ex[s].x, by = pl[s].y - ex[s].y;
+        e_cur += ax * ax + ay * ay;
+        e_plain += bx * bx + by * by;
+        norm += ex[s].x * ex[s].x + ex[s].y * ex[s].y;
+    }
+    if (!(norm > 0.0)) return FA2_OK;  // nothing to compare against
+    c->guard_err_cur = std::sqrt(e_cur / norm);
+    c->guard_err_plain = std::sqrt(e_plain / norm);
+    c->guard_checks += 1;
+    if (c->guard_err_cur > c->guard_err_plain) {
+        // back to the reference's walk: theta 1, cells as point masses
+        c->kp.itolsq = 1.0f;
+        c->kp.multipole = 1;
+        c->prm.theta = 1.0f;
+        c->prm.multipole = 1;
+        c->guard_fallbacks += 1;
+        drop_graphs(c);
+    }
+    return FA2_OK;
+}
+
 int read_state(fa2_ctx *c, DevState *st) {
     CK(cudaMemcpyAsync(st, c->b.st, sizeof(DevState), cudaMemcpyDeviceToHost, c->sA));
     CK(cudaStreamSynchronize(c->sA));
@@ -320,18 +372,21 @@ int run_steps(fa2_ctx *c, int32_t n_iters, bool timed, std::vector<double> *kern
               std::vector<int> *kernel_cnt) {
     if (n_iters <= 0 || c->n == 0) return FA2_OK;
     cudaGraphExec_t *exec = timed ? &c->exec_timed : &c->exec;
-    if (!*exec) {
-        int s = capture(c, timed, exec);
-        if (s) return s;
-    }
     DevState st;
     int s = read_state(c, &st);
     if (s) return s;
     int done = 0;
     c->last_perturb_rounds = 0;
     while (done < n_iters) {
+        // (re)captured here: a guard fallback drops the graphs
+        if (!*exec) {
+            s = capture(c, timed, exec);
+            if (s) return s;
+        }
+        const bool guard = guard_active(c);
         const int before = st.iters_done;
-        const int chunk = n_iters - done;
+        int chunk = n_iters - done;
+        if (guard) chunk = std::min(chunk, std::max(c->guard_left, 1));
         if (timed) {
             size_t need = (size_t)chunk * kNumSlots * 2;
             while (c->event_pool.size() < need) {
@@ -370,6 +425,15 @@ int run_steps(fa2_ctx *c, int32_t n_iters, bool timed, std::vector<double> *kern
             s = resolve_poison(c, &st);
             if (s) return s;
             done += 1;  // the replayed iteration completed
+            completed += 1;
+        }
+        if (guard) {
+            c->guard_left -= completed;
+            if (c->guard_left <= 0) {
+                c->guard_left = c->guard_every;
+                s = guard_check(c);
+                if (s) return s;
+            }
         }
     }
     return FA2_OK;
@@ -780,6 +844,40 @@ int fa2_exact_repulsion(fa2_ctx *c, int32_t n_samples, const uint32_t *samples, 
 }
 
 const char *fa2_last_cuda_error(void) { return g_last_cuda_error; }
+
+int fa2_set_accuracy_guard(fa2_ctx *c, int32_t every, int32_t n_samples) {
+    if (!c || every < 0 || (every > 0 && n_samples <= 0)) return FA2_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(c->device));
+    c->guard_checks = c->guard_fallbacks = 0;
+    c->guard_err_cur = c->guard_err_plain = 0.0;
+    if (every == 0 || c->n == 0) {
+        c->guard_every = 0;
+        return FA2_OK;
+    }
+    const int ns = (int)std::min<uint32_t>((uint32_t)n_samples, c->n);
+    if (ns > c->guard_cap) {
+        int s = FA2_OK;
+        if ((s = dalloc(c, &c->guard_exact, (size_t)ns)) ||
+            (s = dalloc(c, &c->guard_plain, (size_t)ns)) ||
+            (s = dalloc(c, &c->guard_cur, (size_t)ns)))
+            return s;
+        c->guard_cap = ns;
+    }
+    c->guard_every = every;
+    c->guard_samples = ns;
+    c->guard_left = every;
+    return FA2_OK;
+}
+
+int fa2_get_accuracy_guard(fa2_ctx *c, double *err_current, double *err_plain, int32_t *checks,
+                           int32_t *fallbacks) {
+    if (!c) return FA2_ERR_INVALID_ARGUMENT;
+    if (err_current) *err_current = c->guard_err_cur;
+    if (err_plain) *err_plain = c->guard_err_plain;
+    if (checks) *checks = c->guard_checks;
+    if (fallbacks) *fallbacks = c->guard_fallbacks;
+    return FA2_OK;
+}
 
 int fa2_set_overlap(fa2_ctx *c, int32_t enable) {
     if (!c) return FA2_ERR_INVALID_ARGUMENT;

@@ -190,6 +190,8 @@ void launch_displace(const Buffers &b, int nsm, cudaStream_t s);
 void launch_count_interactions(const Buffers &b, const Params &p, int nblocks, cudaStream_t s);
 void launch_exact_f64(const Buffers &b, const Params &p, const uint32_t *ids, int n_ids,
                       double2 *out, cudaStream_t s);
+void launch_guard(const Buffers &b, const Params &p, int ns, double2 *exact, float2 *plain,
+                  float2 *cur, cudaStream_t s);
 void launch_attract(const Buffers &b, const Params &p, const AttractPlan &plan, cudaStream_t s);
 void launch_scatter_xy(int n, const uint32_t *ref_of, const float2 *src_ref, float2 *dst_int,
                        cudaStream_t s);

@@ -414,6 +414,110 @@ __global__ void __launch_bounds__(kExactThreads) k_exact_f64(int n, const float2
     }
 }
 
+// ------------------------------------------------------------------ guard --
+
+// The accuracy guard's three views of the repulsion of ns sampled sorted
+// bodies (k = (2s + 1) n / 2ns), all from the last iteration's tree, whose
+// body records hold the positions that iteration used:
+//   exact  k_r m_k sum_{j != k} m_j d / (d^2 + eps) over every body, FP64;
+//   plain  the reference walk (monopole, theta = 1) of the sample's own group
+//          of 32 sorted bodies over that tree;
+//   cur    what the iteration applied: its total force less gravity and
+//          attraction.
+__device__ __forceinline__ int guard_sample(int s, int ns, int n) {
+    return (int)(((long long)(2 * s + 1) * n) / (2ll * ns));
+}
+
+__global__ void __launch_bounds__(kExactThreads) k_guard_exact(
+    int n, int ns, const float4 *__restrict nodes, const uint32_t *__restrict body_node,
+    const uint32_t *__restrict vals, const float2 *__restrict f, const float2 *__restrict fag,
+    Params prm, double2 *__restrict exact, float2 *__restrict cur) {
+    __shared__ double s_x[kExactThreads], s_y[kExactThreads];
+    const int k = guard_sample(blockIdx.x, ns, n);
+    const float4 me = nodes[body_node[k]];
+    const double px = me.x, py = me.y;
+    double ax = 0.0, ay = 0.0;
+    for (int j = threadIdx.x; j < n; j += kExactThreads) {
+        if (j == k) continue;
+        const float4 o = nodes[body_node[j]];
+        const double dx = px - o.x, dy = py - o.y;
+        const double c = (double)o.z / (dx * dx + dy * dy + (double)prm.epssq);
+        ax += dx * c;
+        ay += dy * c;
+    }
+    s_x[threadIdx.x] = ax;
+    s_y[threadIdx.x] = ay;
+    __syncthreads();
+    for (int o = kExactThreads / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            s_x[threadIdx.x] += s_x[threadIdx.x + o];
+            s_y[threadIdx.x] += s_y[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double kmi = (double)prm.k_r * me.z;
+        exact[blockIdx.x] = make_double2(kmi * s_x[0], kmi * s_y[0]);
+        const uint32_t i = vals[k];
+        cur[blockIdx.x] = make_float2(f[i].x - fag[i].x, f[i].y - fag[i].y);
+    }
+}
+
+// One warp per sample: the plain walk of the sample's group (the k_traverse
+// loop at theta = 1); the sample's lane keeps its sum.
+__global__ void __launch_bounds__(256) k_guard_plain(int n, int ns,
+                                                     const float4 *__restrict nodes,
+                                                     const uint32_t *__restrict body_node,
+                                                     const DevState *st, Params prm,
+                                                     float2 *__restrict plain) {
+    __shared__ float s_dq[64];
+    if (threadIdx.x == 0) {
+        // the thresholds of k_traverse for theta = 1, from the radius that
+        // iteration's walk used
+        float tmp = st->trav_radius * 2;
+        float dq = tmp * tmp * 1.0f;
+        s_dq[0] = 0.0f;
+        for (int l = 1; l <= kLevels; ++l) {
+            s_dq[l] = dq + prm.epssq;
+            dq = dq * 0.25f;
+        }
+        for (int l = kLevels + 1; l < 64; ++l) s_dq[l] = 0.0f;
+    }
+    __syncthreads();
+    const int s = blockIdx.x * (256 / kWarp) + (threadIdx.x >> 5);
+    if (s >= ns) return;
+    const int lane = threadIdx.x & 31;
+    const int ks = guard_sample(s, ns, n);
+    const int k = (ks & ~31) + lane;
+    const bool active = k < n;
+    const float4 me = nodes[body_node[active ? k : n - 1]];
+    const float px = active ? me.x : 1e30f, py = active ? me.y : 1e30f;
+    const uint32_t end = st->tree_nodes;
+    float ax = 0.0f, ay = 0.0f;
+    uint32_t node = 1;
+    if (node < end) {
+        for (;;) {
+            const float4 r = __ldg(&nodes[node]);
+            const int meta = __float_as_int(r.w);
+            const float dx = px - r.x, dy = py - r.y;
+            const float d2 = dx * dx + dy * dy + prm.epssq;
+            if (__all_sync(kFull, !(d2 < s_dq[meta_level(meta)]))) {
+                const float c = __fdividef(r.z, d2);
+                ax = fmaf(dx, c, ax);
+                ay = fmaf(dy, c, ay);
+                node = meta_next(meta);
+                if (node >= end) break;
+            } else {
+                ++node;
+            }
+        }
+    }
+    if (k == ks) {
+        const float kmi = prm.k_r * me.z;
+        plain[s] = make_float2(ax * kmi, ay * kmi);
+    }
+}
+
 __global__ void __launch_bounds__(kDispThreads) k_displace(int n, float2 *__restrict pos,
                                                            const float2 *__restrict f,
                                                            float2 *__restrict fprev,
@@ -644,6 +748,14 @@ void launch_traverse(const Buffers &b, const Params &p, int nblocks, cudaStream_
         k_traverse<false><<<nblocks, kTravThreads, 0, s>>>(b.n, b.nodes, b.quad, b.body_node,
                                                            b.vals[0], b.fag, b.fprev, b.f,
                                                            b.warp_partial, b.st, b.ctr, p);
+}
+
+void launch_guard(const Buffers &b, const Params &p, int ns, double2 *exact, float2 *plain,
+                  float2 *cur, cudaStream_t s) {
+    if (ns <= 0 || b.n <= 0) return;
+    k_guard_exact<<<ns, kExactThreads, 0, s>>>(b.n, ns, b.nodes, b.body_node, b.vals[0], b.f,
+                                               b.fag, p, exact, cur);
+    k_guard_plain<<<(ns + 7) / 8, 256, 0, s>>>(b.n, ns, b.nodes, b.body_node, b.st, p, plain);
 }
 
 void launch_exact_f64(const Buffers &b, const Params &p, const uint32_t *ids, int n_ids,

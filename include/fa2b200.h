@@ -178,6 +178,24 @@ int fa2_set_approximation(fa2_ctx *ctx, float theta, int32_t multipole);
  * for the tree's approximation error; no reference counterpart. */
 int fa2_exact_repulsion(fa2_ctx *ctx, int32_t n_samples, const uint32_t *samples, double *out);
 
+/* Accuracy guard for an approximation other than the reference's (theta != 1
+ * or multipole 2); no reference counterpart.  Every `every` iterations of
+ * fa2_step / fa2_step_timed, after that iteration, the repulsion it applied to
+ * n_samples bodies spread evenly over the sorted order is compared with the
+ * exact FP64 sum over all bodies, and so is the reference walk (monopole,
+ * theta 1) over the same tree.  If the applied repulsion has the larger
+ * relative RMSE, the context falls back to the reference walk for the
+ * iterations that follow (fa2_set_approximation selects an approximation
+ * again).  every = 0 turns the guard off.  A check costs one FP64 sum over all
+ * bodies per sample.  Resets the counts of fa2_get_accuracy_guard. */
+int fa2_set_accuracy_guard(fa2_ctx *ctx, int32_t every, int32_t n_samples);
+
+/* The last check's relative RMSE of the applied and of the reference walk's
+ * repulsion against the FP64 sum, and the numbers of checks and of fallbacks
+ * since fa2_set_accuracy_guard.  Null pointers are skipped. */
+int fa2_get_accuracy_guard(fa2_ctx *ctx, double *err_current, double *err_plain,
+                           int32_t *checks, int32_t *fallbacks);
+
 /* The last CUDA error a call of this thread met that returned FA2_ERR_CUDA or
  * FA2_ERR_OUT_OF_MEMORY: its name, text and the source line that saw it; ""
  * if none.  The string stays valid until this thread's next failing call. */

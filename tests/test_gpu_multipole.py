@@ -171,3 +171,51 @@ def test_quadrupole_replay_of_coincident_bodies_matches_oracle(ba3k):
     assert not ovf
     assert np.array_equal(e.sort_order(), t.sort().astype(np.uint32))
     assert rel_rmse(rep, ref) <= TOL
+
+
+def test_accuracy_guard_errors_match_the_oracle(ba3k):
+    """With as many samples as bodies the guard compares every body: its two
+    errors are the relative RMSEs of the step's repulsion and of the
+    reference walk against the oracle's FP64 sum.  The quadrupole walk at
+    theta 1.5 is the more accurate, so it is kept."""
+    from gpugraphlayout_b200 import Engine
+    from oracle import oracle as O
+    g = ba3k
+    xy = O.random_positions(g.n, 2000, 2000, 14)
+    exact = O.exact_repulsion_f64(xy, g.mass, 10.0, np.arange(g.n, dtype=np.int32))
+    plain_engine = Engine(g.n, g.sources, g.targets, scale=10.0)
+    plain, _ = _rep(plain_engine, xy)
+    e = Engine(g.n, g.sources, g.targets, scale=10.0, theta=1.5, multipole=2)
+    e.set_accuracy_guard(1, g.n)
+    rep, _ = _rep(e, xy)
+    gd = e.accuracy_guard()
+    assert gd["checks"] == 1 and gd["fallbacks"] == 0
+    assert gd["err_current"] == pytest.approx(rel_rmse(rep, exact), rel=1e-9)
+    # the guard keeps the reference walk's sum itself; a step's repulsion is
+    # read back as (gravity + attraction + repulsion) - (gravity + attraction),
+    # rounded twice in float, which moves the error by about 1e-5 of itself
+    assert gd["err_plain"] == pytest.approx(rel_rmse(plain, exact), rel=1e-4)
+    assert gd["err_current"] < gd["err_plain"]
+
+
+def test_accuracy_guard_falls_back_to_the_reference_walk(ba3k):
+    """A monopole walk at theta 2.5 is less accurate than the reference's at
+    theta 1: the first check switches the context to the reference walk, whose
+    forces then equal a plain engine's bit for bit, and checks stop."""
+    from gpugraphlayout_b200 import Engine
+    from oracle import oracle as O
+    g = ba3k
+    xy = O.random_positions(g.n, 2000, 2000, 15)
+    e = Engine(g.n, g.sources, g.targets, scale=10.0)
+    e.set_approximation(2.5, 1)
+    e.set_accuracy_guard(2, 512)
+    e.set_positions(xy)
+    e.step(5)
+    gd = e.accuracy_guard()
+    assert gd["checks"] == 1 and gd["fallbacks"] == 1
+    assert gd["err_current"] > gd["err_plain"] > 0
+    after, _ = _rep(e, xy)
+    plain, _ = _rep(Engine(g.n, g.sources, g.targets, scale=10.0), xy)
+    assert np.array_equal(after, plain)
+    e.step(4)
+    assert e.accuracy_guard()["checks"] == 1
