@@ -41,6 +41,7 @@ SCALE, DRAWS = 20, 16_777_216
 K_R, K_G, STRONG = 10.0, 1.0, True
 WIDTH = 2.0e4
 KERNELS_PER_ITER = 14  # attract, keys, 8 sort passes, tree_count, emit, traverse, displace
+# (the quadrupole walk adds the moment scan and the per-cell a2 kernel)
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_attract
 # launch at this workload, from an ncu capture of
 #   ncu --set full --clock-control none -k regex:k_attract -s 4 -c 1 \
@@ -157,10 +158,11 @@ def run_reference(args, world, rank):
     }))
 
 
-def workload_config(n, m):
+def workload_config(n, m, theta=1.0, multipole=1):
+    walk = ("plain Barnes-Hut" if multipole == 1 else "Barnes-Hut with the quadrupole term")
     return {"workload": f"R-MAT scale {SCALE} ({DRAWS:,} draws, a=.57 b=.19 c=.19, seed 0), "
                         f"N={n:,} E={m:,}; positions U[-1e4,1e4]^2; strong gravity, scale 10, "
-                        f"gravity 1, theta 1; plain Barnes-Hut",
+                        f"gravity 1, theta {theta:g}; {walk}",
             "nodes": n, "edges": m, "l2": "per-iteration working set larger than L2 "
                                           "(padded CSR alone exceeds 126 MB)",
             "parallelism": "replicas (one graph per GPU)"}
@@ -258,7 +260,9 @@ def run_ours(args, world, rank, local):
     n, m = g.num_nodes(), g.num_edges()
     s, t = g.edges()
     xy0 = random_positions(n, WIDTH, WIDTH, 1234)
-    eng = Engine(n, s, t, strong_gravity=STRONG, gravity=K_G, scale=K_R, device=local)
+    eng = Engine(n, s, t, strong_gravity=STRONG, gravity=K_G, scale=K_R, device=local,
+                 theta=args.theta, multipole=args.multipole)
+    plain = args.theta == 1.0 and args.multipole == 1
     eng.set_positions(xy0)
 
     import torch
@@ -302,7 +306,9 @@ def run_ours(args, world, rank, local):
 
     if rank != 0:
         return
-    correction = correction_report(eng, n, args.steps)
+    # the correction report compares against the plain walk, so it runs only
+    # when the plain walk is the workload
+    correction = correction_report(eng, n, args.steps) if plain else None
     names = kernel_names()
     pk, pk_kind = peaks()
     hbm = float(pk["hbm_gbs"])
@@ -344,9 +350,9 @@ def run_ours(args, world, rank, local):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": ms_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "config": workload_config(n, m),
+        "data": "synthetic", "config": workload_config(n, m, args.theta, args.multipole),
         "clocks": clocks_summary(clk_path),
-        "gpu_launches": KERNELS_PER_ITER * args.steps,
+        "gpu_launches": (KERNELS_PER_ITER + (2 if args.multipole == 2 else 0)) * args.steps,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * n,
                 "d2h_bytes_per_step": 8 * n},
         "roofline": roofline,
@@ -484,6 +490,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--theta", type=float, default=1.0,
+                    help="Barnes-Hut opening parameter of the rmat20 workload (reference: 1)")
+    ap.add_argument("--multipole", type=int, default=1, choices=[1, 2],
+                    help="1: cells as point masses (reference); 2: with the quadrupole term")
     ap.add_argument("--workload", default="rmat20", choices=["rmat20", "batched"],
                     help="rmat20: the R-MAT scale-20 graph (default); batched: 4096 SBM graphs")
     args = ap.parse_args()
