@@ -230,16 +230,21 @@ def correction_report(eng, n, steps):
     if best is not None:
         # the corrected walk as a user runs it: with the accuracy guard
         # checking it against the FP64 sum every GUARD_EVERY steps
+        steps_g = 4 * GUARD_EVERY
+        eng.set_approximation(1.0, 1)
+        eng.set_positions(P)
+        ms_plain, _ = eng.step_timed(steps_g)
         eng.set_approximation(best["theta"], 2)
         eng.set_accuracy_guard(GUARD_EVERY, GUARD_SAMPLES)
         eng.set_positions(P)
-        steps_g = 4 * GUARD_EVERY
         ms, _ = eng.step_timed(steps_g)
         gd = eng.accuracy_guard()
         eng.set_accuracy_guard(0, 0)
+        # the same steps from the same positions with the plain walk
         guarded = {"theta": best["theta"], "every": GUARD_EVERY, "samples": GUARD_SAMPLES,
                    "steps": steps_g, "ms_per_step": ms / steps_g,
-                   "speedup_vs_plain": base["ms_per_step"] / (ms / steps_g), **gd}
+                   "plain_ms_per_step": ms_plain / steps_g,
+                   "speedup_vs_plain": ms_plain / ms, **gd}
     eng.set_approximation(1.0, 1)
     eng.set_positions(P)
     return {
