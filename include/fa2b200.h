@@ -122,9 +122,8 @@ typedef struct {
     int32_t device_error;       /* bit set of device-side limit hits, 0 = none:
                                    2 tree-count wait limit, 4 more than 1024 bodies on
                                    one 64-bit key, 8 tree larger than its buffer,
-                                   16 a NaN or infinite position, 32 malformed tree
-                                   seen by the quadrupole sums.  Stepping stops while
-                                   one is set; fa2_set_positions clears them */
+                                   16 a NaN or infinite position.  Stepping stops
+                                   while one is set; fa2_set_positions clears them */
     uint64_t nnz_padded;        /* CSR entries incl. padding */
     float global_speed;         /* adaptive speed after the last step */
     float speed_efficiency;
