@@ -432,6 +432,10 @@ def run_batched(args, world, rank, local):
     eng.set_positions(xy)
     torch.cuda.set_device(local)
     eng.step(max(args.warmup, 3))
+    # CTA sizes picked by measurement on this batch (the layout state is kept)
+    tuned = eng.autotune(2)
+    sizes = [graphs[i][0] for i in mine]
+    classes = (any(s <= tuned["split"] for s in sizes) + any(s > tuned["split"] for s in sizes))
     clk_path = os.path.join(tempfile.gettempdir(), f"fa2_clocks_b{rank}.csv")
     sampler = clocks_sampler(local, clk_path)
     time.sleep(0.3)
@@ -472,7 +476,9 @@ def run_batched(args, world, rank, local):
         "data": "synthetic", "config": batch_config(graphs, world),
         "graph_iters_per_s": value * len(graphs),
         "clocks": clocks_summary(clk_path),
-        "gpu_launches": args.steps,
+        # one persistent launch per size class runs all the timed iterations
+        "gpu_launches": classes,
+        "autotune": tuned,
         "e2e": {"value": e2e, "unit": "batch iters/s", "h2d_bytes_per_step": 8 * n_all // world,
                 "d2h_bytes_per_step": 8 * n_all // world},
         "roofline": {"kernel": "batch", "bound": "hbm", "achieved": achieved, "peak": hbm,

@@ -22,6 +22,7 @@ EXPORTS = (
     "fa2_set_accuracy_guard", "fa2_get_accuracy_guard",
     "fa2_batch_create", "fa2_batch_destroy", "fa2_batch_set_positions", "fa2_batch_get_positions",
     "fa2_batch_step", "fa2_batch_step_timed", "fa2_batch_get_forces", "fa2_batch_get_sort_order",
+    "fa2_batch_configure", "fa2_batch_get_config", "fa2_batch_autotune",
     "fa2_batch_get_speed", "fa2_render_rgb", "fa2_png_encode", "fa2_write_png", "fa2_repulsion_noalloc", "fa2_ugraph_load",
     "fa2_ugraph_from_pairs", "fa2_ugraph_free", "fa2_ugraph_num_nodes",
     "fa2_ugraph_num_edges", "fa2_ugraph_node_map_r", "fa2_ugraph_degrees",
@@ -125,6 +126,9 @@ def lib():
     L.fa2_batch_step_timed.argtypes = [vp, C.c_int32, f32p]
     L.fa2_batch_get_forces.argtypes = [vp, vp, vp]
     L.fa2_batch_get_sort_order.argtypes = [vp, vp]
+    L.fa2_batch_configure.argtypes = [vp, C.c_uint32, C.c_int32]
+    L.fa2_batch_get_config.argtypes = [vp, vp, vp]
+    L.fa2_batch_autotune.argtypes = [vp, C.c_int32, vp, vp, vp]
     L.fa2_batch_get_speed.argtypes = [vp, vp, vp]
     L.fa2_repulsion_noalloc.argtypes = [vp, vp, C.c_uint32, C.POINTER(Params), vp, vp]
     L.fa2_ugraph_load.restype = vp

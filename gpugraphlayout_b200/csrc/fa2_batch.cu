@@ -29,10 +29,10 @@ namespace fa2 {
 
 namespace {
 
-constexpr int kBThreads = 1024;
-constexpr int kBWarps = kBThreads / kWarp;
+// Threads per CTA (T) is a template parameter: 256, 512 or 1024.  Every
+// result is the same for each (stable sort, exact integer sums, per-warp
+// walks, fixed-order speed sums); only the speed differs.
 constexpr int kBRounds = 4;                       // keys per thread in a sort chunk
-constexpr int kBChunk = kBThreads * kBRounds;     // keys per sort chunk
 constexpr uint32_t kBatchMaxNodes = FA2_BATCH_MAX_NODES;  // nodes per graph
 constexpr int kErrPoisonRounds = 1 << 9;          // coincident bodies kept reappearing
 
@@ -95,16 +95,17 @@ __device__ __forceinline__ NodeSums shfl_up_sums(const NodeSums &v, int o) {
 }
 
 // Shared memory of the batch kernel (static part; sort histograms included).
+template <int T>
 struct BatchSmem {
-    uint32_t whist[kBWarps][256];
+    uint32_t whist[T / kWarp][256];
     uint32_t qsum[4][256];
     uint32_t base[256];
     uint32_t coff[256];
-    NodeSums wsum[kBWarps];
+    NodeSums wsum[T / kWarp];
     NodeSums carry;
-    float4 wbox[kBWarps];
+    float4 wbox[T / kWarp];
     float dq[64];
-    float2 wred[kBWarps];
+    float2 wred[T / kWarp];
     float rx, ry, radius;
     uint32_t total_nodes;
     int ticket;
@@ -115,7 +116,8 @@ struct BatchSmem {
 
 // Block-wide exclusive scan of NodeSums; *total receives the block's sum.
 // Every thread of the block calls it.
-__device__ NodeSums block_scan(NodeSums v, BatchSmem &S, NodeSums *total) {
+template <int T>
+__device__ NodeSums block_scan(NodeSums v, BatchSmem<T> &S, NodeSums *total) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     NodeSums inc = v;
 #pragma unroll
@@ -126,7 +128,7 @@ __device__ NodeSums block_scan(NodeSums v, BatchSmem &S, NodeSums *total) {
     if (lane == 31) S.wsum[wid] = inc;
     __syncthreads();
     if (wid == 0) {
-        NodeSums w = S.wsum[lane], wi = w;
+        NodeSums w = lane < T / kWarp ? S.wsum[lane] : NodeSums{0, 0, 0, 0}, wi = w;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const NodeSums t = shfl_up_sums(wi, o);
@@ -137,7 +139,7 @@ __device__ NodeSums block_scan(NodeSums v, BatchSmem &S, NodeSums *total) {
         ex.m -= w.m;
         ex.x -= w.x;
         ex.y -= w.y;
-        S.wsum[lane] = ex;
+        if (lane < T / kWarp) S.wsum[lane] = ex;
         if (lane == 31) S.carry = wi;  // block total, read below before reuse
     }
     __syncthreads();
@@ -159,11 +161,11 @@ __device__ __forceinline__ T *slot_ptr(char *slot, size_t off) {
 // --------------------------------------------------------------- phases --
 
 // Gravity + attraction of the graph's nodes (8 lanes per row), into fa.
-template <bool LINLOG>
+template <int T, bool LINLOG>
 __device__ void phase_attract(const BatchArgs &A, uint32_t base, uint32_t n, float2 *fa) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int sub = lane >> 3, l8 = lane & 7;
-    for (uint32_t r0 = (uint32_t)wid * 4; r0 < n; r0 += kBWarps * 4) {
+    for (uint32_t r0 = (uint32_t)wid * 4; r0 < n; r0 += (T / kWarp) * 4) {
         const uint32_t row = r0 + (uint32_t)sub;
         const bool valid = row < n;
         float ax = 0.0f, ay = 0.0f;
@@ -192,11 +194,12 @@ __device__ void phase_attract(const BatchArgs &A, uint32_t base, uint32_t n, flo
 
 // Bounding box and root cell of the graph (BoundingBoxKernel,
 // src/RPBHKernels.cu:70-157), into S.rx, S.ry, S.radius.
-__device__ void phase_bbox(const BatchArgs &A, uint32_t base, uint32_t n, BatchSmem &S) {
+template <int T>
+__device__ void phase_bbox(const BatchArgs &A, uint32_t base, uint32_t n, BatchSmem<T> &S) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     float4 a = make_float4(FLT_MAX, -FLT_MAX, FLT_MAX, -FLT_MAX);
     bool bad = false;
-    for (uint32_t i = threadIdx.x; i < n; i += kBThreads) {
+    for (uint32_t i = threadIdx.x; i < n; i += T) {
         const float2 p = A.pos[base + i];
         a = make_float4(fminf(a.x, p.x), fmaxf(a.y, p.x), fminf(a.z, p.y), fmaxf(a.w, p.y));
         bad |= !(isfinite(p.x) && isfinite(p.y));
@@ -214,7 +217,7 @@ __device__ void phase_bbox(const BatchArgs &A, uint32_t base, uint32_t n, BatchS
     __syncthreads();
     if (threadIdx.x == 0) {
         float4 b = S.wbox[0];
-        for (int w = 1; w < kBWarps; ++w) {
+        for (int w = 1; w < T / kWarp; ++w) {
             const float4 c = S.wbox[w];
             b = make_float4(fminf(b.x, c.x), fmaxf(b.y, c.y), fminf(b.z, c.z), fmaxf(b.w, c.w));
         }
@@ -225,17 +228,20 @@ __device__ void phase_bbox(const BatchArgs &A, uint32_t base, uint32_t n, BatchS
     __syncthreads();
 }
 
-// One stable LSD pass over the graph's n keys in chunks of kBChunk: digit
+// One stable LSD pass over the graph's n keys in chunks of T x kBRounds: digit
 // histogram, bases, then per chunk a ballot ranking per warp and offsets
 // across warps.
+template <int T>
 __device__ void sort_pass(int pass, uint32_t n, const uint64_t *kin, const uint32_t *vin,
-                          uint64_t *kout, uint32_t *vout, BatchSmem &S) {
+                          uint64_t *kout, uint32_t *vout, BatchSmem<T> &S) {
+    constexpr int kW = T / kWarp, kChunk = T * kBRounds;
+    constexpr int kQ = T / 256;  // threads per digit in the cross-warp offsets
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int shift = 8 * pass;
     const unsigned lt = (1u << lane) - 1u;
     if (threadIdx.x < 256) S.base[threadIdx.x] = 0;
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < n; i += kBThreads)
+    for (uint32_t i = threadIdx.x; i < n; i += T)
         atomicAdd(&S.base[(uint32_t)(kin[i] >> shift) & 255u], 1u);
     __syncthreads();
     if (threadIdx.x < 256) {  // exclusive scan of the 256 counts (warps 0..7)
@@ -257,8 +263,8 @@ __device__ void sort_pass(int pass, uint32_t n, const uint64_t *kin, const uint3
         S.base[threadIdx.x] = S.qsum[0][threadIdx.x] + b;
     }
     __syncthreads();
-    for (uint32_t c0 = 0; c0 < n; c0 += kBChunk) {
-        const uint32_t w0 = c0 + (uint32_t)wid * (kBChunk / kBWarps);
+    for (uint32_t c0 = 0; c0 < n; c0 += kChunk) {
+        const uint32_t w0 = c0 + (uint32_t)wid * (kChunk / kW);
         uint64_t k[kBRounds];
         uint32_t v[kBRounds], rank[kBRounds];
 #pragma unroll
@@ -267,7 +273,7 @@ __device__ void sort_pass(int pass, uint32_t n, const uint64_t *kin, const uint3
             k[r] = idx < n ? kin[idx] : 0ull;
             v[r] = idx < n ? vin[idx] : 0u;
         }
-        for (int j = threadIdx.x; j < kBWarps * 256; j += kBThreads) (&S.whist[0][0])[j] = 0;
+        for (int j = threadIdx.x; j < kW * 256; j += T) (&S.whist[0][0])[j] = 0;
         __syncthreads();
 #pragma unroll
         for (int r = 0; r < kBRounds; ++r) {
@@ -289,7 +295,8 @@ __device__ void sort_pass(int pass, uint32_t n, const uint64_t *kin, const uint3
             __syncwarp();
         }
         __syncthreads();
-        // per digit: exclusive offsets across the 32 warps, 4 threads per digit
+        // per digit: exclusive offsets across the warps, kQ threads per digit
+        // taking 8 warps each
         const int dg = threadIdx.x & 255, qt = threadIdx.x >> 8;
         {
             uint32_t q = 0;
@@ -301,7 +308,7 @@ __device__ void sort_pass(int pass, uint32_t n, const uint64_t *kin, const uint3
         {
             uint32_t run = 0, tot = 0;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (int q = 0; q < kQ; ++q) {
                 const uint32_t c = S.qsum[q][dg];
                 if (q < qt) run += c;
                 tot += c;
@@ -333,12 +340,13 @@ __device__ void sort_pass(int pass, uint32_t n, const uint64_t *kin, const uint3
 // Keys from the positions, the 8 sort passes (ending in keys0/vals0) and the
 // ordering of equal-key runs; returns with S.poison set if exactly
 // coincident bodies were found (perturb = 0) or after scaling them (1).
+template <int T>
 __device__ void phase_keys_sort(const BatchArgs &A, uint32_t base, uint32_t n, char *slot,
-                                BatchSmem &S, int perturb) {
+                                BatchSmem<T> &S, int perturb) {
     uint64_t *k0 = slot_ptr<uint64_t>(slot, A.L.keys0), *k1 = slot_ptr<uint64_t>(slot, A.L.keys1);
     uint32_t *v0 = slot_ptr<uint32_t>(slot, A.L.vals0), *v1 = slot_ptr<uint32_t>(slot, A.L.vals1);
     const float rx = S.rx, ry = S.ry, rr = S.radius;
-    for (uint32_t i = threadIdx.x; i < n; i += kBThreads) {
+    for (uint32_t i = threadIdx.x; i < n; i += T) {
         const float2 p = A.pos[base + i];
         k0[i] = morton_key(p.x, p.y, rx, ry, rr);
         v0[i] = i;
@@ -348,7 +356,7 @@ __device__ void phase_keys_sort(const BatchArgs &A, uint32_t base, uint32_t n, c
         sort_pass(pass, n, k0, v0, k1, v1, S);
         sort_pass(pass + 1, n, k1, v1, k0, v0, S);
     }
-    for (uint32_t k = threadIdx.x; k + 1 < n; k += kBThreads) {
+    for (uint32_t k = threadIdx.x; k + 1 < n; k += T) {
         if (k0[k + 1] != k0[k] || (k > 0 && k0[k - 1] == k0[k])) continue;
         fix_run((int)k, (int)n, k0, v0, A.pos + base, nullptr, rx, ry, rr, &S.err, &S.poison,
                 perturb);
@@ -357,8 +365,9 @@ __device__ void phase_keys_sort(const BatchArgs &A, uint32_t base, uint32_t n, c
 }
 
 // Tree count: L[k], preorder indices, owners and the exact prefix sums.
+template <int T>
 __device__ void phase_count(const BatchArgs &A, uint32_t base, uint32_t n, char *slot,
-                            BatchSmem &S) {
+                            BatchSmem<T> &S) {
     const uint64_t *keys = slot_ptr<uint64_t>(slot, A.L.keys0);
     const uint32_t *vals = slot_ptr<uint32_t>(slot, A.L.vals0);
     int8_t *lcp = slot_ptr<int8_t>(slot, A.L.lcp);
@@ -370,7 +379,7 @@ __device__ void phase_count(const BatchArgs &A, uint32_t base, uint32_t n, char 
     const float rx = S.rx, ry = S.ry;
     const uint32_t cap = A.L.cap;
     NodeSums carry{0, 0, 0, 0};
-    for (uint32_t c0 = 0; c0 < n; c0 += kBThreads) {
+    for (uint32_t c0 = 0; c0 < n; c0 += T) {
         const uint32_t k = c0 + threadIdx.x;
         NodeSums v{0, 0, 0, 0};
         long long im = 0, qx = 0, qy = 0;
@@ -415,8 +424,9 @@ __device__ void phase_count(const BatchArgs &A, uint32_t base, uint32_t n, char 
 }
 
 // Every node of the tree once (k_emit's rule, one thread per node).
+template <int T>
 __device__ void phase_emit(const BatchArgs &A, uint32_t base, uint32_t n, char *slot,
-                           BatchSmem &S) {
+                           BatchSmem<T> &S) {
     const uint64_t *keys = slot_ptr<uint64_t>(slot, A.L.keys0);
     const uint32_t *vals = slot_ptr<uint32_t>(slot, A.L.vals0);
     const int8_t *lcp = slot_ptr<int8_t>(slot, A.L.lcp);
@@ -429,7 +439,7 @@ __device__ void phase_emit(const BatchArgs &A, uint32_t base, uint32_t n, char *
     const double inv_scale = S.radius > 0.0f ? (double)S.radius / kFixedScale : 1.0;
     const double rx = S.rx, ry = S.ry;
     const uint32_t total = S.total_nodes;
-    for (uint32_t g = threadIdx.x; g < total; g += kBThreads) {
+    for (uint32_t g = threadIdx.x; g < total; g += T) {
         const uint32_t w = owner[g];
         const int k = (int)(w >> 6), q = (int)(w & 63u);
         if (q == 63) {
@@ -453,8 +463,9 @@ __device__ void phase_emit(const BatchArgs &A, uint32_t base, uint32_t n, char *
 
 // The warp-vote walk of k_traverse over this graph's tree, the total force,
 // swing and traction per group of 32 bodies, then (thread 0) the speed rule.
+template <int T>
 __device__ void phase_traverse(const BatchArgs &A, uint32_t base, uint32_t n, char *slot,
-                               BatchSmem &S) {
+                               BatchSmem<T> &S) {
     const float4 *nodes = slot_ptr<float4>(slot, A.L.nodes);
     const uint32_t *body_node = slot_ptr<uint32_t>(slot, A.L.body_node);
     const uint32_t *vals = slot_ptr<uint32_t>(slot, A.L.vals0);
@@ -554,11 +565,12 @@ __device__ void phase_traverse(const BatchArgs &A, uint32_t base, uint32_t n, ch
 }
 
 // Displacement (DisplacementKernel, src/RPFA2Kernels.cu:223-251).
+template <int T>
 __device__ void phase_displace(const BatchArgs &A, uint32_t base, uint32_t n, char *slot,
-                               BatchSmem &S) {
+                               BatchSmem<T> &S) {
     const float2 *f = slot_ptr<float2>(slot, A.L.f);
     const float gs = S.gs;
-    for (uint32_t i = threadIdx.x; i < n; i += kBThreads) {
+    for (uint32_t i = threadIdx.x; i < n; i += T) {
         const float2 fi = f[i], fp = A.fprev[base + i];
         const float factor = displacement_factor(fi, fp, gs);
         float2 p = A.pos[base + i];
@@ -570,9 +582,9 @@ __device__ void phase_displace(const BatchArgs &A, uint32_t base, uint32_t n, ch
     __syncthreads();
 }
 
-template <bool LINLOG>
-__global__ void __launch_bounds__(kBThreads, 1) k_batch(BatchArgs A) {
-    __shared__ BatchSmem S;
+template <int T, bool LINLOG>
+__global__ void __launch_bounds__(T, 1024 / T) k_batch(BatchArgs A) {
+    __shared__ BatchSmem<T> S;
     char *slot = A.slots + (size_t)blockIdx.x * A.L.bytes;
     float2 *fa = slot_ptr<float2>(slot, A.L.fa);
     for (;;) {
@@ -594,7 +606,7 @@ __global__ void __launch_bounds__(kBThreads, 1) k_batch(BatchArgs A) {
         int rounds = 0;
         for (int it = 0; it < A.iters && n > 0; ++it) {
             if (S.err) break;
-            phase_attract<LINLOG>(A, base, n, fa);
+            phase_attract<T, LINLOG>(A, base, n, fa);
             phase_bbox(A, base, n, S);
             if (S.err) break;
             phase_keys_sort(A, base, n, slot, S, 0);
@@ -622,7 +634,7 @@ __global__ void __launch_bounds__(kBThreads, 1) k_batch(BatchArgs A) {
         }
         // the body order of the last iteration, graph-local ids
         const uint32_t *vals = slot_ptr<uint32_t>(slot, A.L.vals0);
-        for (uint32_t k = threadIdx.x; k < n; k += kBThreads) A.sortd[base + k] = vals[k];
+        for (uint32_t k = threadIdx.x; k < n; k += T) A.sortd[base + k] = vals[k];
         if (threadIdx.x == 0) {
             BatchSpeed sp;
             sp.global_speed = S.gs;
@@ -671,6 +683,16 @@ SlotLayout make_layout(uint32_t nmax) {
 
 using namespace fa2;
 
+// One size class of the batch: its graphs (a slice of the queue order), the
+// CTA size that runs them, and its grid with one scratch slot per CTA.
+struct BatchClass {
+    BatchArgs args{};
+    int threads = 0;        // 0: the class is empty
+    int grid = 0;
+    void *slots = nullptr;  // grid x args.L.bytes
+    size_t slot_cap = 0;    // bytes allocated at slots
+};
+
 struct fa2_batch {
     int device = 0;
     int nsm = 0;
@@ -678,13 +700,20 @@ struct fa2_batch {
     uint64_t total_nodes = 0;
     fa2_params prm{};
     Params kp{};
-    std::vector<uint32_t> base;  // node base per graph
-    std::vector<uint32_t> count; // nodes per graph
+    std::vector<uint32_t> base;   // node base per graph
+    std::vector<uint32_t> count;  // nodes per graph
+    std::vector<uint32_t> order;  // graphs, largest first
     std::vector<void *> allocs;
-    BatchArgs args{};
-    int grid = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    BatchArgs args{};             // the fields every class shares
+    uint32_t *d_order = nullptr;  // the queue order of the current classes
+    unsigned *queues = nullptr;   // one ticket counter per class
+    // Graphs of at most `split` nodes (class 0) run on CTAs of `small_threads`
+    // threads, the others (class 1) on 1024-thread CTAs.
+    uint32_t split = 0;
+    int small_threads = 256;
+    BatchClass cls[2];
+    cudaStream_t stream = nullptr, side = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evFork = nullptr, evJoin = nullptr;
 };
 
 namespace {
@@ -713,19 +742,107 @@ int balloc(fa2_batch *b, T **p, size_t count) {
 void bfree(fa2_batch *b) {
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->evFork) cudaEventDestroy(b->evFork);
+    if (b->evJoin) cudaEventDestroy(b->evJoin);
     if (b->stream) cudaStreamDestroy(b->stream);
+    if (b->side) cudaStreamDestroy(b->side);
+    for (BatchClass &c : b->cls)
+        if (c.slots) cudaFree(c.slots);
     for (void *p : b->allocs) cudaFree(p);
     b->allocs.clear();
 }
 
+template <int T>
+int occupancy() {
+    int a = 0, c = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_batch<T, false>, T, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_batch<T, true>, T, 0);
+    return std::max(1, std::min(a, c));
+}
+
+int occupancy_for(int threads) {
+    switch (threads) {
+        case 256: return occupancy<256>();
+        case 512: return occupancy<512>();
+        default: return occupancy<1024>();
+    }
+}
+
+// Splits the graphs into the two classes, uploads the queue order (class 1
+// then class 0, each largest first) and sizes each class's grid and slots.
+int configure(fa2_batch *b, uint32_t split, int small_threads) {
+    std::vector<uint32_t> big, small;
+    for (uint32_t g : b->order) (b->count[g] <= split ? small : big).push_back(g);
+    std::vector<uint32_t> q(big);
+    q.insert(q.end(), small.begin(), small.end());
+    if (!q.empty())
+        BCK(cudaMemcpyAsync(b->d_order, q.data(), q.size() * 4, cudaMemcpyHostToDevice,
+                            b->stream));
+    const std::vector<uint32_t> *members[2] = {&small, &big};
+    const uint32_t first[2] = {(uint32_t)big.size(), 0u};
+    const int threads[2] = {small_threads, 1024};
+    for (int k = 0; k < 2; ++k) {
+        BatchClass &c = b->cls[k];
+        const std::vector<uint32_t> &m = *members[k];
+        c.args = b->args;
+        c.threads = m.empty() ? 0 : threads[k];
+        if (!c.threads) continue;
+        uint32_t nmax = 1;
+        for (uint32_t g : m) nmax = std::max(nmax, b->count[g]);
+        c.args.order = b->d_order + first[k];
+        c.args.num_graphs = (int)m.size();
+        c.args.queue = b->queues + k;
+        c.args.L = make_layout(nmax);
+        c.grid = std::max(1, std::min<int>(b->nsm * occupancy_for(c.threads), (int)m.size()));
+        const size_t need = c.args.L.bytes * (size_t)c.grid;
+        if (need > c.slot_cap) {
+            if (c.slots) cudaFree(c.slots);
+            c.slots = nullptr;
+            c.slot_cap = 0;
+            BCK(cudaMalloc(&c.slots, need));
+            c.slot_cap = need;
+        }
+        c.args.slots = static_cast<char *>(c.slots);
+    }
+    b->split = split;
+    b->small_threads = small_threads;
+    BCK(cudaStreamSynchronize(b->stream));
+    return FA2_OK;
+}
+
+template <bool LINLOG>
+void launch_class(const BatchClass &c, cudaStream_t s) {
+    switch (c.threads) {
+        case 256: k_batch<256, LINLOG><<<c.grid, 256, 0, s>>>(c.args); break;
+        case 512: k_batch<512, LINLOG><<<c.grid, 512, 0, s>>>(c.args); break;
+        default: k_batch<1024, LINLOG><<<c.grid, 1024, 0, s>>>(c.args); break;
+    }
+}
+
+// Both classes at once: class 1 (large graphs) on the batch stream, class 0
+// on a second stream, joined back into the batch stream.
 int launch_batch(fa2_batch *b, int iters) {
-    b->args.iters = iters;
-    BCK(cudaMemsetAsync(b->args.queue, 0, sizeof(unsigned), b->stream));
-    if (b->kp.linlog)
-        k_batch<true><<<b->grid, kBThreads, 0, b->stream>>>(b->args);
-    else
-        k_batch<false><<<b->grid, kBThreads, 0, b->stream>>>(b->args);
-    BCK(cudaGetLastError());
+    BCK(cudaMemsetAsync(b->queues, 0, 2 * sizeof(unsigned), b->stream));
+    const bool both = b->cls[0].threads && b->cls[1].threads;
+    if (both) {
+        BCK(cudaEventRecord(b->evFork, b->stream));
+        BCK(cudaStreamWaitEvent(b->side, b->evFork, 0));
+    }
+    for (int k = 1; k >= 0; --k) {
+        BatchClass &c = b->cls[k];
+        if (!c.threads) continue;
+        c.args.iters = iters;
+        cudaStream_t s = (both && k == 0) ? b->side : b->stream;
+        if (b->kp.linlog)
+            launch_class<true>(c, s);
+        else
+            launch_class<false>(c, s);
+        BCK(cudaGetLastError());
+    }
+    if (both) {
+        BCK(cudaEventRecord(b->evJoin, b->side));
+        BCK(cudaStreamWaitEvent(b->stream, b->evJoin, 0));
+    }
     return FA2_OK;
 }
 
@@ -844,28 +961,23 @@ fa2_batch *fa2_batch_create(uint32_t num_graphs, const fa2_graph_desc *graphs,
     std::vector<float> mass(N);
     for (size_t i = 0; i < N; ++i) mass[i] = (float)deg[i] + 1.0f;
     // largest first (nodes + edges), so the long graphs start early
-    std::vector<uint32_t> order(num_graphs);
+    std::vector<uint32_t> &order = b->order;
+    order.resize(num_graphs);
     std::iota(order.begin(), order.end(), 0u);
     std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t c) {
         return (uint64_t)graphs[a].num_nodes + graphs[a].num_edges >
                (uint64_t)graphs[c].num_nodes + graphs[c].num_edges;
     });
+    (void)nmax;
 
     BatchArgs &A = b->args;
-    A.L = make_layout(nmax);
-    int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<false>, kBThreads, 0);
-    int occ2 = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k_batch<true>, kBThreads, 0);
-    occ = std::max(1, std::min(occ, occ2));
-    b->grid = std::max(1, std::min<int>(b->nsm * occ, (int)std::max<uint32_t>(num_graphs, 1)));
 
     BatchGraph *d_graphs = nullptr;
-    uint32_t *d_order = nullptr, *d_off = nullptr, *d_col = nullptr;
+    uint32_t *d_off = nullptr, *d_col = nullptr;
     float *d_mass = nullptr;
     int s = FA2_OK;
     if ((s = balloc(b, &d_graphs, std::max<size_t>(num_graphs, 1))) ||
-        (s = balloc(b, &d_order, std::max<size_t>(num_graphs, 1))) ||
+        (s = balloc(b, &b->d_order, std::max<size_t>(num_graphs, 1))) ||
         (s = balloc(b, &A.pos, std::max<size_t>(N, 1))) ||
         (s = balloc(b, &A.fprev, std::max<size_t>(N, 1))) ||
         (s = balloc(b, &d_mass, std::max<size_t>(N, 1))) || (s = balloc(b, &d_off, N + 1)) ||
@@ -873,12 +985,9 @@ fa2_batch *fa2_batch_create(uint32_t num_graphs, const fa2_graph_desc *graphs,
         (s = balloc(b, &A.speed, std::max<size_t>(num_graphs, 1))) ||
         (s = balloc(b, &A.f_tot, std::max<size_t>(N, 1))) ||
         (s = balloc(b, &A.f_ag, std::max<size_t>(N, 1))) ||
-        (s = balloc(b, &A.sortd, std::max<size_t>(N, 1))) || (s = balloc(b, &A.queue, 1)) ||
-        (s = balloc(b, &A.slots, A.L.bytes * (size_t)b->grid)))
+        (s = balloc(b, &A.sortd, std::max<size_t>(N, 1))) || (s = balloc(b, &b->queues, 2)))
         return fail(s);
     A.graphs = d_graphs;
-    A.order = d_order;
-    A.num_graphs = (int)num_graphs;
     A.mass = d_mass;
     A.off = d_off;
     A.col = d_col;
@@ -886,13 +995,15 @@ fa2_batch *fa2_batch_create(uint32_t num_graphs, const fa2_graph_desc *graphs,
     A.jitter_tolerance = prm->jitter_tolerance;
     A.k_s_max = prm->k_s_max;
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess)
+        cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->evFork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->evJoin, cudaEventDisableTiming) != cudaSuccess)
         return fail(FA2_ERR_CUDA);
     std::vector<BatchSpeed> sp(num_graphs);
     for (auto &x : sp) x = BatchSpeed{1.0f, 1.0f, 0, 0};  // src/RPFA2Kernels.cu:30-31
     cudaStream_t st = b->stream;
     if (cudaMemcpyAsync(d_graphs, hg.data(), hg.size() * sizeof(BatchGraph), cudaMemcpyHostToDevice, st) ||
-        cudaMemcpyAsync(d_order, order.data(), order.size() * 4, cudaMemcpyHostToDevice, st) ||
         cudaMemcpyAsync(d_mass, mass.data(), N * 4, cudaMemcpyHostToDevice, st) ||
         cudaMemcpyAsync(d_off, off.data(), (N + 1) * 4, cudaMemcpyHostToDevice, st) ||
         cudaMemcpyAsync(d_col, col.data(), col.size() * 4, cudaMemcpyHostToDevice, st) ||
@@ -901,6 +1012,8 @@ fa2_batch *fa2_batch_create(uint32_t num_graphs, const fa2_graph_desc *graphs,
         cudaMemsetAsync(A.f_tot, 0, N * 8, st) || cudaMemsetAsync(A.f_ag, 0, N * 8, st) ||
         cudaMemsetAsync(A.sortd, 0, N * 4, st) || cudaStreamSynchronize(st))
         return fail(FA2_ERR_CUDA);
+    // every graph on 1024-thread CTAs until fa2_batch_configure / _autotune
+    if ((s = configure(b, 0, 256))) return fail(s);
     *status = FA2_OK;
     return b;
 }
@@ -959,6 +1072,107 @@ int fa2_batch_step_timed(fa2_batch *b, int32_t n_iters, float *ms) {
     BCK(cudaEventSynchronize(b->ev1));
     BCK(cudaEventElapsedTime(ms, b->ev0, b->ev1));
     return check_errors(b);
+}
+
+int fa2_batch_configure(fa2_batch *b, uint32_t split, int32_t small_threads) {
+    if (!b || (small_threads != 256 && small_threads != 512 && small_threads != 1024))
+        return FA2_ERR_INVALID_ARGUMENT;
+    BCK(cudaSetDevice(b->device));
+    BCK(cudaStreamSynchronize(b->stream));
+    return configure(b, split, small_threads);
+}
+
+int fa2_batch_get_config(fa2_batch *b, uint32_t *split, int32_t *small_threads) {
+    if (!b) return FA2_ERR_INVALID_ARGUMENT;
+    if (split) *split = b->split;
+    if (small_threads) *small_threads = b->small_threads;
+    return FA2_OK;
+}
+
+int fa2_batch_autotune(fa2_batch *b, int32_t iters, uint32_t *split_out, int32_t *threads_out,
+                       float *ms_out) {
+    if (!b || iters <= 0) return FA2_ERR_INVALID_ARGUMENT;
+    BCK(cudaSetDevice(b->device));
+    if (!b->num_graphs || !b->total_nodes) return FA2_OK;
+    BCK(cudaStreamSynchronize(b->stream));
+    // The trial steps change the layout state; it is saved here and put back
+    // before each trial and at the end.
+    const size_t N = b->total_nodes, G = b->num_graphs;
+    BatchArgs &A = b->args;
+    struct Saved {
+        void *dst, *src;
+        size_t bytes;
+    };
+    const Saved parts[] = {{nullptr, A.pos, N * 8},
+                           {nullptr, A.fprev, N * 8},
+                           {nullptr, A.speed, G * sizeof(BatchSpeed)},
+                           {nullptr, A.f_tot, N * 8},
+                           {nullptr, A.f_ag, N * 8},
+                           {nullptr, A.sortd, N * 4}};
+    std::vector<Saved> saved(std::begin(parts), std::end(parts));
+    int s = FA2_OK;
+    for (Saved &x : saved) {
+        if (cudaMalloc(&x.dst, x.bytes) != cudaSuccess) {
+            x.dst = nullptr;
+            s = FA2_ERR_OUT_OF_MEMORY;
+            break;
+        }
+        if (cudaMemcpyAsync(x.dst, x.src, x.bytes, cudaMemcpyDeviceToDevice, b->stream) !=
+            cudaSuccess) {
+            s = FA2_ERR_CUDA;
+            break;
+        }
+    }
+    auto restore = [&]() {
+        for (Saved &x : saved)
+            if (x.dst && cudaMemcpyAsync(x.src, x.dst, x.bytes, cudaMemcpyDeviceToDevice,
+                                         b->stream) != cudaSuccess)
+                return FA2_ERR_CUDA;
+        return cudaStreamSynchronize(b->stream) == cudaSuccess ? FA2_OK : FA2_ERR_CUDA;
+    };
+    // candidates: every graph on 1024-thread CTAs, or the graphs up to a
+    // size on smaller CTAs beside the rest
+    uint32_t nmax = 1;
+    for (uint32_t c : b->count) nmax = std::max(nmax, c);
+    std::vector<std::pair<uint32_t, int>> cand{{0u, 256}};
+    for (uint32_t sp : {256u, 1024u, 4096u, nmax})
+        for (int t : {256, 512})
+            if (sp <= nmax &&
+                std::find(cand.begin(), cand.end(), std::make_pair(sp, t)) == cand.end())
+                cand.emplace_back(sp, t);
+    const uint32_t split0 = b->split;
+    const int threads0 = b->small_threads;
+    float best_ms = 0.0f;
+    std::pair<uint32_t, int> best{split0, threads0};
+    bool found = false;
+    for (const auto &c : cand) {
+        if (s) break;
+        if ((s = configure(b, c.first, c.second))) break;
+        if ((s = restore())) break;
+        float ms = 0.0f;
+        if (cudaEventRecord(b->ev0, b->stream) != cudaSuccess) s = FA2_ERR_CUDA;
+        if (!s) s = launch_batch(b, iters);
+        if (!s && (cudaEventRecord(b->ev1, b->stream) != cudaSuccess ||
+                   cudaEventSynchronize(b->ev1) != cudaSuccess ||
+                   cudaEventElapsedTime(&ms, b->ev0, b->ev1) != cudaSuccess))
+            s = FA2_ERR_CUDA;
+        if (!s && (!found || ms < best_ms)) {
+            best_ms = ms;
+            best = c;
+            found = true;
+        }
+    }
+    const int s2 = configure(b, found ? best.first : split0, found ? best.second : threads0);
+    const int s3 = restore();
+    for (Saved &x : saved)
+        if (x.dst) cudaFree(x.dst);
+    if (s) return s;
+    if (s2) return s2;
+    if (s3) return s3;
+    if (split_out) *split_out = b->split;
+    if (threads_out) *threads_out = b->small_threads;
+    if (ms_out) *ms_out = best_ms / (float)iters;
+    return FA2_OK;
 }
 
 int fa2_batch_get_forces(fa2_batch *b, float *f_total, float *f_attr_grav) {

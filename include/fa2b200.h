@@ -244,6 +244,21 @@ int fa2_batch_step_timed(fa2_batch *batch, int32_t n_iters, float *ms);
  * per node, same order as the positions); the body order of each graph's
  * quadtree (graph-local ids, the reference's sortd); the adaptive speed and
  * speed efficiency per graph. */
+/* CTA sizes: graphs of at most `split` nodes run on CTAs of small_threads
+ * threads (256, 512 or 1024) beside the others on 1024-thread CTAs, each
+ * class from its own queue; split 0 (the default) runs every graph on 1024
+ * threads.  Results do not depend on the choice, only the speed does. */
+int fa2_batch_configure(fa2_batch *batch, uint32_t split, int32_t small_threads);
+int fa2_batch_get_config(fa2_batch *batch, uint32_t *split, int32_t *small_threads);
+
+/* Picks the configuration by measurement: times `iters` iterations of every
+ * candidate split (256, 1024, 4096 nodes, all graphs, or none) and small CTA
+ * size (256, 512) on this batch, keeps the fastest, and puts the layout state
+ * (positions, speeds, and the forces and orders of the last iteration) back
+ * as it was.  Returns the choice and its ms per iteration. */
+int fa2_batch_autotune(fa2_batch *batch, int32_t iters, uint32_t *split,
+                       int32_t *small_threads, float *ms_per_iter);
+
 int fa2_batch_get_forces(fa2_batch *batch, float *f_total, float *f_attr_grav);
 int fa2_batch_get_sort_order(fa2_batch *batch, uint32_t *order);
 int fa2_batch_get_speed(fa2_batch *batch, float *global_speed, float *speed_efficiency);

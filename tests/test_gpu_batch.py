@@ -125,3 +125,47 @@ def test_batch_results_do_not_depend_on_the_other_graphs():
     solo.set_positions(xys[1])
     solo.step(5)
     assert np.array_equal(b.part(b.get_positions(), 1), solo.get_positions())
+
+
+def test_results_do_not_depend_on_the_cta_sizes():
+    """Graphs up to a size on 256- or 512-thread CTAs beside the rest on
+    1024-thread CTAs: stable sort, exact integer sums, per-warp walks and
+    fixed-order speed sums make every graph's steps bit-identical."""
+    graphs = _graphs([50, 3000, 120, 777, 1999, 64, 5000, 300, 40, 2500])
+    xy = np.concatenate(_positions(graphs))
+    runs = []
+    for split, threads in ((0, 256), (1000, 256), (3000, 512), (10000, 256)):
+        b = _batch(graphs, scale=2.0)
+        b.configure(split, threads)
+        assert b.config() == {"split": split, "small_threads": threads}
+        b.set_positions(xy)
+        b.step(3)
+        runs.append((b.get_positions(), b.sort_order(), b.speeds()))
+    for pos, order, (gs, se) in runs[1:]:
+        assert np.array_equal(pos, runs[0][0])
+        assert np.array_equal(order, runs[0][1])
+        assert np.array_equal(gs, runs[0][2][0]) and np.array_equal(se, runs[0][2][1])
+
+
+def test_autotune_leaves_the_layout_state_as_it_was():
+    from gpugraphlayout_b200 import Fa2Error
+    graphs = _graphs([50, 3000, 120, 777, 1999, 64, 5000, 300])
+    xy = np.concatenate(_positions(graphs))
+    b = _batch(graphs, scale=2.0)
+    b.set_positions(xy)
+    b.step(2)
+    before = (b.get_positions(), b.sort_order(), b.speeds())
+    cfg = b.autotune(2)
+    assert cfg["small_threads"] in (256, 512) and cfg["ms_per_iter"] > 0
+    assert b.config() == {"split": cfg["split"], "small_threads": cfg["small_threads"]}
+    after = (b.get_positions(), b.sort_order(), b.speeds())
+    assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
+    assert np.array_equal(before[2][0], after[2][0])
+    # and the steps that follow are those of an untuned batch
+    ref = _batch(graphs, scale=2.0)
+    ref.set_positions(xy)
+    ref.step(4)
+    b.step(2)
+    assert np.array_equal(b.get_positions(), ref.get_positions())
+    with pytest.raises(Fa2Error):
+        b.configure(100, 128)
