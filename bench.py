@@ -40,6 +40,11 @@ UNIT = "iters/s"
 SCALE, DRAWS = 20, 16_777_216
 K_R, K_G, STRONG = 10.0, 1.0, True
 WIDTH = 2.0e4
+# R-MAT workloads: scale, edge draws, side of the square of the initial
+# positions.  rmat23 is the large run: 8.4M ids, 134M draws, U[-1e5,1e5]^2.
+RMAT = {"rmat20": (SCALE, DRAWS, WIDTH), "rmat23": (23, 134_217_728, 2.0e5)}
+FP64_SAMPLES = 4096
+FP64_EVERY, FP64_CHECKS = 50, 4
 KERNELS_PER_ITER = 14  # attract, keys, 8 sort passes, tree_count, emit, traverse, displace
 # (the quadrupole walk adds the moment scan and the per-cell a2 kernel)
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_attract
@@ -158,11 +163,12 @@ def run_reference(args, world, rank):
     }))
 
 
-def workload_config(n, m, theta=1.0, multipole=1):
+def workload_config(n, m, theta=1.0, multipole=1, workload="rmat20"):
     walk = ("plain Barnes-Hut" if multipole == 1 else "Barnes-Hut with the quadrupole term")
-    return {"workload": f"R-MAT scale {SCALE} ({DRAWS:,} draws, a=.57 b=.19 c=.19, seed 0), "
-                        f"N={n:,} E={m:,}; positions U[-1e4,1e4]^2; strong gravity, scale 10, "
-                        f"gravity 1, theta {theta:g}; {walk}",
+    scale, draws, width = RMAT[workload]
+    return {"workload": f"R-MAT scale {scale} ({draws:,} draws, a=.57 b=.19 c=.19, seed 0), "
+                        f"N={n:,} E={m:,}; positions U[-{width / 2:g},{width / 2:g}]^2; "
+                        f"strong gravity, scale 10, gravity 1, theta {theta:g}; {walk}",
             "nodes": n, "edges": m, "l2": "per-iteration working set larger than L2 "
                                           "(padded CSR alone exceeds 126 MB)",
             "parallelism": "replicas (one graph per GPU)"}
@@ -258,13 +264,33 @@ def correction_report(eng, n, steps):
     }
 
 
+def fp64_checks(eng, n):
+    """The large run's accuracy record: every FP64_EVERY steps, the repulsion
+    of the next step on FP64_SAMPLES sampled nodes against the exact FP64
+    all-pairs sum at the same positions (computed on the GPU)."""
+    rng = np.random.default_rng(5)
+    samples = np.sort(rng.choice(n, min(FP64_SAMPLES, n), replace=False)).astype(np.uint32)
+    out = []
+    for c in range(FP64_CHECKS):
+        eng.step(FP64_EVERY - 1)
+        exact = eng.exact_repulsion(samples)
+        eng.step(1)
+        tot, ga = eng.forces()
+        rep = (tot - ga)[samples].astype(np.float64)
+        err = float(np.sqrt(((rep - exact) ** 2).sum() / (exact ** 2).sum()))
+        out.append({"after_steps": (c + 1) * FP64_EVERY, "rel_rmse": err})
+    return {"samples": len(samples), "every": FP64_EVERY, "checks": out}
+
+
 def run_ours(args, world, rank, local):
     from gpugraphlayout_b200 import Engine, UGraph, kernel_names, random_positions, synth
-    s_raw, t_raw = synth.rmat_edges(SCALE, DRAWS, seed=0)
+    scale, draws, width = RMAT[args.workload]
+    large = args.workload != "rmat20"
+    s_raw, t_raw = synth.rmat_edges(scale, draws, seed=0)
     g = UGraph.from_pairs(s_raw, t_raw)
     n, m = g.num_nodes(), g.num_edges()
     s, t = g.edges()
-    xy0 = random_positions(n, WIDTH, WIDTH, 1234)
+    xy0 = random_positions(n, width, width, 1234)
     eng = Engine(n, s, t, strong_gravity=STRONG, gravity=K_G, scale=K_R, device=local,
                  theta=args.theta, multipole=args.multipole)
     plain = args.theta == 1.0 and args.multipole == 1
@@ -313,7 +339,8 @@ def run_ours(args, world, rank, local):
         return
     # the correction report compares against the plain walk, so it runs only
     # when the plain walk is the workload
-    correction = correction_report(eng, n, args.steps) if plain else None
+    correction = correction_report(eng, n, args.steps) if plain and not large else None
+    fp64 = fp64_checks(eng, n) if large else None
     names = kernel_names()
     pk, pk_kind = peaks()
     hbm = float(pk["hbm_gbs"])
@@ -355,7 +382,8 @@ def run_ours(args, world, rank, local):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": ms_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "config": workload_config(n, m, args.theta, args.multipole),
+        "data": "synthetic",
+        "config": workload_config(n, m, args.theta, args.multipole, args.workload),
         "clocks": clocks_summary(clk_path),
         "gpu_launches": (KERNELS_PER_ITER + (2 if args.multipole == 2 else 0)) * args.steps,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * n,
@@ -367,7 +395,14 @@ def run_ours(args, world, rank, local):
                  "max_level": st["max_level"]},
         "far_field_correction": correction,
     }
-    if world == 1 and not args.no_cpu_baseline:
+    if fp64 is not None:
+        out["fp64_checks"] = fp64
+    if large:
+        # ncu's DRAM count above was taken at scale 20
+        out["roofline"]["traffic"] = None
+        out["cpu_baseline_skipped"] = ("one CPUForceAtlas2::doStep at this size takes minutes; "
+                                       "the reference CPU baseline is in the rmat20 line")
+    if world == 1 and not args.no_cpu_baseline and not large:
         from oracle import oracle as O
         out["cpu_baseline"] = cpu_baseline_sample(O.Graph(s_raw, t_raw), xy0)
     print(json.dumps(out))
@@ -505,8 +540,9 @@ def main():
                     help="Barnes-Hut opening parameter of the rmat20 workload (reference: 1)")
     ap.add_argument("--multipole", type=int, default=1, choices=[1, 2],
                     help="1: cells as point masses (reference); 2: with the quadrupole term")
-    ap.add_argument("--workload", default="rmat20", choices=["rmat20", "batched"],
-                    help="rmat20: the R-MAT scale-20 graph (default); batched: 4096 SBM graphs")
+    ap.add_argument("--workload", default="rmat20", choices=["rmat20", "rmat23", "batched"],
+                    help="rmat20: the R-MAT scale-20 graph (default); rmat23: the large "
+                         "R-MAT scale-23 run; batched: 4096 SBM graphs")
     args = ap.parse_args()
     world, rank, local = dist_setup(args.gpus)
     try:
@@ -518,6 +554,11 @@ def main():
                                       "default arm's line"}))
             else:
                 run_batched(args, world, rank, local)
+        elif args.impl == "reference" and args.workload != "rmat20":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "one CPUForceAtlas2::doStep "
+                                  "at R-MAT scale 23 takes minutes; the reference arm runs on "
+                                  "the rmat20 workload"}))
         elif args.impl == "reference":
             run_reference(args, world, rank)
         else:

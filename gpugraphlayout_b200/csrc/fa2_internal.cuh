@@ -18,7 +18,7 @@ constexpr int kWarp = 32;
 constexpr int kLevels = 32;        // quadrant digits in a 64-bit Morton key
 constexpr int kBodyLevel = 63;     // level code of a body (leaf) node
 constexpr int kMetaShift = 6;      // node meta = next_index << 6 | level code
-constexpr uint32_t kMaxTreeNodes = 1u << 26;
+constexpr uint32_t kMaxTreeNodes = (1u << 26) - 1;  // next index fits the 26 meta bits
 constexpr int kMaxRun = 1024;      // longest run of equal 64-bit keys handled
 constexpr int kDeepLevels = 64;    // levels past 32 used to order such a run
 
