@@ -51,7 +51,7 @@ KERNELS_PER_ITER = 14  # attract, keys, 8 sort passes, tree_count, emit, travers
 # launch at this workload, from an ncu capture of
 #   ncu --set full --clock-control none -k regex:k_attract -s 4 -c 1 \
 #       python bench.py --steps 3 --warmup 3 --no-cpu-baseline
-ATTRACT_TRAFFIC_BYTES = 144_659_712
+ATTRACT_TRAFFIC_BYTES = 146_956_800
 
 
 def clocks_sampler(device: int, path: str):

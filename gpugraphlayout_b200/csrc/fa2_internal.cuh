@@ -99,7 +99,7 @@ struct AttractBucket {
     int block_begin;         // first block index of this bucket
 };
 constexpr int kMaxBuckets = 8;
-constexpr int kAttractBatch = 3;  // row groups per warp in short-row buckets
+constexpr int kAttractBatch = 2;  // row groups per warp in short-row buckets
 struct AttractPlan {
     AttractBucket b[kMaxBuckets];
     int nbuckets;

@@ -630,7 +630,7 @@ __device__ __forceinline__ void attract_long_row(uint32_t b, uint32_t e, int fir
 // block-per-row bucket, 8 rows for the warp-per-row bucket, batches of short
 // rows).
 template <bool LINLOG>
-__global__ void __launch_bounds__(256, LINLOG ? 4 : 6) k_attract(AttractPlan plan, const float2 *__restrict pos,
+__global__ void __launch_bounds__(256, LINLOG ? 4 : 8) k_attract(AttractPlan plan, const float2 *__restrict pos,
                                                  const float *__restrict mass,
                                                  const uint32_t *__restrict off,
                                                  const int4 *__restrict col4,
