@@ -267,24 +267,26 @@ class BatchEngine:
         check(lib().fa2_batch_get_speed(self._b, _ptr(gs), _ptr(se)), "fa2_batch_get_speed")
         return gs[: self.num_graphs], se[: self.num_graphs]
 
-    def configure(self, split: int, small_threads: int = 256) -> None:
+    def configure(self, split: int, small_threads: int = 256, large_threads: int = 1024) -> None:
         """Graphs of at most `split` nodes on CTAs of small_threads threads,
-        the rest on 1024-thread CTAs (split 0: all on 1024)."""
-        check(lib().fa2_batch_configure(self._b, int(split), int(small_threads)),
-              "fa2_batch_configure")
+        the rest on CTAs of large_threads (split 0: one class)."""
+        check(lib().fa2_batch_configure(self._b, int(split), int(small_threads),
+                                        int(large_threads)), "fa2_batch_configure")
 
     def config(self) -> dict:
-        sp, th = C.c_uint32(0), C.c_int32(0)
-        check(lib().fa2_batch_get_config(self._b, C.byref(sp), C.byref(th)), "fa2_batch_get_config")
-        return {"split": sp.value, "small_threads": th.value}
+        sp, th, lt = C.c_uint32(0), C.c_int32(0), C.c_int32(0)
+        check(lib().fa2_batch_get_config(self._b, C.byref(sp), C.byref(th), C.byref(lt)),
+              "fa2_batch_get_config")
+        return {"split": sp.value, "small_threads": th.value, "large_threads": lt.value}
 
     def autotune(self, iters: int = 2) -> dict:
         """Times the candidate configurations on this batch and keeps the
         fastest; the layout state is left as it was."""
-        sp, th, ms = C.c_uint32(0), C.c_int32(0), C.c_float(0.0)
+        sp, th, lt, ms = C.c_uint32(0), C.c_int32(0), C.c_int32(0), C.c_float(0.0)
         check(lib().fa2_batch_autotune(self._b, int(iters), C.byref(sp), C.byref(th),
-                                       C.byref(ms)), "fa2_batch_autotune")
-        return {"split": sp.value, "small_threads": th.value, "ms_per_iter": ms.value}
+                                       C.byref(lt), C.byref(ms)), "fa2_batch_autotune")
+        return {"split": sp.value, "small_threads": th.value, "large_threads": lt.value,
+                "ms_per_iter": ms.value}
 
     def part(self, a, g: int):
         """Rows of graph g in a batch-ordered array."""

@@ -126,9 +126,9 @@ def lib():
     L.fa2_batch_step_timed.argtypes = [vp, C.c_int32, f32p]
     L.fa2_batch_get_forces.argtypes = [vp, vp, vp]
     L.fa2_batch_get_sort_order.argtypes = [vp, vp]
-    L.fa2_batch_configure.argtypes = [vp, C.c_uint32, C.c_int32]
-    L.fa2_batch_get_config.argtypes = [vp, vp, vp]
-    L.fa2_batch_autotune.argtypes = [vp, C.c_int32, vp, vp, vp]
+    L.fa2_batch_configure.argtypes = [vp, C.c_uint32, C.c_int32, C.c_int32]
+    L.fa2_batch_get_config.argtypes = [vp, vp, vp, vp]
+    L.fa2_batch_autotune.argtypes = [vp, C.c_int32, vp, vp, vp, vp]
     L.fa2_batch_get_speed.argtypes = [vp, vp, vp]
     L.fa2_repulsion_noalloc.argtypes = [vp, vp, C.c_uint32, C.POINTER(Params), vp, vp]
     L.fa2_ugraph_load.restype = vp

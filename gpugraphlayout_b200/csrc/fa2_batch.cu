@@ -708,9 +708,9 @@ struct fa2_batch {
     uint32_t *d_order = nullptr;  // the queue order of the current classes
     unsigned *queues = nullptr;   // one ticket counter per class
     // Graphs of at most `split` nodes (class 0) run on CTAs of `small_threads`
-    // threads, the others (class 1) on 1024-thread CTAs.
+    // threads, the others (class 1) on CTAs of `large_threads`.
     uint32_t split = 0;
-    int small_threads = 256;
+    int small_threads = 256, large_threads = 1024;
     BatchClass cls[2];
     cudaStream_t stream = nullptr, side = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evFork = nullptr, evJoin = nullptr;
@@ -770,7 +770,7 @@ int occupancy_for(int threads) {
 
 // Splits the graphs into the two classes, uploads the queue order (class 1
 // then class 0, each largest first) and sizes each class's grid and slots.
-int configure(fa2_batch *b, uint32_t split, int small_threads) {
+int configure(fa2_batch *b, uint32_t split, int small_threads, int large_threads) {
     std::vector<uint32_t> big, small;
     for (uint32_t g : b->order) (b->count[g] <= split ? small : big).push_back(g);
     std::vector<uint32_t> q(big);
@@ -780,7 +780,7 @@ int configure(fa2_batch *b, uint32_t split, int small_threads) {
                             b->stream));
     const std::vector<uint32_t> *members[2] = {&small, &big};
     const uint32_t first[2] = {(uint32_t)big.size(), 0u};
-    const int threads[2] = {small_threads, 1024};
+    const int threads[2] = {small_threads, large_threads};
     for (int k = 0; k < 2; ++k) {
         BatchClass &c = b->cls[k];
         const std::vector<uint32_t> &m = *members[k];
@@ -806,6 +806,7 @@ int configure(fa2_batch *b, uint32_t split, int small_threads) {
     }
     b->split = split;
     b->small_threads = small_threads;
+    b->large_threads = large_threads;
     BCK(cudaStreamSynchronize(b->stream));
     return FA2_OK;
 }
@@ -1013,7 +1014,7 @@ fa2_batch *fa2_batch_create(uint32_t num_graphs, const fa2_graph_desc *graphs,
         cudaMemsetAsync(A.sortd, 0, N * 4, st) || cudaStreamSynchronize(st))
         return fail(FA2_ERR_CUDA);
     // every graph on 1024-thread CTAs until fa2_batch_configure / _autotune
-    if ((s = configure(b, 0, 256))) return fail(s);
+    if ((s = configure(b, 0, 256, 1024))) return fail(s);
     *status = FA2_OK;
     return b;
 }
@@ -1074,23 +1075,26 @@ int fa2_batch_step_timed(fa2_batch *b, int32_t n_iters, float *ms) {
     return check_errors(b);
 }
 
-int fa2_batch_configure(fa2_batch *b, uint32_t split, int32_t small_threads) {
-    if (!b || (small_threads != 256 && small_threads != 512 && small_threads != 1024))
-        return FA2_ERR_INVALID_ARGUMENT;
+int fa2_batch_configure(fa2_batch *b, uint32_t split, int32_t small_threads,
+                        int32_t large_threads) {
+    auto ok = [](int32_t t) { return t == 256 || t == 512 || t == 1024; };
+    if (!b || !ok(small_threads) || !ok(large_threads)) return FA2_ERR_INVALID_ARGUMENT;
     BCK(cudaSetDevice(b->device));
     BCK(cudaStreamSynchronize(b->stream));
-    return configure(b, split, small_threads);
+    return configure(b, split, small_threads, large_threads);
 }
 
-int fa2_batch_get_config(fa2_batch *b, uint32_t *split, int32_t *small_threads) {
+int fa2_batch_get_config(fa2_batch *b, uint32_t *split, int32_t *small_threads,
+                         int32_t *large_threads) {
     if (!b) return FA2_ERR_INVALID_ARGUMENT;
     if (split) *split = b->split;
     if (small_threads) *small_threads = b->small_threads;
+    if (large_threads) *large_threads = b->large_threads;
     return FA2_OK;
 }
 
 int fa2_batch_autotune(fa2_batch *b, int32_t iters, uint32_t *split_out, int32_t *threads_out,
-                       float *ms_out) {
+                       int32_t *large_out, float *ms_out) {
     if (!b || iters <= 0) return FA2_ERR_INVALID_ARGUMENT;
     BCK(cudaSetDevice(b->device));
     if (!b->num_graphs || !b->total_nodes) return FA2_OK;
@@ -1130,24 +1134,34 @@ int fa2_batch_autotune(fa2_batch *b, int32_t iters, uint32_t *split_out, int32_t
                 return FA2_ERR_CUDA;
         return cudaStreamSynchronize(b->stream) == cudaSuccess ? FA2_OK : FA2_ERR_CUDA;
     };
-    // candidates: every graph on 1024-thread CTAs, or the graphs up to a
-    // size on smaller CTAs beside the rest
+    // candidates: the large graphs on 1024- or 512-thread CTAs, with every
+    // graph in that class or the graphs up to a size on smaller CTAs beside
+    struct Cand {
+        uint32_t split;
+        int small, large;
+        bool operator==(const Cand &o) const {
+            return split == o.split && small == o.small && large == o.large;
+        }
+    };
     uint32_t nmax = 1;
     for (uint32_t c : b->count) nmax = std::max(nmax, c);
-    std::vector<std::pair<uint32_t, int>> cand{{0u, 256}};
-    for (uint32_t sp : {256u, 1024u, 4096u, nmax})
-        for (int t : {256, 512})
-            if (sp <= nmax &&
-                std::find(cand.begin(), cand.end(), std::make_pair(sp, t)) == cand.end())
-                cand.emplace_back(sp, t);
-    const uint32_t split0 = b->split;
-    const int threads0 = b->small_threads;
+    std::vector<Cand> cand;
+    for (int large : {1024, 512}) {
+        cand.push_back(Cand{0u, 256, large});
+        for (uint32_t sp : {256u, 1024u, 4096u})
+            for (int t : {256, 512})
+                if (sp < nmax && t < large) cand.push_back(Cand{sp, t, large});
+    }
+    for (int t : {256, 512})
+        if (std::find(cand.begin(), cand.end(), Cand{nmax, t, 1024}) == cand.end())
+            cand.push_back(Cand{nmax, t, 1024});
+    const Cand start{b->split, b->small_threads, b->large_threads};
     float best_ms = 0.0f;
-    std::pair<uint32_t, int> best{split0, threads0};
+    Cand best = start;
     bool found = false;
-    for (const auto &c : cand) {
+    for (const Cand &c : cand) {
         if (s) break;
-        if ((s = configure(b, c.first, c.second))) break;
+        if ((s = configure(b, c.split, c.small, c.large))) break;
         if ((s = restore())) break;
         float ms = 0.0f;
         if (cudaEventRecord(b->ev0, b->stream) != cudaSuccess) s = FA2_ERR_CUDA;
@@ -1162,7 +1176,8 @@ int fa2_batch_autotune(fa2_batch *b, int32_t iters, uint32_t *split_out, int32_t
             found = true;
         }
     }
-    const int s2 = configure(b, found ? best.first : split0, found ? best.second : threads0);
+    const Cand pick = found ? best : start;
+    const int s2 = configure(b, pick.split, pick.small, pick.large);
     const int s3 = restore();
     for (Saved &x : saved)
         if (x.dst) cudaFree(x.dst);
@@ -1171,6 +1186,7 @@ int fa2_batch_autotune(fa2_batch *b, int32_t iters, uint32_t *split_out, int32_t
     if (s3) return s3;
     if (split_out) *split_out = b->split;
     if (threads_out) *threads_out = b->small_threads;
+    if (large_out) *large_out = b->large_threads;
     if (ms_out) *ms_out = best_ms / (float)iters;
     return FA2_OK;
 }

@@ -245,19 +245,23 @@ int fa2_batch_step_timed(fa2_batch *batch, int32_t n_iters, float *ms);
  * quadtree (graph-local ids, the reference's sortd); the adaptive speed and
  * speed efficiency per graph. */
 /* CTA sizes: graphs of at most `split` nodes run on CTAs of small_threads
- * threads (256, 512 or 1024) beside the others on 1024-thread CTAs, each
- * class from its own queue; split 0 (the default) runs every graph on 1024
- * threads.  Results do not depend on the choice, only the speed does. */
-int fa2_batch_configure(fa2_batch *batch, uint32_t split, int32_t small_threads);
-int fa2_batch_get_config(fa2_batch *batch, uint32_t *split, int32_t *small_threads);
+ * threads beside the others on CTAs of large_threads threads (each 256, 512
+ * or 1024), each class from its own queue; the default is split 0 with
+ * 1024-thread CTAs, one class.  Results do not depend on the choice, only the
+ * speed does. */
+int fa2_batch_configure(fa2_batch *batch, uint32_t split, int32_t small_threads,
+                        int32_t large_threads);
+int fa2_batch_get_config(fa2_batch *batch, uint32_t *split, int32_t *small_threads,
+                         int32_t *large_threads);
 
 /* Picks the configuration by measurement: times `iters` iterations of every
- * candidate split (256, 1024, 4096 nodes, all graphs, or none) and small CTA
- * size (256, 512) on this batch, keeps the fastest, and puts the layout state
+ * candidate on this batch (large CTAs of 1024 or 512 threads; no split, or
+ * graphs up to 256, 1024 or 4096 nodes on CTAs of 256 or 512 threads; or all
+ * graphs on the small CTAs), keeps the fastest, and puts the layout state
  * (positions, speeds, and the forces and orders of the last iteration) back
  * as it was.  Returns the choice and its ms per iteration. */
 int fa2_batch_autotune(fa2_batch *batch, int32_t iters, uint32_t *split,
-                       int32_t *small_threads, float *ms_per_iter);
+                       int32_t *small_threads, int32_t *large_threads, float *ms_per_iter);
 
 int fa2_batch_get_forces(fa2_batch *batch, float *f_total, float *f_attr_grav);
 int fa2_batch_get_sort_order(fa2_batch *batch, uint32_t *order);

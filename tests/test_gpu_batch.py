@@ -134,10 +134,11 @@ def test_results_do_not_depend_on_the_cta_sizes():
     graphs = _graphs([50, 3000, 120, 777, 1999, 64, 5000, 300, 40, 2500])
     xy = np.concatenate(_positions(graphs))
     runs = []
-    for split, threads in ((0, 256), (1000, 256), (3000, 512), (10000, 256)):
+    for split, threads, large in ((0, 256, 1024), (1000, 256, 1024), (3000, 512, 1024),
+                                  (10000, 256, 1024), (0, 256, 512), (500, 256, 512)):
         b = _batch(graphs, scale=2.0)
-        b.configure(split, threads)
-        assert b.config() == {"split": split, "small_threads": threads}
+        b.configure(split, threads, large)
+        assert b.config() == {"split": split, "small_threads": threads, "large_threads": large}
         b.set_positions(xy)
         b.step(3)
         runs.append((b.get_positions(), b.sort_order(), b.speeds()))
@@ -157,7 +158,8 @@ def test_autotune_leaves_the_layout_state_as_it_was():
     before = (b.get_positions(), b.sort_order(), b.speeds())
     cfg = b.autotune(2)
     assert cfg["small_threads"] in (256, 512) and cfg["ms_per_iter"] > 0
-    assert b.config() == {"split": cfg["split"], "small_threads": cfg["small_threads"]}
+    assert b.config() == {"split": cfg["split"], "small_threads": cfg["small_threads"],
+                          "large_threads": cfg["large_threads"]}
     after = (b.get_positions(), b.sort_order(), b.speeds())
     assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
     assert np.array_equal(before[2][0], after[2][0])
@@ -168,4 +170,4 @@ def test_autotune_leaves_the_layout_state_as_it_was():
     b.step(2)
     assert np.array_equal(b.get_positions(), ref.get_positions())
     with pytest.raises(Fa2Error):
-        b.configure(100, 128)
+        b.configure(100, 128, 1024)
