@@ -712,6 +712,9 @@ struct fa2_batch {
     uint32_t split = 0;
     int small_threads = 256, large_threads = 1024;
     BatchClass cls[2];
+    // the launch of one step call, captured for its iteration count
+    cudaGraphExec_t exec = nullptr;
+    int exec_iters = -1;
     cudaStream_t stream = nullptr, side = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evFork = nullptr, evJoin = nullptr;
 };
@@ -739,7 +742,14 @@ int balloc(fa2_batch *b, T **p, size_t count) {
     return FA2_OK;
 }
 
+void drop_graph(fa2_batch *b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+    b->exec_iters = -1;
+}
+
 void bfree(fa2_batch *b) {
+    drop_graph(b);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->evFork) cudaEventDestroy(b->evFork);
@@ -771,6 +781,7 @@ int occupancy_for(int threads) {
 // Splits the graphs into the two classes, uploads the queue order (class 1
 // then class 0, each largest first) and sizes each class's grid and slots.
 int configure(fa2_batch *b, uint32_t split, int small_threads, int large_threads) {
+    drop_graph(b);  // the classes' grids and arguments are part of the graph
     std::vector<uint32_t> big, small;
     for (uint32_t g : b->order) (b->count[g] <= split ? small : big).push_back(g);
     std::vector<uint32_t> q(big);
@@ -844,6 +855,30 @@ int launch_batch(fa2_batch *b, int iters) {
         BCK(cudaEventRecord(b->evJoin, b->side));
         BCK(cudaStreamWaitEvent(b->stream, b->evJoin, 0));
     }
+    return FA2_OK;
+}
+
+// One step call as a CUDA graph: the queue reset, the fork, a persistent
+// launch per class and the join, captured once per iteration count and
+// replayed.
+int run_batch(fa2_batch *b, int iters) {
+    if (!b->exec || b->exec_iters != iters) {
+        drop_graph(b);
+        BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        const int s = launch_batch(b, iters);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+        if (s) {
+            if (g) cudaGraphDestroy(g);
+            return s;
+        }
+        BCK(e);
+        const cudaError_t e2 = cudaGraphInstantiate(&b->exec, g, 0);
+        cudaGraphDestroy(g);
+        BCK(e2);
+        b->exec_iters = iters;
+    }
+    BCK(cudaGraphLaunch(b->exec, b->stream));
     return FA2_OK;
 }
 
@@ -1056,7 +1091,7 @@ int fa2_batch_step(fa2_batch *b, int32_t n_iters) {
     if (!b || n_iters < 0) return FA2_ERR_INVALID_ARGUMENT;
     BCK(cudaSetDevice(b->device));
     if (!n_iters || !b->num_graphs) return FA2_OK;
-    int s = launch_batch(b, n_iters);
+    int s = run_batch(b, n_iters);
     if (s) return s;
     return check_errors(b);
 }
@@ -1067,7 +1102,7 @@ int fa2_batch_step_timed(fa2_batch *b, int32_t n_iters, float *ms) {
     *ms = 0.0f;
     if (!n_iters || !b->num_graphs) return FA2_OK;
     BCK(cudaEventRecord(b->ev0, b->stream));
-    int s = launch_batch(b, n_iters);
+    int s = run_batch(b, n_iters);
     if (s) return s;
     BCK(cudaEventRecord(b->ev1, b->stream));
     BCK(cudaEventSynchronize(b->ev1));
