@@ -45,8 +45,11 @@ WIDTH = 2.0e4
 RMAT = {"rmat20": (SCALE, DRAWS, WIDTH), "rmat23": (23, 134_217_728, 2.0e5)}
 FP64_SAMPLES = 4096
 FP64_EVERY, FP64_CHECKS = 50, 4
-KERNELS_PER_ITER = 14  # attract, keys, 8 sort passes, tree_count, emit, traverse, displace
-# (the quadrupole walk adds the moment scan and the per-cell a2 kernel)
+# kernels per iteration besides the sort passes: attract, keys, tree_count, emit,
+# traverse, displace; the sort is 8 passes, or 6 passes and a fix-up pass after
+# shallow trees (fa2_stats.sort_passes); the quadrupole walk adds the moment
+# scan and the per-cell a2 kernel
+KERNELS_PER_ITER = 6
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_attract
 # launch at this workload, from an ncu capture of
 #   ncu --set full --clock-control none -k regex:k_attract -s 4 -c 1 \
@@ -385,7 +388,8 @@ def run_ours(args, world, rank, local):
         "data": "synthetic",
         "config": workload_config(n, m, args.theta, args.multipole, args.workload),
         "clocks": clocks_summary(clk_path),
-        "gpu_launches": (KERNELS_PER_ITER + (2 if args.multipole == 2 else 0)) * args.steps,
+        "gpu_launches": (KERNELS_PER_ITER + st["sort_passes"] + (st["sort_passes"] < 8)
+                         + (2 if args.multipole == 2 else 0)) * args.steps,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * n,
                 "d2h_bytes_per_step": 8 * n},
         "roofline": roofline,

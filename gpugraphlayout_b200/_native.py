@@ -59,7 +59,8 @@ class Stats(C.Structure):
                 ("nnz_padded", C.c_uint64), ("global_speed", C.c_float),
                 ("speed_efficiency", C.c_float), ("radius", C.c_float),
                 ("root_x", C.c_float), ("root_y", C.c_float),
-                ("interactions", C.c_uint64), ("visits", C.c_uint64)]
+                ("interactions", C.c_uint64), ("visits", C.c_uint64),
+                ("sort_passes", C.c_int32)]
 
 
 class Fa2Error(RuntimeError):

@@ -236,6 +236,7 @@ void enqueue_iteration(fa2_ctx *c, bool full, bool perturb_first, bool timed) {
     mark(S_KEYS, 1, A);
     mark(S_SORT, 0, A);
     launch_sort(b, A);
+    launch_fix_low(b, c->nsm, A);
     mark(S_SORT, 1, A);
     mark(S_COUNT, 0, A);
     launch_tree_count(b, quad, A);
@@ -356,8 +357,17 @@ int resolve_poison(fa2_ctx *c, DevState *st) {
     int rounds = 0;
     while (st->poison) {
         if (++rounds > kMaxReplayRounds) return FA2_ERR_DEVICE_LIMIT;
+        // A run of keys equal in the sorted digits was too long for
+        // k_fix_low: the iteration again, sorted on every digit.  Otherwise
+        // coincident bodies: the iteration again after the .99 scaling.
+        const bool resort = st->resort != 0;
+        if (resort) {
+            c->b.sort_first = 0;
+            drop_graphs(c);
+            CK(cudaMemsetAsync(&c->b.st->resort, 0, sizeof(int), c->sA));
+        }
         CK(cudaMemsetAsync(&c->b.st->poison, 0, sizeof(int), c->sA));
-        enqueue_iteration(c, false, true, false);
+        enqueue_iteration(c, false, !resort, false);
         CK(cudaGetLastError());
         int s = read_state(c, st);
         if (s) return s;
@@ -365,6 +375,16 @@ int resolve_poison(fa2_ctx *c, DevState *st) {
     }
     c->last_perturb_rounds = rounds;
     return FA2_OK;
+}
+
+// After a tree no deeper than kShallowLevel the next sorts skip their two
+// lowest digits (k_fix_low keeps the order exact); the choice is part of the
+// captured graphs, which are dropped when it changes.
+void choose_sort_passes(fa2_ctx *c, const DevState &st) {
+    const int first = (st.max_level > 0 && st.max_level <= kShallowLevel) ? 2 : 0;
+    if (first == c->b.sort_first) return;
+    c->b.sort_first = first;
+    drop_graphs(c);
 }
 
 // Runs n iterations; with `timed`, kernel_sum accumulates per-slot device ms.
@@ -378,6 +398,7 @@ int run_steps(fa2_ctx *c, int32_t n_iters, bool timed, std::vector<double> *kern
     int done = 0;
     c->last_perturb_rounds = 0;
     while (done < n_iters) {
+        choose_sort_passes(c, st);
         // (re)captured here: a guard fallback drops the graphs
         if (!*exec) {
             s = capture(c, timed, exec);
@@ -699,6 +720,7 @@ int fa2_get_stats(fa2_ctx *c, fa2_stats *out) {
     out->root_y = st.rooty;
     out->interactions = st.interactions;
     out->visits = st.visits;
+    out->sort_passes = 8 - c->b.sort_first;
     return FA2_OK;
 }
 

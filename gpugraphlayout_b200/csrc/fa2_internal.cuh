@@ -45,6 +45,7 @@ struct DevState {
     unsigned long long interactions;  // body-node force terms of the last traversal
     unsigned long long visits;        // body-node acceptance tests of the last traversal
     float trav_radius;                // root radius the last traversal used
+    int resort;                       // a sort that skipped low digits needs all of them
 };
 
 // Per-iteration scratch, cleared by one memset at the start of an iteration.
@@ -160,6 +161,7 @@ struct Buffers {
     DevState *st;
     IterCounters *ctr;
     int sort_rounds;          // keys per sort thread (tile = kSortThreads x rounds)
+    int sort_first;           // first sort pass (0, or 2 after shallow trees: k_fix_low)
     uint32_t *sort_counts;    // [8][sort tiles][256]: digit counts per tile and pass
     uint32_t *count_status;   // [count tiles]
 };
@@ -180,6 +182,10 @@ constexpr int kDispThreads = 512;
 void launch_bbox(const Buffers &b, int nblocks, cudaStream_t s);
 void launch_keys(const Buffers &b, int nsm, cudaStream_t s);
 void launch_sort(const Buffers &b, cudaStream_t s);
+void launch_fix_low(const Buffers &b, int nsm, cudaStream_t s);
+// Deepest tree level after which the next sort may skip its two lowest
+// digits (levels 24..31): bodies then share at most that many digits.
+constexpr int kShallowLevel = 22;
 void launch_runs(const Buffers &b, int perturb, int nsm, cudaStream_t s);
 void launch_tree_count(const Buffers &b, bool keep_moments, cudaStream_t s);
 void launch_moments(const Buffers &b, cudaStream_t s);

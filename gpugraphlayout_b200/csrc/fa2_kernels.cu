@@ -99,13 +99,15 @@ __global__ void __launch_bounds__(kBBoxThreads) k_bbox(int n, const float2 *__re
 
 // ------------------------------------------------------------------- keys --
 
-// One block per sort tile: the tile's keys, the digit-0 counts of the tile
-// (the first sort pass's per-tile input) and the tile's share of the digit
-// histograms of all eight passes (order-independent, so counted once here).
-__global__ void __launch_bounds__(1024) k_keys(int n, int tile, const float2 *__restrict pos,
+// One block per sort tile: the tile's keys, the tile's counts of the digit
+// of the first sort pass (that pass's per-tile input) and the tile's share of
+// the digit histograms of all eight passes (order-independent, so counted
+// once here).
+__global__ void __launch_bounds__(1024) k_keys(int n, int tile, int first,
+                                              const float2 *__restrict pos,
                                               const DevState *__restrict st,
                                               uint64_t *__restrict keys, uint32_t *__restrict vals,
-                                              IterCounters *ctr, uint32_t *__restrict counts0) {
+                                              IterCounters *ctr, uint32_t *__restrict counts) {
     __shared__ unsigned s_hist[8][256];
     if (st->err || st->poison) return;
     for (int j = threadIdx.x; j < 8 * 256; j += blockDim.x) (&s_hist[0][0])[j] = 0;
@@ -124,7 +126,8 @@ __global__ void __launch_bounds__(1024) k_keys(int n, int tile, const float2 *__
     __syncthreads();
     for (int j = threadIdx.x; j < 8 * 256; j += blockDim.x) {
         unsigned c = (&s_hist[0][0])[j];
-        if (j < 256) counts0[(size_t)blockIdx.x * 256 + j] = c;
+        if ((j >> 8) == first)
+            counts[((size_t)first * gridDim.x + blockIdx.x) * 256 + (j & 255)] = c;
         if (c) atomicAdd(&(&ctr->hist[0][0])[j], c);
     }
 }
@@ -731,8 +734,8 @@ void launch_bbox(const Buffers &b, int nblocks, cudaStream_t s) {
 void launch_keys(const Buffers &b, int nsm, cudaStream_t s) {
     (void)nsm;
     k_keys<<<sort_tiles(b.n, b.sort_rounds), 1024, 0, s>>>(
-        b.n, kSortThreads * b.sort_rounds, b.pos, b.st, b.keys[0], b.vals[0], b.ctr,
-        b.sort_counts);
+        b.n, kSortThreads * b.sort_rounds, b.sort_first, b.pos, b.st, b.keys[0], b.vals[0],
+        b.ctr, b.sort_counts);
 }
 
 

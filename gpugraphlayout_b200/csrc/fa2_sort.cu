@@ -1,5 +1,7 @@
 // fa2_sort.cu -- stable LSD radix sort of (64-bit Morton key, 32-bit node id)
 // pairs, 8 passes of 8-bit digits, one kernel per pass, no inter-block waits.
+// After a shallow tree the sort starts at pass 2 and k_fix_low orders the
+// runs of keys equal in the top 48 bits (see there).
 //
 // The keys are cut into fixed tiles of kSortThreads x R keys (R = 4..6 rounds
 // per thread, chosen per context so that the tiles fit one per SM where they
@@ -192,10 +194,47 @@ __global__ void __launch_bounds__(kSortThreads, R == kSortMinRounds ? 2 : 1) k_s
     }
 }
 
+// After a sort that skipped the lowest `first` digits, keys equal in the
+// sorted digits form runs in input order.  Sorting each run by the full key,
+// stably, gives exactly the order of the full sort.  A run longer than
+// kMaxRun asks for the iteration again with every digit (resort + poison: the
+// iteration's later kernels skip their work and the host replays it).
+__global__ void __launch_bounds__(256) k_fix_low(int n, int first, uint64_t *__restrict keys,
+                                                 uint32_t *__restrict vals, DevState *st) {
+    if (st->err || st->poison) return;
+    const int low = 8 * first;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k + 1 < n;
+         k += gridDim.x * blockDim.x) {
+        const uint64_t hk = keys[k] >> low;
+        if ((keys[k + 1] >> low) != hk || (k > 0 && (keys[k - 1] >> low) == hk)) continue;
+        int len = 2;
+        while (k + len < n && (keys[k + len] >> low) == hk && len <= kMaxRun) ++len;
+        if (len > kMaxRun) {
+            atomicExch(&st->resort, 1);
+            atomicExch(&st->poison, 1);
+            continue;
+        }
+        uint64_t *kr = keys + k;
+        uint32_t *vr = vals + k;
+        for (int a = 1; a < len; ++a) {  // insertion sort, stable
+            const uint64_t ka = kr[a];
+            const uint32_t va = vr[a];
+            int j = a - 1;
+            while (j >= 0 && kr[j] > ka) {
+                kr[j + 1] = kr[j];
+                vr[j + 1] = vr[j];
+                --j;
+            }
+            kr[j + 1] = ka;
+            vr[j + 1] = va;
+        }
+    }
+}
+
 template <int R>
 void launch_passes(const Buffers &b, cudaStream_t s) {
     const int tiles = sort_tiles(b.n, R);
-    for (int pass = 0; pass < 8; ++pass) {
+    for (int pass = b.sort_first; pass < 8; ++pass) {
         const int src = pass & 1, dst = src ^ 1;
         k_sort_pass<R><<<tiles, kSortThreads, sizeof(SortSmem<R>), s>>>(
             b.n, pass, b.keys[src], b.vals[src], b.keys[dst], b.vals[dst], b.ctr, b.sort_counts,
@@ -212,6 +251,13 @@ void sort_set_smem_attr() {
                          (int)sizeof(SortSmem<5>));
     cudaFuncSetAttribute(k_sort_pass<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)sizeof(SortSmem<6>));
+}
+
+void launch_fix_low(const Buffers &b, int nsm, cudaStream_t s) {
+    if (b.sort_first <= 0 || b.n < 2) return;
+    int grid = (b.n + 255) / 256;
+    grid = grid > nsm * 8 ? nsm * 8 : grid;
+    k_fix_low<<<grid, 256, 0, s>>>(b.n, b.sort_first, b.keys[0], b.vals[0], b.st);
 }
 
 void launch_sort(const Buffers &b, cudaStream_t s) {
