@@ -377,11 +377,13 @@ int resolve_poison(fa2_ctx *c, DevState *st) {
     return FA2_OK;
 }
 
-// After a tree no deeper than kShallowLevel the next sorts skip their two
-// lowest digits (k_fix_low keeps the order exact); the choice is part of the
-// captured graphs, which are dropped when it changes.
+// After a tree no deeper than kShallowLevel (kMidLevel) the next sorts skip
+// their two lowest digits (their lowest one); k_fix_low keeps the order
+// exact.  The choice is part of the captured graphs, which are dropped when
+// it changes.
 void choose_sort_passes(fa2_ctx *c, const DevState &st) {
-    const int first = (st.max_level > 0 && st.max_level <= kShallowLevel) ? 2 : 0;
+    const int l = st.max_level;
+    const int first = l <= 0 ? 0 : (l <= kShallowLevel ? 2 : (l <= kMidLevel ? 1 : 0));
     if (first == c->b.sort_first) return;
     c->b.sort_first = first;
     drop_graphs(c);

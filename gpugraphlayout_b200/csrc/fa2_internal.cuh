@@ -161,7 +161,7 @@ struct Buffers {
     DevState *st;
     IterCounters *ctr;
     int sort_rounds;          // keys per sort thread (tile = kSortThreads x rounds)
-    int sort_first;           // first sort pass (0, or 2 after shallow trees: k_fix_low)
+    int sort_first;           // first sort pass (0; 1 or 2 after shallow trees: k_fix_low)
     uint32_t *sort_counts;    // [8][sort tiles][256]: digit counts per tile and pass
     uint32_t *count_status;   // [count tiles]
 };
@@ -183,9 +183,11 @@ void launch_bbox(const Buffers &b, int nblocks, cudaStream_t s);
 void launch_keys(const Buffers &b, int nsm, cudaStream_t s);
 void launch_sort(const Buffers &b, cudaStream_t s);
 void launch_fix_low(const Buffers &b, int nsm, cudaStream_t s);
-// Deepest tree level after which the next sort may skip its two lowest
-// digits (levels 24..31): bodies then share at most that many digits.
+// Deepest tree levels after which the next sort may skip its two lowest
+// digits (levels 24..31) or its lowest one (levels 28..31): bodies then share
+// at most that many digits, two levels short of the skipped ones.
 constexpr int kShallowLevel = 22;
+constexpr int kMidLevel = 26;
 void launch_runs(const Buffers &b, int perturb, int nsm, cudaStream_t s);
 void launch_tree_count(const Buffers &b, bool keep_moments, cudaStream_t s);
 void launch_moments(const Buffers &b, cudaStream_t s);

@@ -733,8 +733,10 @@ void launch_bbox(const Buffers &b, int nblocks, cudaStream_t s) {
 
 void launch_keys(const Buffers &b, int nsm, cudaStream_t s) {
     (void)nsm;
+    // the first sort pass reads buffer (first & 1), so the passes end in buffer 0
+    const int in = b.sort_first & 1;
     k_keys<<<sort_tiles(b.n, b.sort_rounds), 1024, 0, s>>>(
-        b.n, kSortThreads * b.sort_rounds, b.sort_first, b.pos, b.st, b.keys[0], b.vals[0],
+        b.n, kSortThreads * b.sort_rounds, b.sort_first, b.pos, b.st, b.keys[in], b.vals[in],
         b.ctr, b.sort_counts);
 }
 

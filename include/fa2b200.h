@@ -130,10 +130,10 @@ typedef struct {
     float radius, root_x, root_y;
     uint64_t interactions;      /* body-node force terms of the last traversal */
     uint64_t visits;            /* body-node acceptance tests of the last traversal */
-    int32_t sort_passes;        /* 8-bit digit passes of the last step's sorts: 8, or 6
-                                   after a tree no deeper than level 22 (runs of keys
-                                   equal in the top 48 bits are then ordered by a
-                                   fix-up pass) */
+    int32_t sort_passes;        /* 8-bit digit passes of the last step's sorts: 8; 6
+                                   after a tree no deeper than level 22, 7 after one no
+                                   deeper than 26 (runs of keys equal in the sorted
+                                   top bits are then ordered by a fix-up pass) */
 } fa2_stats;
 
 int fa2_get_stats(fa2_ctx *ctx, fa2_stats *out);

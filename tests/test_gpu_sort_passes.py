@@ -1,8 +1,9 @@
 """The sort's low digits after a shallow tree.
 
 When the last tree was no deeper than level 22, the next sort skips its two
-lowest 8-bit digits (quadrant levels 24..31) and a fix-up kernel sorts each
-run of keys equal in the remaining digits by the full key.  That gives the
+lowest 8-bit digits (quadrant levels 24..31); no deeper than 26, its lowest
+one (levels 28..31).  A fix-up kernel then sorts each run of keys equal in
+the sorted digits by the full key.  That gives the
 order of the full sort exactly.  A run longer than 1024 bodies instead
 replays the iteration with every digit.  Both paths must leave the body
 order bit-exact with the oracle's (the reference's in-order tree sort).
@@ -49,6 +50,7 @@ def _engine_after_shallow_step(g, seed):
     e.set_positions(_anchored(g, seed))
     e.step(1)
     assert 0 < e.stats()["max_level"] <= 22  # the next sort skips two digits
+    assert e.stats()["sort_passes"] == 8
     return e
 
 
@@ -85,3 +87,29 @@ def test_a_run_too_long_for_the_fix_up_replays_with_every_digit(ba3k):
     # and the layout goes on from there
     e.step(3)
     assert np.isfinite(e.get_positions()).all()
+
+
+def test_seven_passes_after_a_tree_of_depth_26(ba3k):
+    """A pair sharing 26 quadrant digits makes the tree 26 deep: the next
+    sort skips one digit (levels 28..31), and clusters sharing 28 digits are
+    put in order by the fix-up."""
+    from gpugraphlayout_b200 import Engine
+    from oracle import oracle as O
+    g = ba3k
+    w26, w28 = 2048.0 / 2 ** 26, 2048.0 / 2 ** 28
+    e = Engine(g.n, g.sources, g.targets, strong_gravity=True, scale=10.0)
+    xy = _anchored(g, 35)
+    xy[2] = (0.25 * w26, 0.25 * w26)
+    xy[3] = (0.75 * w26, 0.75 * w26)
+    e.set_positions(xy)
+    e.step(1)
+    assert e.stats()["max_level"] == 26
+    xy = _anchored(g, 36)
+    for c in range(10):  # ten 2 x 2 clusters, each centred in its own level-28 cell
+        for j in range(4):
+            xy[2 + 4 * c + j] = ((c + 0.5) * w28 + SPACING * (j % 2 - 0.5),
+                                 0.5 * w28 + SPACING * (j // 2 - 0.5))
+    e.set_positions(xy)
+    e.step(1)
+    assert e.stats()["sort_passes"] == 7
+    assert np.array_equal(e.sort_order(), O.Tree(xy, g.mass).sort().astype(np.uint32))
