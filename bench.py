@@ -489,14 +489,17 @@ def run_batched(args, world, rank, local):
     ms_max = barrier_max(world, ms)
     value = args.steps / (ms_max / 1000.0)
 
-    # end to end through the C ABI: positions in, one iteration, positions out
-    host = np.ascontiguousarray(eng.get_positions())
+    # end to end through the C ABI: positions in from pinned host memory, one
+    # iteration, positions out
+    host = torch.empty((max(eng.n, 1), 2), dtype=torch.float32, pin_memory=True)
+    host.numpy()[: eng.n] = eng.get_positions()
+    ptr = host.data_ptr()
     barrier(world)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        eng.set_positions(host)
+        eng.set_positions_ptr(ptr)
         eng.step(1)
-        host = eng.get_positions()
+        eng.get_positions_ptr(ptr)
     e2e = args.steps / barrier_max(world, time.perf_counter() - t0)
     if rank != 0:
         return

@@ -241,6 +241,15 @@ class BatchEngine:
         check(lib().fa2_batch_get_positions(self._b, _ptr(out)), "fa2_batch_get_positions")
         return out
 
+    def set_positions_ptr(self, host_ptr: int) -> None:
+        """Upload from a raw host pointer (e.g. pinned memory), n x 2 floats."""
+        check(lib().fa2_batch_set_positions(self._b, C.c_void_p(host_ptr)),
+              "fa2_batch_set_positions")
+
+    def get_positions_ptr(self, host_ptr: int) -> None:
+        check(lib().fa2_batch_get_positions(self._b, C.c_void_p(host_ptr)),
+              "fa2_batch_get_positions")
+
     def step(self, n_iters: int = 1) -> None:
         check(lib().fa2_batch_step(self._b, int(n_iters)), "fa2_batch_step")
 

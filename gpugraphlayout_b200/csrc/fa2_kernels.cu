@@ -120,8 +120,8 @@ __global__ void __launch_bounds__(1024) k_keys(int n, int tile, int first,
         uint64_t key = morton_key(p.x, p.y, rx, ry, rr);
         keys[i] = key;
         vals[i] = (uint32_t)i;
-#pragma unroll
-        for (int ps = 0; ps < 8; ++ps) atomicAdd(&s_hist[ps][(key >> (8 * ps)) & 255], 1u);
+        // the histograms of the passes the sort runs
+        for (int ps = first; ps < 8; ++ps) atomicAdd(&s_hist[ps][(key >> (8 * ps)) & 255], 1u);
     }
     __syncthreads();
     for (int j = threadIdx.x; j < 8 * 256; j += blockDim.x) {
