@@ -205,3 +205,47 @@ def test_graph_viewer_cli_matches_api(tmp_path):
     r3 = subprocess.run([exe, "gpu", "3", "1", "sg", "10", "1", "exact", path, str(outdir), "bin"],
                         capture_output=True, text=True, timeout=60)
     assert r3.returncode != 0 and "requires Barnes-Hut" in r3.stderr
+
+
+def test_graphs_of_no_and_one_node():
+    """No nodes: every call works and does nothing.  One node: the tree is the
+    root cell and the body, the body's own term is zero, so only gravity
+    moves it, towards the origin."""
+    from gpugraphlayout_b200 import Engine
+    none = np.zeros(0, np.uint32)
+    e0 = Engine(0, none, none)
+    e0.set_positions(np.zeros((0, 2), np.float32))
+    e0.step(3)
+    assert e0.get_positions().shape == (0, 2)
+    e1 = Engine(1, none, none, strong_gravity=True, gravity=1.0, scale=10.0)
+    e1.set_positions(np.array([[30.0, 40.0]], np.float32))
+    e1.step(1)
+    tot, ga = e1.forces()
+    assert np.array_equal(tot, ga)  # no repulsion on a lone body
+    before = 50.0
+    for _ in range(5):
+        e1.step(1)
+        r = float(np.hypot(*e1.get_positions()[0]))
+        assert np.isfinite(r) and r < before
+        before = r
+
+
+def test_batch_with_empty_and_one_node_graphs():
+    """Graphs of 0 and 1 nodes in a batch step like the rest, and the other
+    graphs' layouts do not depend on them."""
+    from gpugraphlayout_b200 import BatchEngine, synth
+    from oracle import oracle as O
+    s, t = synth.sbm_edges(60, 3, 0.1, 0.01, 40.0, seed=5)
+    g = O.Graph(s, t)
+    none = np.zeros(0, np.uint32)
+    xy = O.random_positions(g.n, 500, 500, 6)
+    b = BatchEngine([(0, none, none), (1, none, none), (g.n, g.sources, g.targets)], scale=2.0)
+    b.set_positions(np.concatenate([np.zeros((0, 2), np.float32),
+                                    np.array([[5.0, -5.0]], np.float32), xy]))
+    b.step(4)
+    pos = b.get_positions()
+    assert pos.shape == (1 + g.n, 2) and np.isfinite(pos).all()
+    alone = BatchEngine([(g.n, g.sources, g.targets)], scale=2.0)
+    alone.set_positions(xy)
+    alone.step(4)
+    assert np.array_equal(pos[1:], alone.get_positions())
