@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(1024) k_keys(int n, int tile, int first,
 //
 // QUAD adds, for every accepted cell, the quadrupole term of its far field,
 // conj(a2 / w^3) = conj(a2) u^3 with w = z - Z, u = w / |w|^2 and the softened
-// |w|^2 = d^2 + eps; a2 is the cell's complex second moment (k_quad_up).  No
+// |w|^2 = d^2 + eps; a2 is the cell's complex second moment (k_quad_cells).  No
 // reference counterpart: it is the option fa2_set_approximation selects.
 template <bool QUAD>
 __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
