@@ -52,16 +52,23 @@ class Engine:
     """One fa2_ctx: a graph on the GPU with its ForceAtlas2 state.
 
     ``sources``/``targets`` list each undirected edge once over node ids
-    0..num_nodes-1 (as UGraph.edges() returns them)."""
+    0..num_nodes-1 (as UGraph.edges() returns them).  ``weights`` (optional,
+    one positive weight per edge) with ``delta`` != 0 makes each edge attract
+    with w**delta times the unweighted force (ForceAtlas2's edge weight
+    influence; delta 0, the reference's default, ignores the weights)."""
 
     def __init__(self, num_nodes: int, sources, targets, *, strong_gravity: bool = False,
                  gravity: float = 1.0, scale: float = 1.0, theta: float = 1.0,
                  epssq: float = 0.05 * 0.05, device: int = 0, use_barneshut: bool = True,
-                 linlog: bool = False, multipole: int = 1):
+                 linlog: bool = False, multipole: int = 1, weights=None, delta: float = 0.0):
         L = lib()
         self._src = np.ascontiguousarray(sources, np.uint32)
         self._dst = np.ascontiguousarray(targets, np.uint32)
-        g = GraphDesc(num_nodes, len(self._src), _ptr(self._src), _ptr(self._dst))
+        self._w = None if weights is None else np.ascontiguousarray(weights, np.float32)
+        if self._w is not None and len(self._w) != len(self._src):
+            raise ValueError("one weight per edge")
+        g = GraphDesc(num_nodes, len(self._src), _ptr(self._src), _ptr(self._dst),
+                      _ptr(self._w))
         p = Params()
         L.fa2_default_params(C.byref(p))
         p.use_barneshut = int(use_barneshut)
@@ -69,6 +76,7 @@ class Engine:
         p.gravity, p.scale, p.theta, p.epssq, p.device = gravity, scale, theta, epssq, device
         p.linlog = int(linlog)
         p.multipole = int(multipole)
+        p.delta = delta
         st = C.c_int(0)
         self._ctx = L.fa2_create(C.byref(g), C.byref(p), C.byref(st))
         check(st.value, "fa2_create")

@@ -42,14 +42,15 @@ STATUS_NAMES = {
 
 class GraphDesc(C.Structure):
     _fields_ = [("num_nodes", C.c_uint32), ("num_edges", C.c_uint64),
-                ("sources", C.c_void_p), ("targets", C.c_void_p)]
+                ("sources", C.c_void_p), ("targets", C.c_void_p), ("weights", C.c_void_p)]
 
 
 class Params(C.Structure):
     _fields_ = [("use_barneshut", C.c_int32), ("strong_gravity", C.c_int32),
                 ("gravity", C.c_float), ("scale", C.c_float), ("theta", C.c_float),
                 ("epssq", C.c_float), ("jitter_tolerance", C.c_float), ("k_s_max", C.c_float),
-                ("device", C.c_int32), ("linlog", C.c_int32), ("multipole", C.c_int32)]
+                ("device", C.c_int32), ("linlog", C.c_int32), ("multipole", C.c_int32),
+                ("delta", C.c_float)]
 
 
 class Stats(C.Structure):

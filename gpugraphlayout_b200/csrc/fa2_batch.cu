@@ -913,6 +913,11 @@ fa2_batch *fa2_batch_create(uint32_t num_graphs, const fa2_graph_desc *graphs,
     for (uint32_t g = 0; g < num_graphs; ++g) {
         const fa2_graph_desc &d = graphs[g];
         if (d.num_edges && (!d.sources || !d.targets)) return nullptr;
+        // the batched attraction has no edge weights (w^0 = 1 is accepted)
+        if (d.weights && prm->delta != 0.0f) {
+            *status = FA2_ERR_UNSUPPORTED;
+            return nullptr;
+        }
         for (uint64_t e = 0; e < d.num_edges; ++e)
             if (d.sources[e] >= d.num_nodes || d.targets[e] >= d.num_nodes ||
                 d.sources[e] == d.targets[e])

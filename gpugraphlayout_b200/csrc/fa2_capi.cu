@@ -13,6 +13,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <numeric>
 #include <vector>
@@ -142,8 +143,13 @@ void free_all(fa2_ctx *c) {
 // Nodes in degree-descending order (ties by reference id), a symmetric CSR
 // over that order with each row sorted and padded with its own id to a
 // multiple of four, and the attraction buckets over it.
-void build_graph(fa2_ctx *c, const fa2_graph_desc *g, std::vector<uint32_t> &off,
-                 std::vector<int32_t> &col, std::vector<float> &mass) {
+// The symmetric CSR in internal ids (degree order), rows sorted by
+// neighbour id and padded with the row's own id to a multiple of four.  With
+// `delta` != 0 and edge weights, wcol holds w^delta beside each entry
+// (rounded once from double; 1 on padding), else it stays empty.
+void build_graph(fa2_ctx *c, const fa2_graph_desc *g, float delta, std::vector<uint32_t> &off,
+                 std::vector<int32_t> &col, std::vector<float> &wcol,
+                 std::vector<float> &mass) {
     const uint32_t n = c->n;
     std::vector<uint32_t> deg(n, 0);
     for (uint64_t e = 0; e < g->num_edges; ++e) {
@@ -166,14 +172,39 @@ void build_graph(fa2_ctx *c, const fa2_graph_desc *g, std::vector<uint32_t> &off
     c->nnz_pad = off[n];
     col.assign(std::max<uint64_t>(c->nnz_pad, 4), 0);
     std::vector<uint32_t> fill(off.begin(), off.end() - 1);
-    for (uint64_t e = 0; e < g->num_edges; ++e) {
-        uint32_t a = int_of[g->sources[e]], b = int_of[g->targets[e]];
-        col[fill[a]++] = (int32_t)b;
-        col[fill[b]++] = (int32_t)a;
-    }
-    for (uint32_t i = 0; i < n; ++i) {
-        std::sort(col.begin() + off[i], col.begin() + fill[i]);
-        for (uint32_t q = fill[i]; q < off[i + 1]; ++q) col[q] = (int32_t)i;
+    const bool weighted = g->weights && delta != 0.0f;
+    if (!weighted) {
+        wcol.clear();
+        for (uint64_t e = 0; e < g->num_edges; ++e) {
+            uint32_t a = int_of[g->sources[e]], b = int_of[g->targets[e]];
+            col[fill[a]++] = (int32_t)b;
+            col[fill[b]++] = (int32_t)a;
+        }
+        for (uint32_t i = 0; i < n; ++i) {
+            std::sort(col.begin() + off[i], col.begin() + fill[i]);
+            for (uint32_t q = fill[i]; q < off[i + 1]; ++q) col[q] = (int32_t)i;
+        }
+    } else {
+        // (neighbour id, w^delta bits) pairs, sorted by id: ids are unique in a row
+        std::vector<uint64_t> pair(col.size(), 0);
+        for (uint64_t e = 0; e < g->num_edges; ++e) {
+            uint32_t a = int_of[g->sources[e]], b = int_of[g->targets[e]];
+            const float wd = (float)std::pow((double)g->weights[e], (double)delta);
+            uint32_t bits;
+            memcpy(&bits, &wd, 4);
+            pair[fill[a]++] = (uint64_t)b << 32 | bits;
+            pair[fill[b]++] = (uint64_t)a << 32 | bits;
+        }
+        wcol.assign(col.size(), 1.0f);
+        for (uint32_t i = 0; i < n; ++i) {
+            std::sort(pair.begin() + off[i], pair.begin() + fill[i]);
+            for (uint32_t q = off[i]; q < fill[i]; ++q) {
+                col[q] = (int32_t)(pair[q] >> 32);
+                const uint32_t bits = (uint32_t)pair[q];
+                memcpy(&wcol[q], &bits, 4);
+            }
+            for (uint32_t q = fill[i]; q < off[i + 1]; ++q) col[q] = (int32_t)i;
+        }
     }
     // buckets: lanes per row from the number of 16-byte loads per row
     auto lanes_for = [](uint32_t q) -> int {
@@ -479,6 +510,7 @@ void fa2_default_params(fa2_params *p) {
     p->device = 0;
     p->linlog = 0;
     p->multipole = 1;
+    p->delta = 0.0f;
 }
 
 fa2_ctx *fa2_create(const fa2_graph_desc *g, const fa2_params *prm, int *status) {
@@ -496,6 +528,15 @@ fa2_ctx *fa2_create(const fa2_graph_desc *g, const fa2_params *prm, int *status)
         if (g->sources[e] >= g->num_nodes || g->targets[e] >= g->num_nodes ||
             g->sources[e] == g->targets[e])
             return nullptr;
+    // edge weights: finite and positive, and w^delta finite and positive
+    if (!std::isfinite(prm->delta)) return nullptr;
+    if (g->weights && prm->delta != 0.0f)
+        for (uint64_t e = 0; e < g->num_edges; ++e) {
+            const float w = g->weights[e];
+            if (!(w > 0.0f) || !std::isfinite(w)) return nullptr;
+            const double wd = std::pow((double)w, (double)prm->delta);
+            if (!(wd >= (double)FLT_MIN && wd <= (double)FLT_MAX)) return nullptr;
+        }
     if ((uint64_t)g->num_nodes * 2 + 2 * g->num_edges + 3ull * g->num_nodes >= (1ull << 32) ||
         g->num_nodes >= (1u << 25)) {
         *status = FA2_ERR_TOO_LARGE;
@@ -531,8 +572,8 @@ fa2_ctx *fa2_create(const fa2_graph_desc *g, const fa2_params *prm, int *status)
 
     std::vector<uint32_t> off;
     std::vector<int32_t> col;
-    std::vector<float> mass;
-    build_graph(c, g, off, col, mass);
+    std::vector<float> wcol, mass;
+    build_graph(c, g, prm->delta, off, col, wcol, mass);
 
     auto fail = [&](int s) {
         *status = s;
@@ -547,6 +588,7 @@ fa2_ctx *fa2_create(const fa2_graph_desc *g, const fa2_params *prm, int *status)
     b.capacity = (uint32_t)cap;
     uint32_t *d_off = nullptr, *d_ref = nullptr;
     int4 *d_col = nullptr;
+    float4 *d_w = nullptr;
     int s = FA2_OK;
     if ((s = dalloc(c, &b.pos, n)) || (s = dalloc(c, &b.fprev, n)) || (s = dalloc(c, &b.f, n)) ||
         (s = dalloc(c, &b.fag, n)) || (s = dalloc(c, &b.mass, n)) ||
@@ -567,9 +609,11 @@ fa2_ctx *fa2_create(const fa2_graph_desc *g, const fa2_params *prm, int *status)
     c->bbox_blocks = c->nsm * 2;
     // partial boxes of k_bbox (bbox_blocks) and of k_displace (up to 4 per SM)
     if ((s = dalloc(c, &b.bbox_partial, (size_t)c->nsm * 4))) return fail(s);
+    if (!wcol.empty() && (s = dalloc(c, &d_w, wcol.size() / 4))) return fail(s);
     c->kp.nsm = c->nsm;
     b.csr_off = d_off;
     b.csr_col4 = d_col;
+    b.csr_w4 = d_w;
     b.ref_of = d_ref;
     // one memset clears counters, histograms, per-tile digit counts and the
     // tree-count look-back flags
@@ -607,6 +651,7 @@ fa2_ctx *fa2_create(const fa2_graph_desc *g, const fa2_params *prm, int *status)
     cudaStream_t A = c->sA;
     if (cudaMemcpyAsync(d_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice, A) ||
         cudaMemcpyAsync(d_col, col.data(), col.size() * 4, cudaMemcpyHostToDevice, A) ||
+        (d_w && cudaMemcpyAsync(d_w, wcol.data(), wcol.size() * 4, cudaMemcpyHostToDevice, A)) ||
         cudaMemcpyAsync(d_ref, c->ref_of.data(), (size_t)n * 4, cudaMemcpyHostToDevice, A) ||
         cudaMemcpyAsync(b.mass, mass.data(), (size_t)n * 4, cudaMemcpyHostToDevice, A) ||
         cudaMemsetAsync(b.pos, 0, (size_t)n * 8, A) || cudaMemsetAsync(b.fprev, 0, (size_t)n * 8, A) ||

@@ -69,6 +69,8 @@ __device__ __forceinline__ float2 with_gravity(float2 p, float m, float ax, floa
 // One neighbour's pull: p_j - p_i, or with linear-log attraction (use_linlog
 // of the reference's CPU path, RPCPUForceAtlas2.cpp:59-67) that vector times
 // log(1 + d) / d, d = 0 taken as FLT_MAX (padding ids give the zero vector).
+// The product is rounded on its own (__fmul_rn, never fused into the sum that
+// follows), as the reference's CPU code rounds it before adding.
 template <bool LINLOG>
 __device__ __forceinline__ float2 pull(float2 q, float2 p) {
     float dx = q.x - p.x, dy = q.y - p.y;
@@ -76,8 +78,8 @@ __device__ __forceinline__ float2 pull(float2 q, float2 p) {
         const float ex = p.x - q.x, ey = p.y - q.y;
         const float dist = sqrtf(ex * ex + ey * ey);
         const float w = dist == 0.0f ? FLT_MAX : logf(1 + dist) / dist;
-        dx *= w;
-        dy *= w;
+        dx = __fmul_rn(dx, w);
+        dy = __fmul_rn(dy, w);
     }
     return make_float2(dx, dy);
 }

@@ -135,6 +135,7 @@ struct Buffers {
     float *mass;
     const uint32_t *csr_off;  // n + 1, padded-row offsets (multiples of 4)
     const int4 *csr_col4;     // neighbour ids in fours
+    const float4 *csr_w4;     // w^delta beside each id (null: unweighted, w^delta = 1)
     const uint32_t *ref_of;   // internal id -> reference id
     // sort
     uint64_t *keys[2];

@@ -563,21 +563,38 @@ struct Gather {
     __device__ __forceinline__ float2 operator()(int c) const { return __ldg(&pos[c]); }
 };
 
-template <bool LINLOG>
-__device__ __forceinline__ void add_four(const int4 c, const float2 p, const Gather &g,
-                                         float &ax, float &ay) {
-    const float2 q0 = pull<LINLOG>(g(c.x), p), q1 = pull<LINLOG>(g(c.y), p);
-    const float2 q2 = pull<LINLOG>(g(c.z), p), q3 = pull<LINLOG>(g(c.w), p);
+// Four neighbours of one CSR chunk.  WEIGHTED multiplies each pull by the
+// edge's w^delta (edge weight influence, `delta` of src/RPForceAtlas2.hpp:49:
+// f_a = w^delta d); a padding entry's pull is zero whatever its weight.  The
+// products are rounded on their own, so a weight of 1 leaves the sums bit for
+// bit those of the unweighted pass.
+template <bool LINLOG, bool WEIGHTED>
+__device__ __forceinline__ void add_four(const int4 c, const float4 w, const float2 p,
+                                         const Gather &g, float &ax, float &ay) {
+    float2 q0 = pull<LINLOG>(g(c.x), p), q1 = pull<LINLOG>(g(c.y), p);
+    float2 q2 = pull<LINLOG>(g(c.z), p), q3 = pull<LINLOG>(g(c.w), p);
+    if (WEIGHTED) {
+        q0 = make_float2(__fmul_rn(q0.x, w.x), __fmul_rn(q0.y, w.x));
+        q1 = make_float2(__fmul_rn(q1.x, w.y), __fmul_rn(q1.y, w.y));
+        q2 = make_float2(__fmul_rn(q2.x, w.z), __fmul_rn(q2.y, w.z));
+        q3 = make_float2(__fmul_rn(q3.x, w.w), __fmul_rn(q3.y, w.w));
+    }
     ax += q0.x + q1.x + (q2.x + q3.x);
     ay += q0.y + q1.y + (q2.y + q3.y);
 }
 
+template <bool WEIGHTED>
+__device__ __forceinline__ float4 chunk_weights(const float4 *__restrict w4, uint32_t q) {
+    return WEIGHTED ? __ldcs(&w4[q]) : make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+}
+
 // Rows of at most LANES int4 chunks (LANES <= 16): one chunk per lane.
-template <int LANES, bool LINLOG>
+template <int LANES, bool LINLOG, bool WEIGHTED>
 __device__ __forceinline__ void attract_short_rows(int row0, int row_end, const Gather &g,
                                                    const float *__restrict mass,
                                                    const uint32_t *__restrict off,
                                                    const int4 *__restrict col4,
+                                                   const float4 *__restrict w4,
                                                    float2 *__restrict fag, const Params &prm,
                                                    int lane) {
     constexpr int R = 32 / LANES;  // rows per warp and batch
@@ -585,6 +602,7 @@ __device__ __forceinline__ void attract_short_rows(int row0, int row_end, const 
     int row[kAttractBatch];
     bool has[kAttractBatch];
     int4 c[kAttractBatch];
+    float4 w[kAttractBatch];
     float2 p[kAttractBatch];
 #pragma unroll
     for (int u = 0; u < kAttractBatch; ++u) {
@@ -594,12 +612,13 @@ __device__ __forceinline__ void attract_short_rows(int row0, int row_end, const 
         const uint32_t e = valid ? off[row[u] + 1] >> 2 : 0u;
         has[u] = q < e;
         c[u] = has[u] ? __ldcs(&col4[q]) : make_int4(0, 0, 0, 0);
+        w[u] = has[u] ? chunk_weights<WEIGHTED>(w4, q) : make_float4(1.0f, 1.0f, 1.0f, 1.0f);
         p[u] = valid ? g.pos[row[u]] : make_float2(0.0f, 0.0f);
     }
 #pragma unroll
     for (int u = 0; u < kAttractBatch; ++u) {
         float ax = 0.0f, ay = 0.0f;
-        if (has[u]) add_four<LINLOG>(c[u], p[u], g, ax, ay);
+        if (has[u]) add_four<LINLOG, WEIGHTED>(c[u], w[u], p[u], g, ax, ay);
 #pragma unroll
         for (int o = LANES / 2; o > 0; o >>= 1) {
             ax += __shfl_xor_sync(kFull, ax, o);
@@ -612,32 +631,38 @@ __device__ __forceinline__ void attract_short_rows(int row0, int row_end, const 
 
 // Partial attraction of one row over chunks [b + first, e) with stride
 // STRIDE, four chunks in flight per lane.
-template <int STRIDE, bool LINLOG>
+template <int STRIDE, bool LINLOG, bool WEIGHTED>
 __device__ __forceinline__ void attract_long_row(uint32_t b, uint32_t e, int first, float2 p,
                                                  const Gather &g,
-                                                 const int4 *__restrict col4, float &ax,
+                                                 const int4 *__restrict col4,
+                                                 const float4 *__restrict w4, float &ax,
                                                  float &ay) {
     uint32_t q = b + first;
     for (; q + 3 * STRIDE < e; q += 4 * STRIDE) {
         const int4 c0 = __ldcs(&col4[q]), c1 = __ldcs(&col4[q + STRIDE]);
         const int4 c2 = __ldcs(&col4[q + 2 * STRIDE]), c3 = __ldcs(&col4[q + 3 * STRIDE]);
-        add_four<LINLOG>(c0, p, g, ax, ay);
-        add_four<LINLOG>(c1, p, g, ax, ay);
-        add_four<LINLOG>(c2, p, g, ax, ay);
-        add_four<LINLOG>(c3, p, g, ax, ay);
+        const float4 w0 = chunk_weights<WEIGHTED>(w4, q);
+        const float4 w1 = chunk_weights<WEIGHTED>(w4, q + STRIDE);
+        const float4 w2 = chunk_weights<WEIGHTED>(w4, q + 2 * STRIDE);
+        const float4 w3 = chunk_weights<WEIGHTED>(w4, q + 3 * STRIDE);
+        add_four<LINLOG, WEIGHTED>(c0, w0, p, g, ax, ay);
+        add_four<LINLOG, WEIGHTED>(c1, w1, p, g, ax, ay);
+        add_four<LINLOG, WEIGHTED>(c2, w2, p, g, ax, ay);
+        add_four<LINLOG, WEIGHTED>(c3, w3, p, g, ax, ay);
     }
-    for (; q < e; q += STRIDE) add_four<LINLOG>(__ldcs(&col4[q]), p, g, ax, ay);
+    for (; q < e; q += STRIDE)
+        add_four<LINLOG, WEIGHTED>(__ldcs(&col4[q]), chunk_weights<WEIGHTED>(w4, q), p, g, ax,
+                                   ay);
 }
 
 // The attraction pass: one block per work block of the plan (a row for the
 // block-per-row bucket, 8 rows for the warp-per-row bucket, batches of short
 // rows).
-template <bool LINLOG>
-__global__ void __launch_bounds__(256, LINLOG ? 4 : 8) k_attract(AttractPlan plan, const float2 *__restrict pos,
-                                                 const float *__restrict mass,
-                                                 const uint32_t *__restrict off,
-                                                 const int4 *__restrict col4,
-                                                 float2 *__restrict fag, Params prm) {
+template <bool LINLOG, bool WEIGHTED>
+__global__ void __launch_bounds__(256, (LINLOG || WEIGHTED) ? 4 : 8) k_attract(
+    AttractPlan plan, const float2 *__restrict pos, const float *__restrict mass,
+    const uint32_t *__restrict off, const int4 *__restrict col4, const float4 *__restrict w4,
+    float2 *__restrict fag, Params prm) {
     __shared__ float2 s_red[256 / kWarp];
     const Gather g{pos};
     int bi = 0;
@@ -652,8 +677,8 @@ __global__ void __launch_bounds__(256, LINLOG ? 4 : 8) k_attract(AttractPlan pla
         const int row = bk.row_begin + blk;
         const float2 p = g.pos[row];
         float ax = 0.0f, ay = 0.0f;
-        attract_long_row<256, LINLOG>(off[row] >> 2, off[row + 1] >> 2, threadIdx.x, p, g, col4,
-                                      ax, ay);
+        attract_long_row<256, LINLOG, WEIGHTED>(off[row] >> 2, off[row + 1] >> 2, threadIdx.x, p,
+                                                g, col4, w4, ax, ay);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             ax += __shfl_xor_sync(kFull, ax, o);
@@ -678,7 +703,8 @@ __global__ void __launch_bounds__(256, LINLOG ? 4 : 8) k_attract(AttractPlan pla
         if (row >= bk.row_end) return;
         const float2 p = g.pos[row];
         float ax = 0.0f, ay = 0.0f;
-        attract_long_row<32, LINLOG>(off[row] >> 2, off[row + 1] >> 2, lane, p, g, col4, ax, ay);
+        attract_long_row<32, LINLOG, WEIGHTED>(off[row] >> 2, off[row + 1] >> 2, lane, p, g, col4,
+                                               w4, ax, ay);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             ax += __shfl_xor_sync(kFull, ax, o);
@@ -690,11 +716,14 @@ __global__ void __launch_bounds__(256, LINLOG ? 4 : 8) k_attract(AttractPlan pla
     // short rows: kAttractBatch groups of 32/lanes rows per warp
     const int row0 = bk.row_begin + (blk * (256 / kWarp) + wid) * kAttractBatch * (32 / bk.lanes);
     switch (bk.lanes) {
-        case 16: attract_short_rows<16, LINLOG>(row0, bk.row_end, g, mass, off, col4, fag, prm, lane); break;
-        case 8: attract_short_rows<8, LINLOG>(row0, bk.row_end, g, mass, off, col4, fag, prm, lane); break;
-        case 4: attract_short_rows<4, LINLOG>(row0, bk.row_end, g, mass, off, col4, fag, prm, lane); break;
-        case 2: attract_short_rows<2, LINLOG>(row0, bk.row_end, g, mass, off, col4, fag, prm, lane); break;
-        default: attract_short_rows<1, LINLOG>(row0, bk.row_end, g, mass, off, col4, fag, prm, lane); break;
+#define FA2_SHORT_ROWS(L) \
+    attract_short_rows<L, LINLOG, WEIGHTED>(row0, bk.row_end, g, mass, off, col4, w4, fag, prm, lane)
+        case 16: FA2_SHORT_ROWS(16); break;
+        case 8: FA2_SHORT_ROWS(8); break;
+        case 4: FA2_SHORT_ROWS(4); break;
+        case 2: FA2_SHORT_ROWS(2); break;
+        default: FA2_SHORT_ROWS(1); break;
+#undef FA2_SHORT_ROWS
     }
 }
 
@@ -780,12 +809,15 @@ void launch_count_interactions(const Buffers &b, const Params &p, int nblocks, c
 
 void launch_attract(const Buffers &b, const Params &p, const AttractPlan &plan, cudaStream_t s) {
     if (plan.nblocks == 0) return;
-    if (p.linlog)
-        k_attract<true><<<plan.nblocks, 256, 0, s>>>(plan, b.pos, b.mass, b.csr_off, b.csr_col4,
-                                                     b.fag, p);
+    const float4 *w4 = b.csr_w4;
+    auto go = [&](auto kernel) {
+        kernel<<<plan.nblocks, 256, 0, s>>>(plan, b.pos, b.mass, b.csr_off, b.csr_col4, w4, b.fag,
+                                            p);
+    };
+    if (w4)
+        p.linlog ? go(k_attract<true, true>) : go(k_attract<false, true>);
     else
-        k_attract<false><<<plan.nblocks, 256, 0, s>>>(plan, b.pos, b.mass, b.csr_off, b.csr_col4,
-                                                      b.fag, p);
+        p.linlog ? go(k_attract<true, false>) : go(k_attract<false, false>);
 }
 
 void launch_scatter_xy(int n, const uint32_t *ref_of, const float2 *src_ref, float2 *dst_int,

@@ -69,6 +69,7 @@ namespace RPGraph
         g.num_edges = sources.size();
         g.sources = sources.data();
         g.targets = targets.data();
+        g.weights = nullptr;  // UGraph has no edge weights
         fa2_params p;
         fa2_default_params(&p);
         // The reference's GPU step is Barnes-Hut whatever use_barneshut says
@@ -81,6 +82,7 @@ namespace RPGraph
         p.epssq = epssq;
         p.jitter_tolerance = jitter_tolerance;
         p.k_s_max = k_s_max;
+        p.delta = delta;
         int status = FA2_OK;
         ctx = fa2_create(&g, &p, &status);
         if (status == FA2_ERR_NO_DEVICE) {

@@ -44,12 +44,18 @@ typedef struct fa2_ctx fa2_ctx;
 
 /* An undirected graph: each edge once, no self-loops, ids < num_nodes.
  * Replaces the graph half of the CUDAForceAtlas2 constructor
- * (src/RPGPUForceAtlas2.cu:51-84), which reads UGraph::neighbors_with_geq_id. */
+ * (src/RPGPUForceAtlas2.cu:51-84), which reads UGraph::neighbors_with_geq_id.
+ * weights (may be NULL) gives each edge a weight w > 0, in the order of
+ * sources/targets; with fa2_params.delta != 0 an edge attracts with
+ * w^delta times the unweighted force.  UGraph has no weights and the
+ * reference's GPU path no edge weight influence (ForceAtlas2::delta,
+ * src/RPForceAtlas2.hpp:49, is 0 and unread), so the drop-in passes NULL. */
 typedef struct {
     uint32_t num_nodes;
     uint64_t num_edges;
     const uint32_t *sources;
     const uint32_t *targets;
+    const float *weights;
 } fa2_graph_desc;
 
 /* The ForceAtlas2 parameters of src/RPForceAtlas2.cpp:28-55. */
@@ -72,6 +78,13 @@ typedef struct {
                                  of mass, as in the reference (src/RPBHKernels.cu:661-668);
                                  2: each accepted cell also adds its quadrupole term (no
                                  reference counterpart; see fa2_set_approximation) */
+    float delta;              /* edge weight influence (ForceAtlas2::delta,
+                                 src/RPForceAtlas2.hpp:49; 0 by default, :49 of
+                                 src/RPForceAtlas2.cpp): the attraction of an edge of
+                                 weight w is w^delta times the unweighted one, linear or
+                                 linear-log.  Used only with fa2_graph_desc.weights; 0
+                                 ignores the weights.  No counterpart on the reference's
+                                 GPU path. */
 } fa2_params;
 
 /* Fills the reference defaults (weak gravity, gravity 1, scale 1). */
@@ -227,7 +240,8 @@ typedef struct fa2_batch fa2_batch;
 
 /* num_graphs graphs, each as fa2_create takes one (ids local to the graph);
  * the parameters apply to every graph.  Positions start at zero. */
-/* params->multipole must be 1 (FA2_ERR_UNSUPPORTED otherwise). */
+/* params->multipole must be 1, and edge weights need params->delta == 0
+ * (FA2_ERR_UNSUPPORTED otherwise). */
 fa2_batch *fa2_batch_create(uint32_t num_graphs, const fa2_graph_desc *graphs,
                             const fa2_params *params, int *status);
 void fa2_batch_destroy(fa2_batch *batch);

@@ -211,6 +211,33 @@ void orc_attraction_linlog(int64_t n_edges, const int32_t *sources, const int32_
     }
 }
 
+void orc_attraction_weighted(int64_t n_edges, const int32_t *sources, const int32_t *targets,
+                             const float *wd, int32_t linlog, const float *xy, float *fx,
+                             float *fy) {
+    for (int64_t e = 0; e < n_edges; ++e) {
+        const int32_t s = sources[e], t = targets[e];
+        float w = 1.0f;
+        if (linlog) {
+            const float ex = xy[2 * s] - xy[2 * t];
+            const float ey = xy[2 * s + 1] - xy[2 * t + 1];
+            const float dist = sqrtf(ex * ex + ey * ey);
+            w = dist == 0.0f ? FLT_MAX : logf(1 + dist) / dist;
+        }
+        float dx = xy[2 * t] - xy[2 * s];
+        float dy = xy[2 * t + 1] - xy[2 * s + 1];
+        if (linlog) {
+            dx = dx * w;
+            dy = dy * w;
+        }
+        dx = dx * wd[e];
+        dy = dy * wd[e];
+        fx[s] += dx;
+        fy[s] += dy;
+        fx[t] += -dx;
+        fy[t] += -dy;
+    }
+}
+
 void orc_speed_init(orc_speed_state *st) {
     st->global_speed = 1.0f;
     st->speed_efficiency = 1.0f;

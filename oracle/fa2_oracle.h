@@ -62,6 +62,17 @@ void orc_attraction_linlog(int64_t n_edges, const int32_t *sources, const int32_
 void orc_attraction(int64_t n_edges, const int32_t *sources, const int32_t *targets,
                     const float *xy, float *fx, float *fy);
 
+/* Edge weight influence (ForceAtlas2::delta, src/RPForceAtlas2.hpp:49): an
+ * edge of weight w attracts with w^delta times the force of orc_attraction
+ * (linlog 0) or orc_attraction_linlog (linlog 1), the rule F_a = w^delta d of
+ * the ForceAtlas2 paper (Jacomy et al., PLoS ONE 9(6), 2014).  wd[e] holds
+ * w^delta of edge e.  The reference declares delta but its UGraph has no
+ * weights, so nothing of the reference runs this; it restates the published
+ * rule in the edge order of the unweighted forms. */
+void orc_attraction_weighted(int64_t n_edges, const int32_t *sources, const int32_t *targets,
+                             const float *wd, int32_t linlog, const float *xy, float *fx,
+                             float *fy);
+
 typedef struct {
     float global_speed;      /* RPFA2Kernels.cu:30, starts at 1 */
     float speed_efficiency;  /* :31, starts at 1 */

@@ -45,6 +45,8 @@ def lib():
         L.orc_gravity.argtypes = [C.c_int32, _f32p, _f32p, C.c_float, C.c_int32, _f32p, _f32p]
         L.orc_attraction.argtypes = [C.c_int64, _i32p, _i32p, _f32p, _f32p, _f32p]
         L.orc_attraction_linlog.argtypes = [C.c_int64, _i32p, _i32p, _f32p, _f32p, _f32p]
+        L.orc_attraction_weighted.argtypes = [C.c_int64, _i32p, _i32p, _f32p, C.c_int32, _f32p,
+                                              _f32p, _f32p]
         L.orc_tree_build.restype = C.c_void_p
         L.orc_tree_build.argtypes = [C.c_int32, _f32p, C.POINTER(C.c_int32)]
         L.orc_tree_free.argtypes = [C.c_void_p]
@@ -113,14 +115,27 @@ def random_positions(n: int, width: float, height: float, seed: int = 1234) -> n
 
 # ---------------------------------------------------------------- pieces --
 
-def gravity_attraction(g: Graph, xy: np.ndarray, k_g: float, strong: bool, linlog: bool = False):
+def edge_weight_powers(weights, delta: float) -> np.ndarray:
+    """w**delta per edge, from float32 weights in double, rounded once to float32."""
+    w = np.ascontiguousarray(weights, np.float32).astype(np.float64)
+    return np.power(w, float(delta)).astype(np.float32)
+
+
+def gravity_attraction(g: Graph, xy: np.ndarray, k_g: float, strong: bool, linlog: bool = False,
+                       weights=None, delta: float = 0.0):
+    """Gravity plus attraction per node; with weights and delta != 0, each edge's
+    attraction times w**delta (orc_attraction_weighted)."""
     n = g.n
     fx = np.zeros(n, np.float32)
     fy = np.zeros(n, np.float32)
     p = np.ascontiguousarray(xy, np.float32).reshape(-1)
     lib().orc_gravity(n, p, g.mass, k_g, int(strong), fx, fy)
-    attract = lib().orc_attraction_linlog if linlog else lib().orc_attraction
-    attract(g.m, g.sources, g.targets, p, fx, fy)
+    if weights is not None and delta != 0.0:
+        wd = edge_weight_powers(weights, delta)
+        lib().orc_attraction_weighted(g.m, g.sources, g.targets, wd, int(linlog), p, fx, fy)
+    else:
+        attract = lib().orc_attraction_linlog if linlog else lib().orc_attraction
+        attract(g.m, g.sources, g.targets, p, fx, fy)
     return np.stack([fx, fy], 1)
 
 
