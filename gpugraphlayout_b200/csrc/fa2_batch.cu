@@ -582,8 +582,14 @@ __device__ void phase_displace(const BatchArgs &A, uint32_t base, uint32_t n, ch
     __syncthreads();
 }
 
+// 2048 threads per SM: 32 registers a thread, which spills about 1.4 KB of
+// the tree and sort phases' state to local memory (L1).  The walk, like the
+// single-graph engine's, needs every warp the SM holds to cover its load
+// latency: on the 4096-graph batch this bound gives 124 batch iterations/s
+// against 107 with 64 registers and 1024 threads per SM (118 with 42
+// registers and 1536 threads).
 template <int T, bool LINLOG>
-__global__ void __launch_bounds__(T, 1024 / T) k_batch(BatchArgs A) {
+__global__ void __launch_bounds__(T, 2048 / T) k_batch(BatchArgs A) {
     __shared__ BatchSmem<T> S;
     char *slot = A.slots + (size_t)blockIdx.x * A.L.bytes;
     float2 *fa = slot_ptr<float2>(slot, A.L.fa);
