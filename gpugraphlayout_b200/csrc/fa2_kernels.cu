@@ -521,7 +521,9 @@ __global__ void __launch_bounds__(256) k_guard_plain(int n, int ns,
     }
 }
 
-__global__ void __launch_bounds__(kDispThreads) k_displace(int n, float2 *__restrict pos,
+// 4 blocks per SM (32 registers): the launch's up to 4 blocks per SM are all
+// resident at once
+__global__ void __launch_bounds__(kDispThreads, 2048 / kDispThreads) k_displace(int n, float2 *__restrict pos,
                                                            const float2 *__restrict f,
                                                            float2 *__restrict fprev,
                                                            float4 *__restrict partial, DevState *st,

@@ -522,7 +522,9 @@ __global__ void __launch_bounds__(kQuadThreads) k_quad_cells(const float4 *__res
 // centre of mass from the prefix sums at its two ends.  Node-parallel, so the
 // body that starts many nested cells (body 0 starts one per level) spreads
 // their searches over many threads.
-__global__ void __launch_bounds__(256) k_emit(int n, const uint64_t *__restrict keys,
+// 8 blocks of 256 per SM (32 registers): the launch's up to 8 blocks per SM
+// are all resident at once
+__global__ void __launch_bounds__(256, 8) k_emit(int n, const uint64_t *__restrict keys,
                                               const uint32_t *__restrict vals,
                                               const int8_t *__restrict lcp,
                                               const uint32_t *__restrict group,
