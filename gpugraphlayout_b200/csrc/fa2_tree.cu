@@ -475,7 +475,8 @@ __device__ __forceinline__ float2 cell_quadrupole(const Moments &hi, const Momen
 // queue and works through it 32 cells at a time, so no lane idles on bodies.
 constexpr int kQuadThreads = 256;
 
-__global__ void __launch_bounds__(kQuadThreads) k_quad_cells(const float4 *__restrict nodes,
+// 4 blocks per SM (64 registers); the launch puts no more than that on an SM
+__global__ void __launch_bounds__(kQuadThreads, 4) k_quad_cells(const float4 *__restrict nodes,
                                                              const uint32_t *__restrict owner,
                                                              const long long *__restrict pm,
                                                              const Moments *__restrict pmom,
@@ -593,7 +594,7 @@ void launch_emit(const Buffers &b, int nsm, cudaStream_t s) {
 }
 
 void launch_quad_cells(const Buffers &b, int nsm, cudaStream_t s) {
-    k_quad_cells<<<grid_for(b.n, kQuadThreads, nsm * 8), kQuadThreads, 0, s>>>(
+    k_quad_cells<<<grid_for(b.n, kQuadThreads, nsm * 4), kQuadThreads, 0, s>>>(
         b.nodes, b.owner, b.pm, b.pmom, b.quad, b.st);
 }
 
