@@ -97,3 +97,9 @@ def test_oracle_weighted_attraction(linlog):
         ref = _float64_restatement(g, xy, wd, linlog)
         assert np.sqrt(np.mean((got - ref) ** 2) / np.mean(ref ** 2)) < 1e-6, delta
     assert np.array_equal(O.gravity_attraction(g, xy, 0.0, True, linlog, w, 0.0), plain)
+
+
+def test_engine_wants_one_weight_per_edge():
+    from gpugraphlayout_b200 import Engine
+    with pytest.raises(ValueError):
+        Engine(3, [0, 1], [1, 2], weights=[1.0], delta=1.0)
