@@ -167,9 +167,15 @@ int run(const float *d_xy, const float *d_mass, uint32_t n, const fa2_params *pr
     // coincidence flags, interaction count); the gravity + attraction term
     // the traversal adds to the repulsion (zero here, so d_force receives the
     // repulsion alone).  The reference ids are the caller's indices.
-    cudaMemsetAsync(b.ctr, 0, zero_bytes, s);
-    cudaMemsetAsync(b.st, 0, sizeof(DevState), s);
-    cudaMemsetAsync(b.fag, 0, (size_t)n * sizeof(float2), s);
+    cudaError_t e = cudaMemsetAsync(b.ctr, 0, zero_bytes, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b.st, 0, sizeof(DevState), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b.fag, 0, (size_t)n * sizeof(float2), s);
+    if (e != cudaSuccess) return status_of(e);
+    // A launch error is read from the runtime's last-error slot.  An error
+    // the caller left there before this call is not ours to report or to
+    // clear, so launch errors are taken from the slot only if it was empty on
+    // entry (otherwise a failed launch still shows in the stream wait below).
+    const bool slot_was_clear = cudaPeekAtLastError() == cudaSuccess;
     k_prepare<<<(n + 255) / 256, 256, 0, s>>>(n, d_mass, const_cast<uint32_t *>(b.ref_of), b.st);
     launch_bbox(b, d.nsm * 2, s);
     launch_keys(b, d.nsm, s);
@@ -177,8 +183,10 @@ int run(const float *d_xy, const float *d_mass, uint32_t n, const fa2_params *pr
     launch_tree_count(b, false, s);
     launch_emit(b, d.nsm, s);
     launch_traverse(b, kp, d.trav_blocks, s);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return status_of(e);
+    if (slot_was_clear) {
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return status_of(e);
+    }
     int flags[2] = {0, 0};  // DevState::poison, DevState::err (adjacent)
     static_assert(offsetof(DevState, err) == offsetof(DevState, poison) + sizeof(int),
                   "poison and err are read with one copy");
@@ -200,7 +208,8 @@ extern "C" int fa2_repulsion_noalloc(const float *d_xy, const float *d_mass, uin
     using namespace fa2;
     if (!prm) return FA2_ERR_INVALID_ARGUMENT;
     if (n > kMaxBodies) return FA2_ERR_TOO_LARGE;
-    if (!prm->use_barneshut || prm->multipole > 1) return FA2_ERR_UNSUPPORTED;
+    if (prm->multipole < 1) return FA2_ERR_INVALID_ARGUMENT;
+    if (!prm->use_barneshut || prm->multipole != 1) return FA2_ERR_UNSUPPORTED;
     if (!(prm->theta > 0.0f)) return FA2_ERR_INVALID_ARGUMENT;
     if (n == 0) return FA2_OK;
     if (!d_xy || !d_mass || !d_force || ((uintptr_t)d_xy & 7) || ((uintptr_t)d_force & 7) ||

@@ -314,7 +314,8 @@ int fa2_batch_get_speed(fa2_batch *batch, float *global_speed, float *speed_effi
  *    any first CUDA call, may create the device's context).  Make it before
  *    any stream capture.
  *  - The work is enqueued on `stream` (a cudaStream_t; NULL is the default
- *    stream) and the call waits for that stream before it returns, then
+ *    stream); the call then copies two device flags to host memory and
+ *    waits for that stream (cudaStreamSynchronize) before it returns, and
  *    reports: coincident bodies, a NaN or infinite position, or a mass that
  *    is not a whole number in [0, 2^24) -> FA2_ERR_INVALID_ARGUMENT (fa2_step moves coincident bodies
  *    apart, and its masses are degree + 1; this call does neither), a
@@ -324,7 +325,11 @@ int fa2_batch_get_speed(fa2_batch *batch, float *global_speed, float *speed_effi
  *    wrong forces.  Serialise them.
  *  - d_xy and d_force 8-byte aligned, d_mass 4-byte aligned; d_force must not
  *    overlap d_xy or d_mass.
- *  - prm->multipole must be 1 (FA2_ERR_UNSUPPORTED otherwise). */
+ *  - prm->multipole must be 1: 2 (the quadrupole walk) gives
+ *    FA2_ERR_UNSUPPORTED, a value below 1 FA2_ERR_INVALID_ARGUMENT.
+ *  - Launch errors are read from the CUDA runtime's last-error slot only when
+ *    that slot was empty on entry: an error the caller left there is neither
+ *    reported as this call's nor cleared. */
 int fa2_repulsion_noalloc(const float *d_xy, const float *d_mass, uint32_t n,
                           const fa2_params *prm, void *stream, float *d_force);
 

@@ -6,9 +6,15 @@ fa2_step's forces come back as the total and the gravity + attraction part;
 their difference is the repulsion, rounded once more by the subtraction, so
 the comparison is a relative RMSE of at most 1e-5 (the same tree, cell tests
 and walk order give the same terms).  Two calls in a row, on different
-positions, check that each call starts from cleared scratch.  This file runs
-last in the suite and also passes on its own in a fresh process, where its
-first call does the per-device set-up.
+positions, check that each call starts from cleared scratch.  Its name sorts
+last, so pytest collects it after every other test file; it also passes on
+its own in a fresh process, where its first call does the per-device set-up.
+
+The entry point exists for callers that may not allocate device memory at the
+call: code with a fixed device-memory budget, or a library running inside a
+host framework whose caching allocator it must not disturb.  After the first
+call on a device, neither torch's allocator nor the device's free memory
+(cudaMemGetInfo) may change across calls.
 """
 import ctypes as C
 
@@ -115,3 +121,46 @@ def test_noalloc_refuses_non_finite_positions():
     xy = O.random_positions(n, 100, 100, 3)
     assert _noalloc(torch.from_numpy(xy).cuda(), mass, out, prm) == 0
     assert bool(torch.isfinite(out).all())
+
+
+def test_noalloc_leaves_device_memory_untouched_after_the_first_call():
+    """Calls after the first neither allocate through torch's caching
+    allocator nor change the device's free memory (cudaMemGetInfo)."""
+    import torch
+    from gpugraphlayout_b200 import synth
+    from oracle import oracle as O
+    s, t = synth.ba_edges(4000, 3, seed=21)
+    g = O.Graph(s, t)
+    xy = torch.from_numpy(O.random_positions(g.n, 2000, 2000, 21)).cuda()
+    mass = torch.from_numpy(g.mass).cuda()
+    out = torch.empty((g.n, 2), dtype=torch.float32, device="cuda")
+    prm = _params(10.0)
+    assert _noalloc(xy, mass, out, prm) == 0  # set-up and first kernel loads
+    torch.cuda.synchronize()
+    first = out.clone()
+    alloc0 = torch.cuda.memory_allocated()
+    reserved0 = torch.cuda.memory_reserved()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        assert _noalloc(xy, mass, out, prm) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert torch.cuda.memory_allocated() == alloc0
+    assert torch.cuda.memory_reserved() == reserved0
+    assert free1 == free0
+    assert torch.equal(out, first)  # and every call gives the same bits
+
+
+def test_noalloc_refuses_other_multipole_orders():
+    """multipole 2 (the quadrupole walk) is not offered here; 0 or less is
+    not a multipole order at all."""
+    import torch
+    n = 100
+    xy = torch.zeros((n, 2), dtype=torch.float32, device="cuda")
+    mass = torch.ones(n, dtype=torch.float32, device="cuda")
+    out = torch.full((n, 2), 7.0, dtype=torch.float32, device="cuda")
+    for mp, status in ((2, 7), (0, 1), (-1, 1)):  # FA2_ERR_UNSUPPORTED, _INVALID_ARGUMENT
+        prm = _params(1.0)
+        prm.multipole = mp
+        assert _noalloc(xy, mass, out, prm) == status, mp
+    assert bool((out == 7.0).all())  # nothing ran
