@@ -21,10 +21,10 @@ import ctypes as C
 
 import numpy as np
 
-from ._native import Fa2Error, GraphDesc, Params, Stats, check, lib
+from ._native import Fa2Error, GraphDesc, Mlp, Params, Stats, check, lib
 
 __all__ = ["Engine", "BatchEngine", "UGraph", "GraphLayout", "CUDAForceAtlas2", "Fa2Error", "kernel_names",
-           "random_positions", "render_rgb", "write_png"]
+           "random_positions", "render_rgb", "write_png", "FarFieldMLP", "LearnSet"]
 
 
 def _ptr(a: np.ndarray):
@@ -164,6 +164,12 @@ class Engine:
                                            C.byref(fb)), "fa2_get_accuracy_guard")
         return {"err_current": ec.value, "err_plain": ep.value, "checks": ck.value,
                 "fallbacks": fb.value}
+
+    def set_learned_correction(self, mlp: "FarFieldMLP | None") -> None:
+        """The learned far-field correction on top of the walk
+        set_approximation selected, from the next step on; None turns it off."""
+        check(lib().fa2_set_learned_correction(self._ctx, None if mlp is None else C.byref(mlp.c)),
+              "fa2_set_learned_correction")
 
     def set_overlap(self, enable: bool) -> None:
         """Attraction beside the tree build (default) or alone before it."""
@@ -431,6 +437,110 @@ def write_png(rgb, path: str) -> None:
     a = np.ascontiguousarray(rgb, np.uint8)
     check(lib().fa2_png_encode(_ptr(a), a.shape[1], a.shape[0], str(path).encode()),
           f"write {path}")
+
+
+class FarFieldMLP:
+    """fa2_mlp: the learned far-field correction's 12 -> 64 -> 64 -> 2 MLP
+    (FP32 parameters; inference runs in BF16 with FP32 accumulation).  The
+    arrays are views of the C struct, [out][in] like torch's nn.Linear."""
+
+    NAMES = ("w1", "b1", "w2", "b2", "w3", "b3")
+    SHAPES = {"w1": (64, 12), "b1": (64,), "w2": (64, 64), "b2": (64,), "w3": (2, 64), "b3": (2,)}
+
+    def __init__(self, seed: int | None = 0):
+        """nn.Linear's default initialisation from `seed`; None leaves zeros."""
+        self.c = Mlp()
+        if seed is not None:
+            lib().fa2_mlp_init(C.byref(self.c), int(seed))
+
+    def __getitem__(self, name: str) -> np.ndarray:
+        return np.ctypeslib.as_array(getattr(self.c, name)).reshape(self.SHAPES[name])
+
+    def __setitem__(self, name: str, value) -> None:
+        self[name][...] = np.asarray(value, np.float32).reshape(self.SHAPES[name])
+
+    def vector(self) -> np.ndarray:
+        """All parameters as one float32 vector, in the struct's order."""
+        return np.concatenate([self[n].ravel() for n in self.NAMES]).copy()
+
+    @classmethod
+    def from_vector(cls, v) -> "FarFieldMLP":
+        m = cls(seed=None)
+        v = np.asarray(v, np.float32).ravel()
+        at = 0
+        for n in cls.NAMES:
+            k = int(np.prod(cls.SHAPES[n]))
+            m[n] = v[at:at + k]
+            at += k
+        return m
+
+    def forward(self, features, device: int = 0) -> np.ndarray:
+        """The tensor-core inference kernel on (n, 12) features: (n, 2)."""
+        x = np.ascontiguousarray(features, np.float32).reshape(-1, 12)
+        out = np.zeros((len(x), 2), np.float32)
+        check(lib().fa2_mlp_forward(int(device), C.byref(self.c), _ptr(x), len(x), _ptr(out)),
+              "fa2_mlp_forward")
+        return out
+
+    def train_step(self, m: "FarFieldMLP", v: "FarFieldMLP", step: int, lr: float, features,
+                   targets, weights, device: int = 0) -> float:
+        """One Adam step of the training kernels on the given samples (in
+        place, with Adam's moments m and v); returns the loss before it."""
+        x = np.ascontiguousarray(features, np.float32).reshape(-1, 12)
+        t = np.ascontiguousarray(targets, np.float32).reshape(-1, 2)
+        w = np.ascontiguousarray(weights, np.float32).ravel()
+        loss = C.c_float(0.0)
+        check(lib().fa2_mlp_train_step(int(device), C.byref(self.c), C.byref(m.c), C.byref(v.c),
+                                       int(step), float(lr), _ptr(x), _ptr(t), _ptr(w), len(x),
+                                       C.byref(loss)), "fa2_mlp_train_step")
+        return loss.value
+
+
+class LearnSet:
+    """fa2_learn_set: training samples of the learned correction in device
+    memory, collected from an Engine's layouts (FP64 exact targets)."""
+
+    def __init__(self, capacity: int, device: int = 0):
+        st = C.c_int(0)
+        self._h = lib().fa2_learn_set_create(int(device), int(capacity), C.byref(st))
+        if not self._h:
+            raise Fa2Error(st.value, "fa2_learn_set_create")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fa2_learn_set_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __len__(self) -> int:
+        return int(lib().fa2_learn_set_size(self._h))
+
+    def collect(self, engine: Engine, theta: float, multipole: int = 1) -> int:
+        """Samples of the engine's current positions, walked at theta."""
+        added = C.c_int64(0)
+        check(lib().fa2_learn_collect(self._h, engine._ctx, float(theta), int(multipole),
+                                      C.byref(added)), "fa2_learn_collect")
+        return added.value
+
+    def read(self, first: int = 0, count: int | None = None):
+        """(features (k, 12), targets (k, 2), weights (k,)) of samples [first, first + k)."""
+        count = len(self) - first if count is None else count
+        f = np.zeros((count, 12), np.float32)
+        t = np.zeros((count, 2), np.float32)
+        w = np.zeros(count, np.float32)
+        check(lib().fa2_learn_set_read(self._h, int(first), int(count), _ptr(f), _ptr(t),
+                                       _ptr(w)), "fa2_learn_set_read")
+        return f, t, w
+
+    def fit(self, mlp: FarFieldMLP, steps: int, batch: int = 4096, lr: float = 2e-3,
+            seed: int = 0) -> float:
+        """Trains mlp in place with the training kernels; returns the last loss."""
+        loss = C.c_float(0.0)
+        check(lib().fa2_learn_fit(self._h, C.byref(mlp.c), int(steps), int(batch), float(lr),
+                                  int(seed), C.byref(loss)), "fa2_learn_fit")
+        return loss.value
 
 
 class CUDAForceAtlas2:

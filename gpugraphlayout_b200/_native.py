@@ -28,6 +28,9 @@ EXPORTS = (
     "fa2_ugraph_num_edges", "fa2_ugraph_node_map_r", "fa2_ugraph_degrees",
     "fa2_ugraph_edges", "fa2_random_positions", "fa2_write_layout",
     "fa2_status_string", "fa2_version",
+    "fa2_mlp_init", "fa2_set_learned_correction", "fa2_mlp_forward", "fa2_mlp_train_step",
+    "fa2_learn_set_create", "fa2_learn_set_destroy", "fa2_learn_set_size", "fa2_learn_collect",
+    "fa2_learn_set_read", "fa2_learn_fit",
 )
 
 FA2_OK = 0
@@ -62,6 +65,16 @@ class Stats(C.Structure):
                 ("root_x", C.c_float), ("root_y", C.c_float),
                 ("interactions", C.c_uint64), ("visits", C.c_uint64),
                 ("sort_passes", C.c_int32)]
+
+
+MLP_IN, MLP_HIDDEN, MLP_OUT = 12, 64, 2  # include/fa2b200.h
+
+
+class Mlp(C.Structure):
+    """fa2_mlp: the learned correction's FP32 parameters, [out][in] weights."""
+    _fields_ = [("w1", C.c_float * (MLP_HIDDEN * MLP_IN)), ("b1", C.c_float * MLP_HIDDEN),
+                ("w2", C.c_float * (MLP_HIDDEN * MLP_HIDDEN)), ("b2", C.c_float * MLP_HIDDEN),
+                ("w3", C.c_float * (MLP_OUT * MLP_HIDDEN)), ("b3", C.c_float * MLP_OUT)]
 
 
 class Fa2Error(RuntimeError):
@@ -150,6 +163,20 @@ def lib():
     L.fa2_status_string.restype = C.c_char_p
     L.fa2_status_string.argtypes = [C.c_int]
     L.fa2_version.restype = C.c_char_p
+    mp = C.POINTER(Mlp)
+    L.fa2_mlp_init.argtypes = [mp, C.c_uint32]
+    L.fa2_set_learned_correction.argtypes = [vp, mp]
+    L.fa2_mlp_forward.argtypes = [C.c_int32, mp, vp, C.c_int64, vp]
+    L.fa2_mlp_train_step.argtypes = [C.c_int32, mp, mp, mp, C.c_int32, C.c_float, vp, vp, vp,
+                                     C.c_int32, f32p]
+    L.fa2_learn_set_create.restype = vp
+    L.fa2_learn_set_create.argtypes = [C.c_int32, C.c_int64, ip]
+    L.fa2_learn_set_destroy.argtypes = [vp]
+    L.fa2_learn_set_size.restype = C.c_int64
+    L.fa2_learn_set_size.argtypes = [vp]
+    L.fa2_learn_collect.argtypes = [vp, vp, C.c_float, C.c_int32, C.POINTER(C.c_int64)]
+    L.fa2_learn_set_read.argtypes = [vp, C.c_int64, C.c_int64, vp, vp, vp]
+    L.fa2_learn_fit.argtypes = [vp, mp, C.c_int32, C.c_int32, C.c_float, C.c_uint32, f32p]
     _lib = L
     return L
 

@@ -16,20 +16,22 @@
 #include <cfloat>
 #include <cmath>
 #include <numeric>
+#include <random>
 #include <vector>
 
 #include "../../include/fa2b200.h"
 #include "fa2_internal.cuh"
+#include "fa2_learn.cuh"
 
 using namespace fa2;
 
 namespace {
 
-constexpr int kNumSlots = 9;
+constexpr int kNumSlots = 10;
 const char *const kSlotNames[kNumSlots] = {"attract",  "keys",     "sort",    "tree_count",
                                            "emit",     "traverse", "displace", "moments",
-                                           "quadrupole"};
-enum Slot { S_ATTRACT, S_KEYS, S_SORT, S_COUNT, S_EMIT, S_TRAV, S_DISP, S_MOM, S_QUAD };
+                                           "quadrupole", "learn"};
+enum Slot { S_ATTRACT, S_KEYS, S_SORT, S_COUNT, S_EMIT, S_TRAV, S_DISP, S_MOM, S_QUAD, S_LEARN };
 
 // The last CUDA error a call of this thread met, with the source line that saw
 // it (fa2_last_cuda_error).
@@ -74,6 +76,10 @@ struct fa2_ctx {
     double guard_err_cur = 0.0, guard_err_plain = 0.0;
     double2 *guard_exact = nullptr;
     float2 *guard_plain = nullptr, *guard_cur = nullptr;
+    // learned correction (fa2_set_learned_correction)
+    bool learn_on = false;
+    LearnBuffers lb{};
+    MlpDevice *d_mlp = nullptr;
 };
 
 namespace {
@@ -122,6 +128,25 @@ int ensure_quad_buffers(fa2_ctx *c) {
         (!b.mom_m && (s = dalloc(c, &b.mom_m, (size_t)b.n))) ||
         (!b.mom_q && (s = dalloc(c, &b.mom_q, (size_t)b.n))))
         return s;
+    return FA2_OK;
+}
+
+// Buffers of the learned correction, allocated when it is first used: the
+// pair list (up to 32 pairs per body), the groups' geometry and corrections,
+// the sorted bodies' repulsion and the MLP's weights.
+int ensure_learn_buffers(fa2_ctx *c) {
+    LearnBuffers &lb = c->lb;
+    const size_t groups = ((size_t)c->n + 31) / 32;
+    const uint64_t cap = std::min<uint64_t>(32ull * c->n + 4096, 0xFFFFFFFFull);
+    int s = FA2_OK;
+    if ((!lb.pairs && (s = dalloc(c, &lb.pairs, (size_t)cap))) ||
+        (!lb.ggeo && (s = dalloc(c, &lb.ggeo, 2 * groups))) ||
+        (!lb.rep && (s = dalloc(c, &lb.rep, (size_t)c->n))) ||
+        (!lb.corr && (s = dalloc(c, &lb.corr, groups))) ||
+        (!c->d_mlp && (s = dalloc(c, &c->d_mlp, 1))))
+        return s;
+    lb.pair_cap = (uint32_t)cap;
+    lb.mlp = c->d_mlp;
     return FA2_OK;
 }
 
@@ -246,9 +271,13 @@ void enqueue_iteration(fa2_ctx *c, bool full, bool perturb_first, bool timed) {
         if (timed)
             cudaEventRecordWithFlags(c->slot_events[slot * 2 + end], s, cudaEventRecordExternal);
     };
-    const bool quad = c->kp.multipole >= 2;
+    const bool learn = c->learn_on;
+    // the moment scan and per-cell second moments: the quadrupole walk and
+    // the learned correction's features use them
+    const bool quad = c->kp.multipole >= 2 || learn;
     const bool side = full && c->overlap;  // stream B carries the attraction
     cudaMemsetAsync(c->scratch, 0, c->scratch_bytes, A);
+    if (learn) cudaMemsetAsync(c->lb.corr, 0, ((size_t)c->n + 31) / 32 * sizeof(float2), A);
     if (full && !c->overlap) {
         mark(S_ATTRACT, 0, A);
         launch_attract(b, c->kp, c->plan, A);
@@ -295,8 +324,17 @@ void enqueue_iteration(fa2_ctx *c, bool full, bool perturb_first, bool timed) {
         mark(S_QUAD, 1, A);
     }
     mark(S_TRAV, 0, A);
-    launch_traverse(b, c->kp, c->trav_blocks, A);
+    if (learn)
+        launch_traverse_learn(b, c->kp, c->lb, c->trav_blocks, A);
+    else
+        launch_traverse(b, c->kp, c->trav_blocks, A);
     mark(S_TRAV, 1, A);
+    if (learn) {
+        mark(S_LEARN, 0, A);
+        launch_learn_mlp(b, c->kp, c->lb, c->nsm, A);
+        launch_learn_tail(b, c->kp, c->lb, c->nsm, A);
+        mark(S_LEARN, 1, A);
+    }
     mark(S_DISP, 0, A);
     launch_displace(b, c->nsm, A);
     mark(S_DISP, 1, A);
@@ -334,7 +372,7 @@ int capture(fa2_ctx *c, bool timed, cudaGraphExec_t *out) {
 
 // The guard checks only an approximation other than the reference's.
 bool guard_active(const fa2_ctx *c) {
-    return c->guard_every > 0 && (c->kp.multipole >= 2 || c->kp.itolsq != 1.0f);
+    return c->guard_every > 0 && (c->kp.multipole >= 2 || c->kp.itolsq != 1.0f || c->learn_on);
 }
 
 // One check of the accuracy guard on the last iteration's tree: relative RMSE
@@ -366,9 +404,11 @@ int guard_check(fa2_ctx *c) {
     c->guard_err_plain = std::sqrt(e_plain / norm);
     c->guard_checks += 1;
     if (c->guard_err_cur > c->guard_err_plain) {
-        // back to the reference's walk: theta 1, cells as point masses
+        // back to the reference's walk: theta 1, cells as point masses, no
+        // learned correction
         c->kp.itolsq = 1.0f;
         c->kp.multipole = 1;
+        c->learn_on = false;
         c->prm.theta = 1.0f;
         c->prm.multipole = 1;
         c->guard_fallbacks += 1;
@@ -490,6 +530,144 @@ int run_steps(fa2_ctx *c, int32_t n_iters, bool timed, std::vector<double> *kern
             }
         }
     }
+    return FA2_OK;
+}
+
+
+// ------------------------------------------------ learned correction --
+
+// Round to the nearest BF16 (ties to even), as bits and as a float.
+uint16_t bf16_bits(float x) {
+    uint32_t u;
+    memcpy(&u, &x, 4);
+    if ((u & 0x7F800000u) == 0x7F800000u && (u & 0x007FFFFFu)) return (uint16_t)((u >> 16) | 0x40u);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
+
+float bf16_value(float x) {
+    const uint32_t u = (uint32_t)bf16_bits(x) << 16;
+    float f;
+    memcpy(&f, &u, 4);
+    return f;
+}
+
+bool mlp_is_finite(const fa2_mlp &m) {
+    const float *p = reinterpret_cast<const float *>(&m);
+    for (size_t i = 0; i < sizeof(fa2_mlp) / sizeof(float); ++i)
+        if (!std::isfinite(p[i])) return false;
+    return true;
+}
+
+// The FP32 parameters as the kernels read them (MlpDevice): W1 and W2 in BF16
+// in the tensor cores' operand layout (W1's K padded from 12 to 16 with
+// zeros), W3 as BF16 values in {W3[0][j], W3[1][j]} pairs, biases as given.
+void mlp_to_device(const fa2_mlp &m, MlpDevice &d) {
+    memset(&d, 0, sizeof(d));
+    for (int j = 0; j < kLearnHidden; ++j) {
+        for (int k = 0; k < kLearnInPad; ++k)
+            d.w1[operand_offset(j, k, kLearnInPad / 8) / 2] =
+                k < kLearnIn ? bf16_bits(m.w1[j * kLearnIn + k]) : (uint16_t)0;
+        for (int k = 0; k < kLearnHidden; ++k)
+            d.w2[operand_offset(j, k, kLearnHidden / 8) / 2] = bf16_bits(m.w2[j * kLearnHidden + k]);
+        d.b1[j] = m.b1[j];
+        d.b2[j] = m.b2[j];
+        d.w3[j] = make_float2(bf16_value(m.w3[j]), bf16_value(m.w3[kLearnHidden + j]));
+    }
+    d.b3[0] = m.b3[0];
+    d.b3[1] = m.b3[1];
+}
+
+// nn.Linear's default initialisation: U(-1/sqrt(fan_in), 1/sqrt(fan_in)).
+void mlp_default_init(fa2_mlp *m, uint32_t seed) {
+    std::mt19937 rng(seed);
+    auto fill = [&](float *p, int count, int fan_in) {
+        const float bound = 1.0f / std::sqrt((float)fan_in);
+        std::uniform_real_distribution<float> u(-bound, bound);
+        for (int i = 0; i < count; ++i) p[i] = u(rng);
+    };
+    fill(m->w1, kLearnHidden * kLearnIn, kLearnIn);
+    fill(m->b1, kLearnHidden, kLearnIn);
+    fill(m->w2, kLearnHidden * kLearnHidden, kLearnHidden);
+    fill(m->b2, kLearnHidden, kLearnHidden);
+    fill(m->w3, kLearnOut * kLearnHidden, kLearnHidden);
+    fill(m->b3, kLearnOut, kLearnHidden);
+}
+
+// Makes `device` current after checking it is an sm_100 part.
+int use_device(int device, int *nsm) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+        return FA2_ERR_NO_DEVICE;
+    cudaDeviceProp dp;
+    if (cudaGetDeviceProperties(&dp, device) != cudaSuccess || dp.major < 10)
+        return FA2_ERR_NO_DEVICE;
+    if (cudaSetDevice(device) != cudaSuccess) return FA2_ERR_CUDA;
+    *nsm = dp.multiProcessorCount;
+    return FA2_OK;
+}
+
+// Device buffers and a stream for the length of one call.
+struct DeviceScratch {
+    std::vector<void *> ptrs;
+    cudaStream_t stream = nullptr;
+    DeviceScratch() { cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking); }
+    ~DeviceScratch() {
+        if (stream) cudaStreamSynchronize(stream);
+        for (void *p : ptrs) cudaFree(p);
+        if (stream) cudaStreamDestroy(stream);
+    }
+    template <typename T>
+    int get(T **p, size_t count) {
+        void *q = nullptr;
+        const cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+        if (e != cudaSuccess) return cuda_status(e);
+        ptrs.push_back(q);
+        *p = (T *)q;
+        return stream ? FA2_OK : FA2_ERR_CUDA;
+    }
+};
+
+}  // namespace
+
+struct fa2_learn_set {
+    int device = 0;
+    int64_t cap = 0, size = 0;
+    float *feat = nullptr;  // cap x 12
+    float2 *tgt = nullptr;
+    float *w = nullptr;
+    cudaStream_t stream = nullptr;
+    // one collect's samples before they are put in order
+    int64_t st_cap = 0;
+    float *st_feat = nullptr;
+    float2 *st_tgt = nullptr;
+    float *st_w = nullptr;
+    uint64_t *st_key = nullptr;
+    unsigned long long *st_count = nullptr;
+};
+
+namespace {
+
+int set_staging(fa2_learn_set *set, int64_t need) {
+    if (set->st_cap >= need && set->st_count) return FA2_OK;
+    cudaFree(set->st_feat);
+    cudaFree(set->st_tgt);
+    cudaFree(set->st_w);
+    cudaFree(set->st_key);
+    cudaFree(set->st_count);
+    set->st_feat = nullptr;
+    set->st_tgt = nullptr;
+    set->st_w = nullptr;
+    set->st_key = nullptr;
+    set->st_count = nullptr;
+    set->st_cap = 0;
+    const size_t k = (size_t)need;
+    CK(cudaMalloc(&set->st_feat, k * kLearnIn * 4));
+    CK(cudaMalloc(&set->st_tgt, k * 8));
+    CK(cudaMalloc(&set->st_w, k * 4));
+    CK(cudaMalloc(&set->st_key, k * 8));
+    CK(cudaMalloc(&set->st_count, sizeof(unsigned long long)));
+    set->st_cap = need;
     return FA2_OK;
 }
 
@@ -955,6 +1133,296 @@ int fa2_set_overlap(fa2_ctx *c, int32_t enable) {
     CK(cudaStreamSynchronize(c->sA));
     c->overlap = enable != 0;
     drop_graphs(c);  // recaptured with the new stream layout at the next step
+    return FA2_OK;
+}
+
+// ------------------------------------------------ learned correction --
+
+void fa2_mlp_init(fa2_mlp *mlp, uint32_t seed) {
+    if (!mlp) return;
+    mlp_default_init(mlp, seed);
+}
+
+int fa2_set_learned_correction(fa2_ctx *c, const fa2_mlp *mlp) {
+    if (!c) return FA2_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->sA));
+    if (!mlp) {
+        if (c->learn_on) {
+            c->learn_on = false;
+            drop_graphs(c);
+        }
+        return FA2_OK;
+    }
+    if (!mlp_is_finite(*mlp)) return FA2_ERR_INVALID_ARGUMENT;
+    int s = ensure_quad_buffers(c);
+    if (!s) s = ensure_learn_buffers(c);
+    if (s) return s;
+    MlpDevice host;
+    mlp_to_device(*mlp, host);
+    CK(cudaMemcpyAsync(c->d_mlp, &host, sizeof(host), cudaMemcpyHostToDevice, c->sA));
+    CK(cudaStreamSynchronize(c->sA));
+    if (!c->learn_on) {
+        c->learn_on = true;
+        drop_graphs(c);  // the learned walk, MLP and tail are captured anew
+    }
+    return FA2_OK;
+}
+
+int fa2_mlp_forward(int32_t device, const fa2_mlp *mlp, const float *features, int64_t n,
+                    float *out) {
+    if (!mlp || n < 0 || (n && (!features || !out))) return FA2_ERR_INVALID_ARGUMENT;
+    if (n == 0) return FA2_OK;
+    int nsm = 0;
+    int s = use_device(device, &nsm);
+    if (s) return s;
+    MlpDevice host;
+    mlp_to_device(*mlp, host);
+    DeviceScratch mem;
+    MlpDevice *d_mlp = nullptr;
+    float *d_feat = nullptr;
+    float2 *d_out = nullptr;
+    int *d_err = nullptr;
+    if ((s = mem.get(&d_mlp, 1)) || (s = mem.get(&d_feat, (size_t)n * FA2_MLP_IN)) ||
+        (s = mem.get(&d_out, (size_t)n)) || (s = mem.get(&d_err, 1)))
+        return s;
+    cudaStream_t st = mem.stream;
+    CK(cudaMemcpyAsync(d_mlp, &host, sizeof(host), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_feat, features, (size_t)n * FA2_MLP_IN * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+    launch_mlp_rows(d_mlp, d_feat, n, d_out, d_err, nsm, st);
+    CK(cudaGetLastError());
+    int err = 0;
+    CK(cudaMemcpyAsync(out, d_out, (size_t)n * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return err ? FA2_ERR_DEVICE_LIMIT : FA2_OK;
+}
+
+int fa2_mlp_train_step(int32_t device, fa2_mlp *params, fa2_mlp *adam_m, fa2_mlp *adam_v,
+                       int32_t step, float lr, const float *features, const float *targets,
+                       const float *weights, int32_t n, float *loss) {
+    if (!params || !adam_m || !adam_v || step < 1 || n < 1 || !features || !targets || !weights)
+        return FA2_ERR_INVALID_ARGUMENT;
+    static_assert(sizeof(fa2_mlp) == sizeof(float) * kLearnParams, "fa2_mlp is the parameter vector");
+    int nsm = 0;
+    int s = use_device(device, &nsm);
+    if (s) return s;
+    DeviceScratch mem;
+    float *d_p = nullptr, *d_m = nullptr, *d_v = nullptr, *d_x = nullptr, *d_w = nullptr,
+          *d_scr = nullptr, *d_loss = nullptr;
+    float2 *d_t = nullptr;
+    if ((s = mem.get(&d_p, kLearnParams)) || (s = mem.get(&d_m, kLearnParams)) ||
+        (s = mem.get(&d_v, kLearnParams)) || (s = mem.get(&d_x, (size_t)n * FA2_MLP_IN)) ||
+        (s = mem.get(&d_t, (size_t)n)) || (s = mem.get(&d_w, (size_t)n)) ||
+        (s = mem.get(&d_scr, learn_train_scratch_floats(n))) || (s = mem.get(&d_loss, 1)))
+        return s;
+    cudaStream_t st = mem.stream;
+    CK(cudaMemcpyAsync(d_p, params, sizeof(fa2_mlp), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_m, adam_m, sizeof(fa2_mlp), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_v, adam_v, sizeof(fa2_mlp), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_x, features, (size_t)n * FA2_MLP_IN * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_t, targets, (size_t)n * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_w, weights, (size_t)n * 4, cudaMemcpyHostToDevice, st));
+    launch_learn_train_step(d_p, d_m, d_v, step, lr, d_x, d_t, d_w, 1.0f, nullptr, n, d_scr,
+                            d_loss, st);
+    CK(cudaGetLastError());
+    float l = 0.0f;
+    CK(cudaMemcpyAsync(params, d_p, sizeof(fa2_mlp), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(adam_m, d_m, sizeof(fa2_mlp), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(adam_v, d_v, sizeof(fa2_mlp), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&l, d_loss, sizeof(float), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (loss) *loss = l;
+    return FA2_OK;
+}
+
+fa2_learn_set *fa2_learn_set_create(int32_t device, int64_t capacity, int *status) {
+    int dummy;
+    if (!status) status = &dummy;
+    *status = FA2_ERR_INVALID_ARGUMENT;
+    if (capacity < 1) return nullptr;
+    int nsm = 0;
+    if ((*status = use_device(device, &nsm))) return nullptr;
+    fa2_learn_set *set = new fa2_learn_set();
+    set->device = device;
+    set->cap = capacity;
+    const size_t cap = (size_t)capacity;
+    if (cudaMalloc(&set->feat, cap * FA2_MLP_IN * 4) != cudaSuccess ||
+        cudaMalloc(&set->tgt, cap * 8) != cudaSuccess ||
+        cudaMalloc(&set->w, cap * 4) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&set->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        fa2_learn_set_destroy(set);
+        *status = FA2_ERR_OUT_OF_MEMORY;
+        return nullptr;
+    }
+    *status = FA2_OK;
+    return set;
+}
+
+void fa2_learn_set_destroy(fa2_learn_set *set) {
+    if (!set) return;
+    cudaSetDevice(set->device);
+    if (set->stream) cudaStreamSynchronize(set->stream);
+    cudaFree(set->feat);
+    cudaFree(set->tgt);
+    cudaFree(set->w);
+    cudaFree(set->st_feat);
+    cudaFree(set->st_tgt);
+    cudaFree(set->st_w);
+    cudaFree(set->st_key);
+    cudaFree(set->st_count);
+    if (set->stream) cudaStreamDestroy(set->stream);
+    delete set;
+}
+
+int64_t fa2_learn_set_size(const fa2_learn_set *set) { return set ? set->size : 0; }
+
+int fa2_learn_collect(fa2_learn_set *set, fa2_ctx *c, float theta, int32_t multipole,
+                      int64_t *added) {
+    if (added) *added = 0;
+    if (!set || !c || !(theta > 0.0f) || multipole < 1 || multipole > 2 ||
+        set->device != c->device)
+        return FA2_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(c->device));
+    if (c->n == 0) return FA2_OK;
+    CK(cudaStreamSynchronize(c->sA));
+    int s = ensure_quad_buffers(c);
+    if (!s) s = ensure_learn_buffers(c);
+    if (!s) s = set_staging(set, c->lb.pair_cap);
+    if (s) return s;
+    Params kp = c->kp;
+    kp.itolsq = 1.0f / (theta * theta);
+    kp.multipole = multipole;
+    Buffers b = c->b;
+    b.sort_first = 0;  // every digit: the walk needs no earlier tree
+    cudaStream_t A = c->sA;
+    CK(cudaMemsetAsync(c->scratch, 0, c->scratch_bytes, A));
+    CK(cudaMemsetAsync(set->st_count, 0, sizeof(unsigned long long), A));
+    launch_keys(b, c->nsm, A);
+    launch_sort(b, A);
+    launch_tree_count(b, true, A);
+    launch_moments(b, A);
+    launch_emit(b, c->nsm, A);
+    launch_quad_cells(b, c->nsm, A);
+    launch_traverse_learn(b, kp, c->lb, c->trav_blocks, A);
+    launch_learn_targets(b, kp, c->lb, set->st_feat, set->st_tgt, set->st_w, set->st_key,
+                         set->st_count, (uint64_t)set->st_cap, c->nsm, A);
+    CK(cudaGetLastError());
+    DevState st;
+    s = read_state(c, &st);
+    if (s) return s;
+    if (st.err) return FA2_ERR_DEVICE_LIMIT;
+    if (st.poison) {
+        // coincident bodies: the next step moves them apart; the flag goes
+        // with this walk
+        CK(cudaMemsetAsync(&c->b.st->poison, 0, sizeof(int), A));
+        CK(cudaStreamSynchronize(A));
+        return FA2_OK;
+    }
+    unsigned long long got = 0;
+    CK(cudaMemcpy(&got, set->st_count, sizeof(got), cudaMemcpyDeviceToHost));
+    const size_t k = (size_t)std::min<unsigned long long>(got, (unsigned long long)set->st_cap);
+    if (k == 0) return FA2_OK;
+    // the samples in (group, node) order, whatever order the warps wrote them in
+    std::vector<uint64_t> key(k);
+    std::vector<float> feat(k * FA2_MLP_IN), w(k);
+    std::vector<float2> tgt(k);
+    CK(cudaMemcpy(key.data(), set->st_key, k * 8, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(feat.data(), set->st_feat, k * FA2_MLP_IN * 4, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(tgt.data(), set->st_tgt, k * 8, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(w.data(), set->st_w, k * 4, cudaMemcpyDeviceToHost));
+    std::vector<uint32_t> order(k);
+    std::iota(order.begin(), order.end(), 0u);
+    std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b2) { return key[a] < key[b2]; });
+    const size_t room = (size_t)std::max<int64_t>(set->cap - set->size, 0);
+    const size_t take = std::min(k, room);
+    std::vector<float> feat2(take * FA2_MLP_IN), w2(take);
+    std::vector<float2> tgt2(take);
+    for (size_t q = 0; q < take; ++q) {
+        const uint32_t o = order[q];
+        std::copy(&feat[(size_t)o * FA2_MLP_IN], &feat[(size_t)o * FA2_MLP_IN] + FA2_MLP_IN,
+                  &feat2[q * FA2_MLP_IN]);
+        tgt2[q] = tgt[o];
+        w2[q] = w[o];
+    }
+    if (take) {
+        const size_t at = (size_t)set->size;
+        CK(cudaMemcpy(set->feat + at * FA2_MLP_IN, feat2.data(), take * FA2_MLP_IN * 4,
+                      cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(set->tgt + at, tgt2.data(), take * 8, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(set->w + at, w2.data(), take * 4, cudaMemcpyHostToDevice));
+        set->size += (int64_t)take;
+    }
+    if (added) *added = (int64_t)take;
+    return FA2_OK;
+}
+
+int fa2_learn_set_read(const fa2_learn_set *set, int64_t first, int64_t count, float *features,
+                       float *targets, float *weights) {
+    if (!set || first < 0 || count < 0 || first + count > set->size) return FA2_ERR_INVALID_ARGUMENT;
+    if (count == 0) return FA2_OK;
+    CK(cudaSetDevice(set->device));
+    const size_t f0 = (size_t)first, k = (size_t)count;
+    if (features)
+        CK(cudaMemcpy(features, set->feat + f0 * FA2_MLP_IN, k * FA2_MLP_IN * 4,
+                      cudaMemcpyDeviceToHost));
+    if (targets) CK(cudaMemcpy(targets, set->tgt + f0, k * 8, cudaMemcpyDeviceToHost));
+    if (weights) CK(cudaMemcpy(weights, set->w + f0, k * 4, cudaMemcpyDeviceToHost));
+    return FA2_OK;
+}
+
+int fa2_learn_fit(fa2_learn_set *set, fa2_mlp *mlp, int32_t steps, int32_t batch, float lr,
+                  uint32_t seed, float *final_loss) {
+    if (!set || !mlp || steps < 1 || batch < 1 || !(lr > 0.0f) || set->size < 1)
+        return FA2_ERR_INVALID_ARGUMENT;
+    if (set->size > (int64_t)0xFFFFFFFFll) return FA2_ERR_TOO_LARGE;
+    CK(cudaSetDevice(set->device));
+    const int64_t size = set->size;
+    const int bsz = (int)std::min<int64_t>(batch, size);
+    cudaStream_t st = set->stream;
+    DeviceScratch mem;
+    float *d_p = nullptr, *d_m = nullptr, *d_v = nullptr, *d_scr = nullptr, *d_loss = nullptr;
+    double *d_wsum = nullptr;
+    uint32_t *d_idx = nullptr;
+    int s = FA2_OK;
+    if ((s = mem.get(&d_p, kLearnParams)) || (s = mem.get(&d_m, kLearnParams)) ||
+        (s = mem.get(&d_v, kLearnParams)) || (s = mem.get(&d_scr, learn_train_scratch_floats(bsz))) ||
+        (s = mem.get(&d_loss, 1)) || (s = mem.get(&d_wsum, 1)) ||
+        (s = mem.get(&d_idx, (size_t)size)))
+        return s;
+    CK(cudaMemcpyAsync(d_p, mlp, sizeof(fa2_mlp), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(d_m, 0, sizeof(fa2_mlp), st));
+    CK(cudaMemsetAsync(d_v, 0, sizeof(fa2_mlp), st));
+    launch_learn_weight_sum(set->w, (uint64_t)size, d_wsum, st);
+    CK(cudaGetLastError());
+    double wsum = 0.0;
+    CK(cudaMemcpyAsync(&wsum, d_wsum, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const float wscale = wsum > 0.0 ? (float)((double)size / wsum) : 1.0f;
+    std::vector<uint32_t> perm((size_t)size);
+    std::iota(perm.begin(), perm.end(), 0u);
+    std::mt19937 rng(seed);
+    int64_t pos = size;  // forces a shuffle before the first batch
+    for (int32_t t = 0; t < steps; ++t) {
+        if (pos + bsz > size) {
+            std::shuffle(perm.begin(), perm.end(), rng);
+            CK(cudaStreamSynchronize(st));  // the last batch no longer reads d_idx
+            CK(cudaMemcpyAsync(d_idx, perm.data(), (size_t)size * 4, cudaMemcpyHostToDevice, st));
+            pos = 0;
+        }
+        const float lr_t =
+            steps > 1 ? lr * (float)std::pow(0.05, (double)t / (double)(steps - 1)) : lr;
+        launch_learn_train_step(d_p, d_m, d_v, t + 1, lr_t, set->feat, set->tgt, set->w, wscale,
+                                d_idx + pos, bsz, d_scr, t + 1 == steps ? d_loss : nullptr, st);
+        pos += bsz;
+    }
+    CK(cudaGetLastError());
+    float l = 0.0f;
+    CK(cudaMemcpyAsync(mlp, d_p, sizeof(fa2_mlp), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&l, d_loss, sizeof(float), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (final_loss) *final_loss = l;
     return FA2_OK;
 }
 

@@ -244,6 +244,56 @@ __device__ __forceinline__ void speed_update(float swg, float etra, int n, float
     gs += fminf(targetSpeed - gs, max_rise * gs);
 }
 
+// End of a pass that wrote one (swing, traction) partial per group of 32
+// sorted bodies: the last block to finish sums the partials in a fixed order
+// (thread-strided, then the warp's lanes, then the block's warps) and applies
+// the speed rule (src/RPFA2Kernels.cu:177-219).  Every thread of the block
+// calls it; s_last and s_red are the caller's shared memory.
+template <int THREADS>
+__device__ __forceinline__ void speed_finish(int n, const float2 *warp_partial, unsigned *done,
+                                             DevState *st, bool &s_last,
+                                             float (&s_red)[2][THREADS / kWarp]) {
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (n + 31) >> 5;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    float sw = 0.0f, tr = 0.0f;
+    for (int w = threadIdx.x; w < nwarps; w += THREADS) {
+        float2 v = __ldcg(&warp_partial[w]);
+        sw += v.x;
+        tr += v.y;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        sw += __shfl_xor_sync(kFullMask, sw, o);
+        tr += __shfl_xor_sync(kFullMask, tr, o);
+    }
+    if (lane == 0) {
+        s_red[0][threadIdx.x >> 5] = sw;
+        s_red[1][threadIdx.x >> 5] = tr;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float swg = 0.0f, etra = 0.0f;
+        for (int w = 0; w < THREADS / kWarp; ++w) {
+            swg += s_red[0][w];
+            etra += s_red[1][w];
+        }
+        st->swg_sum = swg;
+        st->etra_sum = etra;
+        float se = st->speed_efficiency, gs = st->global_speed;
+        speed_update(swg, etra, n, st->jitter_tolerance, st->k_s_max, se, gs);
+        st->speed_efficiency = se;
+        st->global_speed = gs;
+    }
+}
+
 // Displacement factor of one body (DisplacementKernel, src/RPFA2Kernels.cu:
 // 223-251): speed / (1 + sqrt(speed * |f - f_prev|)), the sum in double.
 __device__ __forceinline__ float displacement_factor(float2 fi, float2 fp, float global_speed) {

@@ -12,6 +12,7 @@
 #include <stdint.h>
 
 #include "fa2_device.cuh"
+#include "fa2_learn.cuh"
 
 namespace fa2 {
 
@@ -148,17 +149,25 @@ __global__ void __launch_bounds__(1024) k_keys(int n, int tile, int first,
 // conj(a2 / w^3) = conj(a2) u^3 with w = z - Z, u = w / |w|^2 and the softened
 // |w|^2 = d^2 + eps; a2 is the cell's complex second moment (k_quad_cells).  No
 // reference counterpart: it is the option fa2_set_approximation selects.
-template <bool QUAD>
+//
+// LEARN (the learned correction, fa2_learn.cuh) also records, per group, the
+// centroid and second moments of its bodies and every cell the whole group
+// accepted (a (group, node) pair, gathered 32 at a time in shared memory),
+// and writes each body's repulsion in sorted order instead of the tail: the
+// MLP and k_learn_tail finish the iteration.  The sums are the same.
+template <bool QUAD, bool LEARN>
 __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
     int n, const float4 *__restrict nodes, const float2 *__restrict quad,
     const uint32_t *__restrict body_node,
     const uint32_t *__restrict vals, const float2 *__restrict fag,
     const float2 *__restrict fprev, float2 *__restrict f, float2 *__restrict warp_partial,
-    DevState *st, IterCounters *ctr, Params prm) {
+    DevState *st, IterCounters *ctr, Params prm, LearnBuffers lb) {
     __shared__ float s_dq[64];
     __shared__ bool s_last;
     __shared__ float s_red[2][kTravThreads / kWarp];
+    __shared__ uint32_t s_pair[LEARN ? kTravThreads : 1];
     if (st->err || st->poison) return;
+    uint32_t *my_pairs = s_pair + (LEARN ? (threadIdx.x & ~31u) : 0u);
     if (threadIdx.x == 0) {
         // src/RPBHKernels.cu:579-592: dq for the children of the root is
         // (2 radius)^2 / theta^2 + eps, quartering per level.
@@ -195,6 +204,42 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
         // k_r m_i multiplies the sum once at the end
         float ax = 0.0f, ay = 0.0f;
         uint32_t node = 1;
+        int npend = 0;  // LEARN: accepted cells waiting in my_pairs
+        if (LEARN) {
+            // the group's centroid and second moments about it
+            const float cnt = (float)__popc(__ballot_sync(kFull, active));
+            float sx = active ? px : 0.0f, sy = active ? py : 0.0f;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                sx += __shfl_xor_sync(kFull, sx, o);
+                sy += __shfl_xor_sync(kFull, sy, o);
+            }
+            const float gx = sx / cnt, gy = sy / cnt;
+            const float u = active ? px - gx : 0.0f, v = active ? py - gy : 0.0f;
+            float t0 = u * u + v * v, t1 = u * u - v * v, t2 = 2.0f * u * v;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                t0 += __shfl_xor_sync(kFull, t0, o);
+                t1 += __shfl_xor_sync(kFull, t1, o);
+                t2 += __shfl_xor_sync(kFull, t2, o);
+            }
+            if (lane == 0) {
+                lb.ggeo[2 * w] = make_float4(gx, gy, t0 / cnt, cnt);
+                lb.ggeo[2 * w + 1] = make_float4(t1 / cnt, t2 / cnt, 0.0f, 0.0f);
+            }
+        }
+        // LEARN: the pending cells to the pair list, one atomic per flush
+        auto flush = [&]() {
+            __syncwarp();
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(&ctr->pair_count, (unsigned)npend);
+            base = __shfl_sync(kFull, base, 0);
+            if (lane < npend && base + lane < lb.pair_cap)
+                lb.pairs[base + lane] = make_uint2((uint32_t)w, my_pairs[lane]);
+            if (lane == 0 && base + (uint32_t)npend > lb.pair_cap) atomicOr(&st->err, kErrPairs);
+            __syncwarp();
+            npend = 0;
+        };
         // An opened cell's first child is node + 1 and always exists, so only
         // a jump to "next" can end the walk.
         if (!QUAD && node < end) {
@@ -209,6 +254,10 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
                     const float c = __fdividef(r.z, d2);
                     ax = fmaf(dx, c, ax);
                     ay = fmaf(dy, c, ay);
+                    if (LEARN && meta_level(meta) != kBodyLevel) {
+                        if (lane == 0) my_pairs[npend] = node;
+                        if (++npend == 32) flush();
+                    }
                     node = meta_next(meta);
                     if (node >= end) break;
                 } else {
@@ -246,6 +295,10 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
                         const float ui = uy * fmaf(-3.0f, xx, yy);
                         ax = fmaf(q.x, ur, fmaf(-q.y, ui, ax));
                         ay = fmaf(-q.x, ui, fmaf(-q.y, ur, ay));
+                        if (LEARN) {
+                            if (lane == 0) my_pairs[npend] = node;
+                            if (++npend == 32) flush();
+                        }
                     }
                     node = next;
                     if (node >= end) break;
@@ -258,6 +311,11 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
         const float kmi = prm.k_r * me.z;
         ax *= kmi;
         ay *= kmi;
+        if (LEARN) {
+            if (npend) flush();
+            if (active) lb.rep[k] = make_float2(ax, ay);
+            continue;
+        }
         float sw = 0.0f, tr = 0.0f;
         if (active) {
             const uint32_t i = vals[k];
@@ -277,44 +335,9 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
         }
         if (lane == 0) warp_partial[w] = make_float2(sw, tr);
     }
+    if (LEARN) return;
     // last block: fixed-order sum of the per-warp partials, then the speed rule
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        s_last = atomicAdd(&ctr->trav_done, 1u) == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    float sw = 0.0f, tr = 0.0f;
-    for (int w = threadIdx.x; w < nwarps; w += blockDim.x) {
-        float2 v = __ldcg(&warp_partial[w]);
-        sw += v.x;
-        tr += v.y;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        sw += __shfl_xor_sync(kFull, sw, o);
-        tr += __shfl_xor_sync(kFull, tr, o);
-    }
-    if (lane == 0) {
-        s_red[0][threadIdx.x >> 5] = sw;
-        s_red[1][threadIdx.x >> 5] = tr;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        float swg = 0.0f, etra = 0.0f;
-        for (int w = 0; w < kTravThreads / kWarp; ++w) {
-            swg += s_red[0][w];
-            etra += s_red[1][w];
-        }
-        st->swg_sum = swg;
-        st->etra_sum = etra;
-        float se = st->speed_efficiency, gs = st->global_speed;
-        speed_update(swg, etra, n, st->jitter_tolerance, st->k_s_max, se, gs);
-        st->speed_efficiency = se;
-        st->global_speed = gs;
-    }
+    speed_finish<kTravThreads>(n, warp_partial, &ctr->trav_done, st, s_last, s_red);
 }
 
 // The walk of k_traverse without the force arithmetic, over the tree still in
@@ -776,14 +799,29 @@ void launch_keys(const Buffers &b, int nsm, cudaStream_t s) {
 
 
 void launch_traverse(const Buffers &b, const Params &p, int nblocks, cudaStream_t s) {
+    const LearnBuffers none{};
+    auto go = [&](auto kernel) {
+        kernel<<<nblocks, kTravThreads, 0, s>>>(b.n, b.nodes, b.quad, b.body_node, b.vals[0],
+                                                b.fag, b.fprev, b.f, b.warp_partial, b.st, b.ctr,
+                                                p, none);
+    };
     if (p.multipole >= 2)
-        k_traverse<true><<<nblocks, kTravThreads, 0, s>>>(b.n, b.nodes, b.quad, b.body_node,
-                                                          b.vals[0], b.fag, b.fprev, b.f,
-                                                          b.warp_partial, b.st, b.ctr, p);
+        go(k_traverse<true, false>);
     else
-        k_traverse<false><<<nblocks, kTravThreads, 0, s>>>(b.n, b.nodes, b.quad, b.body_node,
-                                                           b.vals[0], b.fag, b.fprev, b.f,
-                                                           b.warp_partial, b.st, b.ctr, p);
+        go(k_traverse<false, false>);
+}
+
+void launch_traverse_learn(const Buffers &b, const Params &p, const LearnBuffers &lb,
+                           int nblocks, cudaStream_t s) {
+    auto go = [&](auto kernel) {
+        kernel<<<nblocks, kTravThreads, 0, s>>>(b.n, b.nodes, b.quad, b.body_node, b.vals[0],
+                                                b.fag, b.fprev, b.f, b.warp_partial, b.st, b.ctr,
+                                                p, lb);
+    };
+    if (p.multipole >= 2)
+        go(k_traverse<true, true>);
+    else
+        go(k_traverse<false, true>);
 }
 
 void launch_guard(const Buffers &b, const Params &p, int ns, double2 *exact, float2 *plain,
@@ -839,10 +877,12 @@ void launch_sorted_ref_ids(int n, const uint32_t *ref_of, const uint32_t *vals, 
 
 int traverse_blocks_per_sm() {
     // the walk lives on L1 hits: give L1 the most of the SM's on-chip memory
-    cudaFuncSetAttribute(k_traverse<false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-    cudaFuncSetAttribute(k_traverse<true>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+    cudaFuncSetAttribute(k_traverse<false, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+    cudaFuncSetAttribute(k_traverse<true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+    cudaFuncSetAttribute(k_traverse<false, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+    cudaFuncSetAttribute(k_traverse<true, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_traverse<false>, kTravThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_traverse<false, false>, kTravThreads, 0);
     return nb < 1 ? 1 : nb;
 }
 

@@ -217,6 +217,106 @@ int fa2_get_accuracy_guard(fa2_ctx *ctx, double *err_current, double *err_plain,
  * if none.  The string stays valid until this thread's next failing call. */
 const char *fa2_last_cuda_error(void);
 
+/* ------------------------------------------------------------------------
+ * Learned far-field correction.  No counterpart in the reference: its walk
+ * adds every accepted cell as a point mass at its centre of mass
+ * (src/RPBHKernels.cu:656-668), and that term is what the correction mends.
+ *
+ * A warp walks the tree for a group of 32 sorted bodies and accepts a cell
+ * only if all 32 pass the cell test.  Every (group, accepted cell) pair goes
+ * through a 12 -> 64 -> 64 -> 2 MLP.  Its features are the cell's multipole
+ * statistics as the group sees them: mass, second moments, width, level and
+ * acceptance margin, plus the group's spread and moments, taken relative to
+ * the distance d from the cell's centre of mass to the group's centroid, in a
+ * frame turned to that direction.  Its two outputs, turned back and
+ * multiplied by M / d, estimate the mean over the group's bodies of the error
+ * the walk's term makes for that cell.  Each body of the group receives k_r
+ * m_i times the sum of its pairs' estimates.
+ * The MLP runs on the tensor cores with BF16 weights and activations and
+ * FP32 accumulation.  A pair whose group spread is more than half of d gets
+ * no correction.
+ * ---------------------------------------------------------------------- */
+
+#define FA2_MLP_IN 12
+#define FA2_MLP_HIDDEN 64
+#define FA2_MLP_OUT 2
+
+/* The MLP's parameters in FP32, laid out like PyTorch's nn.Linear weights
+ * ([out][in], row-major).  Inference rounds w1, w2 and w3 and the hidden
+ * activations to BF16; the biases stay FP32. */
+typedef struct fa2_mlp {
+    float w1[FA2_MLP_HIDDEN * FA2_MLP_IN];
+    float b1[FA2_MLP_HIDDEN];
+    float w2[FA2_MLP_HIDDEN * FA2_MLP_HIDDEN];
+    float b2[FA2_MLP_HIDDEN];
+    float w3[FA2_MLP_OUT * FA2_MLP_HIDDEN];
+    float b3[FA2_MLP_OUT];
+} fa2_mlp;
+
+/* PyTorch's default initialisation of nn.Linear: every weight and bias
+ * uniform in +-1/sqrt(fan_in), drawn from a generator seeded with seed. */
+void fa2_mlp_init(fa2_mlp *mlp, uint32_t seed);
+
+/* Turns the correction on for the iterations that follow (mlp != NULL), on
+ * top of the walk fa2_set_approximation selected (theta, multipole 1 or 2);
+ * NULL turns it off.  The weights are copied.  A learned iteration also runs
+ * the moment scan of the quadrupole option (the features need each cell's
+ * second moment), the MLP and a separate tail kernel for the force sum and
+ * the speed rule.  With all-zero weights it gives the plain walk's forces
+ * and positions bit for bit.  The accuracy guard (fa2_set_accuracy_guard)
+ * checks the corrected repulsion and, on a fallback, also turns the
+ * correction off. */
+int fa2_set_learned_correction(fa2_ctx *ctx, const fa2_mlp *mlp);
+
+/* The inference kernel alone: out[2 r], out[2 r + 1] = MLP(features[12 r ..
+ * 12 r + 11]) for n rows (host arrays), on CUDA device `device`. */
+int fa2_mlp_forward(int32_t device, const fa2_mlp *mlp, const float *features, int64_t n,
+                    float *out);
+
+/* The training kernels alone: one Adam step (PyTorch's Adam with its default
+ * betas 0.9, 0.999 and eps 1e-8; `step` counts from 1) over n samples (host
+ * arrays: features n x 12, targets n x 2, weights n) of the loss
+ * sum_s min(w_s, 100) |MLP(x_s) - t_s|^2 / (2 n), in FP32.  params, adam_m and
+ * adam_v are updated in place; *loss (if not NULL) receives the loss before
+ * the step. */
+int fa2_mlp_train_step(int32_t device, fa2_mlp *params, fa2_mlp *adam_m, fa2_mlp *adam_v,
+                       int32_t step, float lr, const float *features, const float *targets,
+                       const float *weights, int32_t n, float *loss);
+
+/* Training samples held in device memory. */
+typedef struct fa2_learn_set fa2_learn_set;
+
+/* Room for `capacity` samples on CUDA device `device` (60 bytes each). */
+fa2_learn_set *fa2_learn_set_create(int32_t device, int64_t capacity, int *status);
+void fa2_learn_set_destroy(fa2_learn_set *set);
+int64_t fa2_learn_set_size(const fa2_learn_set *set);
+
+/* Adds the samples of ctx's current positions: builds the tree, walks it at
+ * `theta` with `multipole` (the walk the correction will be used on) and, for
+ * every (group, cell) pair that passes the spread test, stores its features,
+ * its target (the exact FP64 mean over the group's bodies of the error of the
+ * walk's term for that cell, turned and scaled as the MLP's outputs are) and
+ * its weight ((M/d)^2 times the sum of the group's squared masses: the
+ * pair's share of the squared force error).  The samples of one call are
+ * stored in (group, node) order.  Positions, speeds and the forces of the
+ * last step are left as they were; the tree, sort order and fa2_get_stats
+ * then describe this walk.  Samples past the capacity are dropped (*added
+ * counts those stored).  Coincident bodies stop the walk: nothing is added. */
+int fa2_learn_collect(fa2_learn_set *set, fa2_ctx *ctx, float theta, int32_t multipole,
+                      int64_t *added);
+
+/* Copies samples [first, first + count) to host arrays (NULL skips one). */
+int fa2_learn_set_read(const fa2_learn_set *set, int64_t first, int64_t count, float *features,
+                       float *targets, float *weights);
+
+/* Trains mlp (in place, from its current values) for `steps` Adam steps on
+ * batches of `batch` samples: the set in a random order drawn from `seed`,
+ * reshuffled at every pass; weights scaled to a mean of 1 over the set;
+ * learning rate lr decaying exponentially to lr / 20 at the last step.
+ * *final_loss (if not NULL) is the last batch's loss. */
+int fa2_learn_fit(fa2_learn_set *set, fa2_mlp *mlp, int32_t steps, int32_t batch, float lr,
+                  uint32_t seed, float *final_loss);
+
 /* Measurement hook, no reference counterpart.  enable = 1 (the default) runs
  * the attraction on a second stream beside the tree build, the two sharing
  * the GPU; enable = 0 runs it alone before the tree build, so that the
