@@ -3,8 +3,8 @@
 
 Workload (one "step" = one ForceAtlas2 iteration of the whole graph):
   R-MAT scale 20, 16,777,216 edge draws, a=.57 b=.19 c=.19 (seed 0), self-loops
-  and repeated undirected edges removed (N = 646,043 nodes, E = 15,701,711
-  edges); positions uniform in [-1e4, 1e4]^2 (srandom(1234) + the reference's
+  and repeated undirected edges removed (N = 646,567 nodes, E = 15,702,443
+  edges with this generator); positions uniform in [-1e4, 1e4]^2 (srandom(1234) + the reference's
   randomizePositions); strong gravity, scale 10, gravity 1, theta 1.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
@@ -201,9 +201,32 @@ def cpu_baseline_sample(og, xy):
 CORRECTION_SAMPLES = 4096
 GUARD_EVERY, GUARD_SAMPLES = 25, 512
 CORRECTION_THETAS = (1.2, 1.4, 1.5, 1.6, 1.7, 1.8, 2.0)
+# The learned correction: trained on R-MAT scale 16 (1,048,576 draws) from
+# 200 layout snapshots of a plain run, evaluated on the workload at these
+# (theta, multipole) walks against the plain walk at theta 1.
+TRAIN_SCALE, TRAIN_DRAWS = 16, 1 << 20
+LEARNED = ((1.2, 1), (1.5, 1), (2.0, 1), (2.0, 2))
+EQUAL_RMSE_TARGET = 1.5  # the speed-up at equal or lower error the design aims at
 
 
-def correction_report(eng, n, steps):
+def train_learned(eng_device):
+    """One MLP per (theta, multipole) of LEARNED, trained on the engine's
+    own layouts of the scale-16 R-MAT graph (gpugraphlayout_b200.learn)."""
+    from gpugraphlayout_b200 import UGraph, synth
+    from gpugraphlayout_b200.learn import train_correction
+    s_raw, t_raw = synth.rmat_edges(TRAIN_SCALE, TRAIN_DRAWS, seed=0)
+    g = UGraph.from_pairs(s_raw, t_raw)
+    s, t = g.edges()
+    out = {}
+    for theta, mp in LEARNED:
+        out[(theta, mp)] = train_correction(g.num_nodes(), s, t, theta=theta, multipole=mp,
+                                            strong_gravity=STRONG, gravity=K_G, scale=K_R,
+                                            width=WIDTH, device=eng_device)
+    return out, {"graph": f"R-MAT scale {TRAIN_SCALE} ({TRAIN_DRAWS:,} draws, seed 0)",
+                 "nodes": g.num_nodes(), "edges": g.num_edges()}
+
+
+def correction_report(eng, n, steps, device=0):
     """Far-field accuracy against cost at the current layout: the reference's
     monopole walk at theta 1 beside the quadrupole walk at larger theta.  Each
     configuration computes one step's repulsion from the same positions P; the
@@ -233,6 +256,70 @@ def correction_report(eng, n, steps):
                      "moments_ms": kms.get("moments", 0.0),
                      "quadrupole_ms": kms.get("quadrupole", 0.0)})
     base = rows[0]
+
+    # the learned correction on the same positions, samples and FP64 sums
+    models, train_graph = train_learned(device)
+    learned = []
+    for (theta, mp), (mlp, info) in models.items():
+        eng.set_approximation(theta, mp)
+        eng.set_learned_correction(mlp)
+        eng.set_positions(P)
+        eng.step(1)
+        tot, ga = eng.forces()
+        rep = (tot - ga)[samples].astype(np.float64)
+        err = float(np.sqrt(((rep - exact) ** 2).sum() / (exact ** 2).sum()))
+        visits = eng.stats()["visits"]
+        eng.set_positions(P)
+        ms, kms = eng.step_timed(k)
+        learned.append({"theta": theta, "multipole": mp, "rel_rmse": err, "visits": visits,
+                        "ms_per_step": ms / k,
+                        "walk_ms": kms.get("traverse", 0.0) + kms.get("quadrupole", 0.0),
+                        "moments_ms": kms.get("moments", 0.0),
+                        "mlp_and_tail_ms": kms.get("learn", 0.0),
+                        "training": {kk: info[kk] for kk in ("samples", "snapshots", "final_loss",
+                                                             "collect_s", "fit_s")}})
+        eng.set_learned_correction(None)
+    eng.set_approximation(1.0, 1)
+    ok_l = [r for r in learned if r["rel_rmse"] <= base["rel_rmse"]]
+    best_l = min(ok_l, key=lambda r: r["ms_per_step"]) if ok_l else None
+    fastest_l = min(learned, key=lambda r: r["ms_per_step"]) if learned else None
+    learned_guarded = None
+    if best_l is not None:
+        steps_g = 4 * GUARD_EVERY
+        eng.set_positions(P)
+        ms_plain, _ = eng.step_timed(steps_g)
+        eng.set_approximation(best_l["theta"], best_l["multipole"])
+        eng.set_learned_correction(models[(best_l["theta"], best_l["multipole"])][0])
+        eng.set_accuracy_guard(GUARD_EVERY, GUARD_SAMPLES)
+        eng.set_positions(P)
+        ms, _ = eng.step_timed(steps_g)
+        gd = eng.accuracy_guard()
+        eng.set_accuracy_guard(0, 0)
+        eng.set_learned_correction(None)
+        eng.set_approximation(1.0, 1)
+        learned_guarded = {"theta": best_l["theta"], "multipole": best_l["multipole"],
+                           "every": GUARD_EVERY, "samples": GUARD_SAMPLES, "steps": steps_g,
+                           "ms_per_step": ms / steps_g, "plain_ms_per_step": ms_plain / steps_g,
+                           "speedup_vs_plain": ms_plain / ms, **gd}
+    learned_report = {
+        "mlp": "12 -> 64 -> 64 -> 2, BF16 weights and activations, FP32 accumulation "
+               "(tcgen05, accumulators in tensor memory); trained with the FP32 training "
+               "kernels on FP64 exact targets",
+        "training_graph": train_graph,
+        "configs": learned,
+        "equal_rmse_speedup": (None if best_l is None else
+                               {"theta": best_l["theta"], "multipole": best_l["multipole"],
+                                "step": base["ms_per_step"] / best_l["ms_per_step"],
+                                "target": EQUAL_RMSE_TARGET,
+                                "met": base["ms_per_step"] / best_l["ms_per_step"]
+                                >= EQUAL_RMSE_TARGET}),
+        "fastest": (None if fastest_l is None else
+                    {"theta": fastest_l["theta"], "multipole": fastest_l["multipole"],
+                     "step": base["ms_per_step"] / fastest_l["ms_per_step"],
+                     "rel_rmse": fastest_l["rel_rmse"]}),
+        "guarded": learned_guarded,
+    }
+
     ok = [r for r in rows[1:] if r["rel_rmse"] <= base["rel_rmse"]]
     best = min(ok, key=lambda r: r["ms_per_step"]) if ok else None
     guarded = None
@@ -264,17 +351,18 @@ def correction_report(eng, n, steps):
                                 "step": base["ms_per_step"] / best["ms_per_step"],
                                 "walk": base["walk_ms"] / best["walk_ms"]}),
         "guarded": guarded,
+        "learned": learned_report,
     }
 
 
-def fp64_checks(eng, n):
+def fp64_checks(eng, n, checks=FP64_CHECKS):
     """The large run's accuracy record: every FP64_EVERY steps, the repulsion
     of the next step on FP64_SAMPLES sampled nodes against the exact FP64
     all-pairs sum at the same positions (computed on the GPU)."""
     rng = np.random.default_rng(5)
     samples = np.sort(rng.choice(n, min(FP64_SAMPLES, n), replace=False)).astype(np.uint32)
     out = []
-    for c in range(FP64_CHECKS):
+    for c in range(checks):
         eng.step(FP64_EVERY - 1)
         exact = eng.exact_repulsion(samples)
         eng.step(1)
@@ -285,7 +373,8 @@ def fp64_checks(eng, n):
     return {"samples": len(samples), "every": FP64_EVERY, "checks": out}
 
 
-def run_ours(args, world, rank, local):
+def run_ours(args, world, rank, local, fp64_n=FP64_CHECKS, correction=True):
+    """The R-MAT workload's record (rank 0; None on the other ranks)."""
     from gpugraphlayout_b200 import Engine, UGraph, kernel_names, random_positions, synth
     scale, draws, width = RMAT[args.workload]
     large = args.workload != "rmat20"
@@ -339,17 +428,22 @@ def run_ours(args, world, rank, local):
     e2e = world * args.steps / e2e_s
 
     if rank != 0:
-        return
+        eng.close()
+        return None
     # the correction report compares against the plain walk, so it runs only
     # when the plain walk is the workload
-    correction = correction_report(eng, n, args.steps) if plain and not large else None
-    fp64 = fp64_checks(eng, n) if large else None
+    correction = (correction_report(eng, n, args.steps, local)
+                  if correction and plain and not large else None)
+    fp64 = fp64_checks(eng, n, fp64_n) if large else None
     names = kernel_names()
     pk, pk_kind = peaks()
     hbm = float(pk["hbm_gbs"])
-    # algorithmic bytes per launch
-    nnz = st["nnz_padded"]
-    attract_bytes = 4 * nnz + 4 * (n + 1) + 8 * n + 4 * n + 8 * n
+    # algorithmic bytes per launch: the attraction reads both directions of
+    # every edge (4 B ids), the row offsets and each node's own position, and
+    # writes its force, 8E + 20N + 4 (each neighbour position is gathered
+    # from L2, not counted; the row padding and the mass read are not
+    # algorithmic either)
+    attract_bytes = 8 * m + 20 * n + 4
     disp_bytes = 40 * n
     trav_ms = kms_iso.get("traverse", 0.0)
     kernels = {}
@@ -406,10 +500,11 @@ def run_ours(args, world, rank, local):
         out["roofline"]["traffic"] = None
         out["cpu_baseline_skipped"] = ("one CPUForceAtlas2::doStep at this size takes minutes; "
                                        "the reference CPU baseline is in the rmat20 line")
+    eng.close()
     if world == 1 and not args.no_cpu_baseline and not large:
         from oracle import oracle as O
         out["cpu_baseline"] = cpu_baseline_sample(O.Graph(s_raw, t_raw), xy0)
-    print(json.dumps(out))
+    return out
 
 
 # ---------------------------------------------------------------- batched --
@@ -459,6 +554,7 @@ def batch_cpu_baseline(graphs, sample_ids):
 
 
 def run_batched(args, world, rank, local):
+    """The batched workload's record (rank 0; None on the other ranks)."""
     import torch
     from gpugraphlayout_b200 import BatchEngine, random_positions, shard, synth
     graphs = synth.sbm_batch(BATCH_GRAPHS, seed=0)
@@ -501,8 +597,9 @@ def run_batched(args, world, rank, local):
         eng.step(1)
         eng.get_positions_ptr(ptr)
     e2e = args.steps / barrier_max(world, time.perf_counter() - t0)
+    eng.close()
     if rank != 0:
-        return
+        return None
     pk, pk_kind = peaks()
     hbm = float(pk["hbm_gbs"])
     n_all = sum(g[0] for g in graphs)
@@ -533,7 +630,109 @@ def run_batched(args, world, rank, local):
         sizes = np.array([g[0] for g in graphs])
         sample = [int(i) for i in np.argsort(sizes)[:: len(graphs) // 8][:8]]
         out["cpu_baseline"] = batch_cpu_baseline(graphs, sample)
-    print(json.dumps(out))
+    return out
+
+
+# Wall-clock budget of the default run: the sub-records are skipped once the
+# run has taken this long (their graphs take tens of seconds to build).
+EXTRAS_BUDGET_S = 240.0
+SUB_STEPS, SUB_WARMUP = 10, 3
+
+
+def _compact(rec, keys):
+    return {k: rec[k] for k in keys if k in rec}
+
+
+CONFIG1_ITERS = 500
+
+
+def config1_record(local, no_cpu_baseline):
+    """The CPU baseline configuration: Barabasi-Albert, 10,000 nodes, m = 3,
+    seed 0; positions U[-1000,1000]^2; weak gravity, scale 80, gravity 1;
+    500 iterations, on the engine (device-timed, and end to end through the
+    C ABI) and on the reference's CPUForceAtlas2 from the same positions,
+    with both final layouts' statistics."""
+    from gpugraphlayout_b200 import Engine, UGraph, random_positions, synth
+    from gpugraphlayout_b200.layout_stats import summary
+    s_raw, t_raw = synth.ba_edges(10000, 3, seed=0)
+    g = UGraph.from_pairs(s_raw, t_raw)
+    n, m = g.num_nodes(), g.num_edges()
+    s, t = g.edges()
+    xy0 = random_positions(n, 2000.0, 2000.0, 1234)
+    eng = Engine(n, s, t, strong_gravity=False, gravity=1.0, scale=80.0, device=local)
+    eng.set_positions(xy0)
+    eng.step(5)  # warm-up, then the run starts again from the same state
+    eng.set_positions(xy0)
+    eng.set_speed_state(1.0, 1.0)
+    ms, _ = eng.step_timed(CONFIG1_ITERS)
+    ours_xy = eng.get_positions()
+    eng.set_speed_state(1.0, 1.0)
+    t0 = time.perf_counter()
+    eng.set_positions(xy0)
+    eng.step(CONFIG1_ITERS)
+    eng.get_positions()
+    e2e_s = time.perf_counter() - t0
+    eng.close()
+    rec = {"workload": f"Barabasi-Albert n=10,000 m=3 seed 0 (N={n:,} E={m:,}); positions "
+                       "U[-1000,1000]^2; weak gravity, scale 80, gravity 1, theta 1; "
+                       f"{CONFIG1_ITERS} iterations",
+           "value": CONFIG1_ITERS / (ms / 1000.0), "unit": UNIT, "ms_per_step": ms / CONFIG1_ITERS,
+           "e2e": {"value": CONFIG1_ITERS / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8 * n,
+                   "d2h_bytes_per_step": 8 * n,
+                   "note": "positions in once and out once around the 500 iterations"},
+           "layout": {"ours": summary(ours_xy, s, t, 64)}}
+    if not no_cpu_baseline:
+        from oracle import oracle as O
+        if O.ref_available():
+            og = O.Graph(s_raw, t_raw)
+            ref = O.RefCPUFA2(O.RefGraph(graph=og), 2000.0, 2000.0, 1234, True, False, 1.0,
+                              80.0)
+            ref.set_positions(xy0)
+            t0 = time.perf_counter()
+            ref.step(CONFIG1_ITERS)
+            dt = time.perf_counter() - t0
+            rec["cpu_baseline"] = {
+                "value": CONFIG1_ITERS / dt, "unit": UNIT, "cores": 1, "kind": "reference",
+                "sample": f"{CONFIG1_ITERS} iterations of CPUForceAtlas2::doStep (Barnes-Hut, "
+                          "1 thread) on the whole graph, from the same positions"}
+            rec["layout"]["reference_cpu"] = summary(ref.positions(), og.sources, og.targets, 64)
+    return rec
+
+
+def extras(args, local, out, t_start):
+    """The batched (4096 SBM graphs), the large (R-MAT scale 23) and the CPU
+    baseline (BA 10k) workloads, measured in the same run as compact
+    sub-records of the default line."""
+    import argparse as _ap
+    sub = _ap.Namespace(**vars(args))
+    sub.steps, sub.warmup, sub.no_cpu_baseline = SUB_STEPS, SUB_WARMUP, args.no_cpu_baseline
+    keys = ("metric", "value", "unit", "steps", "warmup", "ms_per_step", "config", "clocks",
+            "gpu_launches", "e2e", "roofline", "cpu_baseline", "autotune", "graph_iters_per_s",
+            "fp64_checks", "tree", "cpu_baseline_skipped")
+    if time.perf_counter() - t_start < EXTRAS_BUDGET_S:
+        try:
+            sub.workload = "batched"
+            out["batched"] = _compact(run_batched(sub, 1, 0, local), keys)
+        except Exception as e:  # a failed sub-record leaves the main line intact
+            out["batched"] = {"error": repr(e)}
+    else:
+        out["batched"] = {"skipped": "over the default run's wall-clock budget"}
+    if time.perf_counter() - t_start < EXTRAS_BUDGET_S:
+        try:
+            sub.workload = "rmat23"
+            sub.no_cpu_baseline = True
+            rec = run_ours(sub, 1, 0, local, fp64_n=1, correction=False)
+            rec["kernels_ms_alone"] = {k: v["ms_alone"] for k, v in rec.get("kernels", {}).items()
+                                       if v.get("ms_alone")}
+            out["rmat23"] = _compact(rec, keys + ("kernels_ms_alone",))
+        except Exception as e:
+            out["rmat23"] = {"error": repr(e)}
+    else:
+        out["rmat23"] = {"skipped": "over the default run's wall-clock budget"}
+    try:
+        out["config1"] = config1_record(local, args.no_cpu_baseline)
+    except Exception as e:
+        out["config1"] = {"error": repr(e)}
 
 
 def main():
@@ -543,6 +742,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="rmat20 at N=1 only: leave out the batched and rmat23 sub-records")
     ap.add_argument("--theta", type=float, default=1.0,
                     help="Barnes-Hut opening parameter of the rmat20 workload (reference: 1)")
     ap.add_argument("--multipole", type=int, default=1, choices=[1, 2],
@@ -560,7 +761,9 @@ def main():
                                       "has no reference arm; its cpu_baseline is in the "
                                       "default arm's line"}))
             else:
-                run_batched(args, world, rank, local)
+                out = run_batched(args, world, rank, local)
+                if out is not None:
+                    print(json.dumps(out))
         elif args.impl == "reference" and args.workload != "rmat20":
             if rank == 0:
                 print(json.dumps({"impl": "reference", "unavailable": "one CPUForceAtlas2::doStep "
@@ -569,7 +772,13 @@ def main():
         elif args.impl == "reference":
             run_reference(args, world, rank)
         else:
-            run_ours(args, world, rank, local)
+            t_start = time.perf_counter()
+            out = run_ours(args, world, rank, local)
+            if (out is not None and world == 1 and args.workload == "rmat20"
+                    and not args.no_extras):
+                extras(args, local, out, t_start)
+            if out is not None:
+                print(json.dumps(out))
     finally:
         if world > 1:
             import torch.distributed as dist

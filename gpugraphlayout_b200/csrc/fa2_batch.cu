@@ -504,7 +504,7 @@ __device__ void phase_traverse(const BatchArgs &A, uint32_t base, uint32_t n, ch
                 const float4 r = nodes[node];
                 const int meta = __float_as_int(r.w);
                 const float dx = px - r.x, dy = py - r.y;
-                const float d2 = dx * dx + dy * dy + A.prm.epssq;
+                const float d2 = sq_dist(dx, dy, A.prm.epssq);
                 // !(d2 < dq): a NaN distance accepts, so the walk still ends
                 if (__all_sync(kFullMask, !(d2 < S.dq[meta_level(meta)]))) {
                     const float c = __fdividef(r.z, d2);

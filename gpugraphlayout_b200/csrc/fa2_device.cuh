@@ -24,6 +24,19 @@ __device__ __forceinline__ float make_meta(uint32_t next, int level) {
 }
 
 
+// Softened squared distance dx^2 + dy^2 + eps of the walk, with every
+// rounding spelled out so that each kernel that restates it gets the same
+// bits whatever the compiler would contract.
+__device__ __forceinline__ float sq_dist(float dx, float dy, float eps) {
+    return __fadd_rn(__fmaf_rn(dx, dx, __fmul_rn(dy, dy)), eps);
+}
+
+// dx^2 + dy^2 with the same spelled-out roundings (the swing and traction
+// terms of the passes that end an iteration).
+__device__ __forceinline__ float sq_norm(float dx, float dy) {
+    return __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
+}
+
 // --------------------------------------------------- shared by the kernels --
 
 // Quadrant digits of (px, py) under the root cell, computed the way

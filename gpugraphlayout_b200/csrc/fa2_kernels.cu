@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
                 const float4 r = __ldg(&nodes[node]);
                 const int meta = __float_as_int(r.w);
                 const float dx = px - r.x, dy = py - r.y;
-                const float d2 = dx * dx + dy * dy + prm.epssq;
+                const float d2 = sq_dist(dx, dy, prm.epssq);
                 // written as !(d2 < dq): a NaN distance accepts, so a warp
                 // with a non-finite lane still ends its walk
                 if (__all_sync(kFull, !(d2 < s_dq[meta_level(meta)]))) {
@@ -272,7 +272,7 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
                 const int lvl = meta_level(meta);
                 const float m = r.z;
                 const float dx = px - r.x, dy = py - r.y;
-                const float d2 = dx * dx + dy * dy + prm.epssq;
+                const float d2 = sq_dist(dx, dy, prm.epssq);
                 if (__all_sync(kFull, !(d2 < s_dq[lvl]))) {
                     const uint32_t next = meta_next(meta);
                     // the loads of the next node (and of this cell's second
@@ -308,9 +308,11 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
                 }
             }
         }
+        // rounded on its own (never fused into the force sum that follows), so
+        // the learned iteration, which stores it, adds the same value
         const float kmi = prm.k_r * me.z;
-        ax *= kmi;
-        ay *= kmi;
+        ax = __fmul_rn(ax, kmi);
+        ay = __fmul_rn(ay, kmi);
         if (LEARN) {
             if (npend) flush();
             if (active) lb.rep[k] = make_float2(ax, ay);
@@ -323,10 +325,10 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
             const float fx = g.x + ax, fy = g.y + ay;
             f[i] = make_float2(fx, fy);
             float dx = fx - fp.x, dy = fy - fp.y;
-            sw = me.z * sqrtf(dx * dx + dy * dy);
+            sw = me.z * sqrtf(sq_norm(dx, dy));
             dx = fx + fp.x;
             dy = fy + fp.y;
-            tr = me.z * (float)(sqrtf(dx * dx + dy * dy) / 2.0);
+            tr = me.z * (float)(sqrtf(sq_norm(dx, dy)) / 2.0);
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -376,7 +378,7 @@ __global__ void __launch_bounds__(kTravThreads) k_count_interactions(
             const float4 r = nodes[node];
             const int meta = __float_as_int(r.w);
             const float dx = px - r.x, dy = py - r.y;
-            const float d2 = dx * dx + dy * dy + prm.epssq;
+            const float d2 = sq_dist(dx, dy, prm.epssq);
             ++steps;
             if (__all_sync(kFull, !(d2 < s_dq[meta_level(meta)]))) {
                 ++acc;
@@ -526,7 +528,7 @@ __global__ void __launch_bounds__(256) k_guard_plain(int n, int ns,
             const float4 r = __ldg(&nodes[node]);
             const int meta = __float_as_int(r.w);
             const float dx = px - r.x, dy = py - r.y;
-            const float d2 = dx * dx + dy * dy + prm.epssq;
+            const float d2 = sq_dist(dx, dy, prm.epssq);
             if (__all_sync(kFull, !(d2 < s_dq[meta_level(meta)]))) {
                 const float c = __fdividef(r.z, d2);
                 ax = fmaf(dx, c, ax);

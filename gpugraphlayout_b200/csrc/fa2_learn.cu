@@ -438,7 +438,7 @@ __global__ void __launch_bounds__(256) k_learn_targets(
         }
         // the walk's term for this cell (fa2_kernels.cu, k_traverse)
         const float dxf = me.x - cell.x, dyf = me.y - cell.y;
-        const float d2f = dxf * dxf + dyf * dyf + prm.epssq;
+        const float d2f = sq_dist(dxf, dyf, prm.epssq);
         float bx, by;
         if (QUAD) {
             const float inv = __fdividef(1.0f, d2f);
@@ -694,10 +694,10 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_learn_tai
             fy = fmaf(kmi, cg.y, fy);
             f[i] = make_float2(fx, fy);
             float dx = fx - fp.x, dy = fy - fp.y;
-            sw = mi * sqrtf(dx * dx + dy * dy);
+            sw = mi * sqrtf(sq_norm(dx, dy));
             dx = fx + fp.x;
             dy = fy + fp.y;
-            tr = mi * (float)(sqrtf(dx * dx + dy * dy) / 2.0);
+            tr = mi * (float)(sqrtf(sq_norm(dx, dy)) / 2.0);
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {

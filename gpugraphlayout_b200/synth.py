@@ -26,28 +26,53 @@ def _unique(x: np.ndarray) -> np.ndarray:
     return y[np.concatenate(([True], y[1:] != y[:-1]))]
 
 
+def _rmat_chunk_keys(args):
+    """Keys (lo << scale | hi) of draws [start, start + m) of the R-MAT stream:
+    the generator jumps ahead to the chunk's first random number (each level
+    of a chunk takes m numbers, so draw block `start` begins at number
+    start * scale)."""
+    scale, start, m, a, b, c, seed = args
+    bg = np.random.PCG64(seed)
+    bg.advance(start * scale)
+    rng = np.random.Generator(bg)
+    src = np.zeros(m, np.int64)
+    dst = np.zeros(m, np.int64)
+    for lvl in range(scale):
+        r = rng.random(m)
+        sbit = r >= a + b
+        dbit = ((r >= a) & (r < a + b)) | (r >= a + b + c)
+        src |= sbit.astype(np.int64) << lvl
+        dst |= dbit.astype(np.int64) << lvl
+    keep = src != dst
+    src, dst = src[keep], dst[keep]
+    lo = np.minimum(src, dst)
+    hi = np.maximum(src, dst)
+    return _unique((lo << scale) | hi)
+
+
 def rmat_edges(scale: int, n_draws: int, a: float = 0.57, b: float = 0.19,
-               c: float = 0.19, seed: int = 0, chunk: int = 1 << 22):
+               c: float = 0.19, seed: int = 0, chunk: int = 1 << 22,
+               workers: int | None = None):
     """R-MAT draws over 2**scale ids: per level, quadrant (0,0) w.p. a, (0,1) b,
     (1,0) c, (1,1) d = 1-a-b-c.  Returns the unique undirected (lo, hi) pairs
-    sorted ascending, self-loops dropped."""
-    rng = np.random.default_rng(seed)
-    keys = []
-    for start in range(0, n_draws, chunk):
-        m = min(chunk, n_draws - start)
-        src = np.zeros(m, np.int64)
-        dst = np.zeros(m, np.int64)
-        for lvl in range(scale):
-            r = rng.random(m)
-            sbit = r >= a + b
-            dbit = ((r >= a) & (r < a + b)) | (r >= a + b + c)
-            src |= sbit.astype(np.int64) << lvl
-            dst |= dbit.astype(np.int64) << lvl
-        keep = src != dst
-        src, dst = src[keep], dst[keep]
-        lo = np.minimum(src, dst)
-        hi = np.maximum(src, dst)
-        keys.append(_unique((lo << scale) | hi))
+    sorted ascending, self-loops dropped.  The draws come from one PCG64
+    stream seeded with `seed`, in chunks of `chunk` draws level by level;
+    chunks are generated by `workers` spawned processes (default: the CPU
+    count when there are more than 8 chunks), each jumping the stream ahead to
+    its chunk, so the result does not depend on the number of workers."""
+    import os
+    jobs = [(scale, start, min(chunk, n_draws - start), a, b, c, seed)
+            for start in range(0, n_draws, chunk)]
+    if workers is None:
+        workers = min(32, os.cpu_count() or 1) if len(jobs) > 8 else 1
+    if workers <= 1:
+        keys = [_rmat_chunk_keys(j) for j in jobs]
+    else:
+        import multiprocessing as mp
+        from concurrent.futures import ProcessPoolExecutor
+        with ProcessPoolExecutor(min(workers, len(jobs)),
+                                 mp_context=mp.get_context("spawn")) as ex:
+            keys = list(ex.map(_rmat_chunk_keys, jobs))
     k = _unique(np.concatenate(keys)) if len(keys) > 1 else keys[0]
     lo = (k >> scale).astype(np.uint32)
     hi = (k & ((1 << scale) - 1)).astype(np.uint32)

@@ -21,26 +21,13 @@ TOL_STRESS = 0.05
 
 
 def _edge_lengths(xy, g):
-    d = xy[g.sources] - xy[g.targets]
-    return np.sqrt((d.astype(np.float64) ** 2).sum(1))
+    from gpugraphlayout_b200.layout_stats import edge_lengths
+    return edge_lengths(xy, g.sources, g.targets)
 
 
 def _stress(xy, g, n_src=24, seed=0):
-    """Kamada-Kawai stress over all pairs (source, v) from a few BFS sources,
-    at the layout scale that minimises it: sum((a |p_u - p_v| - d)^2 / d^2)
-    / pairs, with a = sum(|p|/d) / sum(|p|^2/d^2)."""
-    from scipy.sparse import coo_matrix
-    from scipy.sparse.csgraph import shortest_path
-    n = len(xy)
-    a = coo_matrix((np.ones(len(g.sources)), (g.sources, g.targets)), shape=(n, n)).tocsr()
-    src = np.random.default_rng(seed).choice(n, n_src, replace=False)
-    dist = shortest_path(a, directed=False, unweighted=True, indices=src)
-    ok = np.isfinite(dist) & (dist > 0)
-    rows, cols = np.nonzero(ok)
-    d = dist[rows, cols]
-    e = np.sqrt(((xy[src[rows]].astype(np.float64) - xy[cols]) ** 2).sum(1))
-    scale = (e / d).sum() / ((e / d) ** 2).sum()
-    return float((((scale * e - d) / d) ** 2).mean())
+    from gpugraphlayout_b200.layout_stats import stress
+    return stress(xy, g.sources, g.targets, n_src, seed)
 
 
 @pytest.mark.parametrize("sg,k_r", [(False, 80.0), (True, 10.0)])
