@@ -137,7 +137,10 @@ int ensure_quad_buffers(fa2_ctx *c) {
 int ensure_learn_buffers(fa2_ctx *c) {
     LearnBuffers &lb = c->lb;
     const size_t groups = ((size_t)c->n + 31) / 32;
-    const uint64_t cap = std::min<uint64_t>(32ull * c->n + 4096, 0xFFFFFFFFull);
+    // 32 pairs per body on average (a group accepts a few hundred cells at
+    // theta >= 1), in kPairSegments segments with room for imbalance
+    const uint64_t seg = std::min<uint64_t>((32ull * c->n) / kPairSegments + 4096, 0x7FFFFFFFull);
+    const uint64_t cap = seg * kPairSegments;
     int s = FA2_OK;
     if ((!lb.pairs && (s = dalloc(c, &lb.pairs, (size_t)cap))) ||
         (!lb.ggeo && (s = dalloc(c, &lb.ggeo, 2 * groups))) ||
@@ -145,7 +148,7 @@ int ensure_learn_buffers(fa2_ctx *c) {
         (!lb.corr && (s = dalloc(c, &lb.corr, groups))) ||
         (!c->d_mlp && (s = dalloc(c, &c->d_mlp, 1))))
         return s;
-    lb.pair_cap = (uint32_t)cap;
+    lb.seg_cap = (uint32_t)seg;
     lb.mlp = c->d_mlp;
     return FA2_OK;
 }
@@ -1155,6 +1158,7 @@ int fa2_set_learned_correction(fa2_ctx *c, const fa2_mlp *mlp) {
         return FA2_OK;
     }
     if (!mlp_is_finite(*mlp)) return FA2_ERR_INVALID_ARGUMENT;
+    mlp_blocks_per_sm();  // the launch shape, settled outside any graph capture
     int s = ensure_quad_buffers(c);
     if (!s) s = ensure_learn_buffers(c);
     if (s) return s;
@@ -1289,7 +1293,7 @@ int fa2_learn_collect(fa2_learn_set *set, fa2_ctx *c, float theta, int32_t multi
     CK(cudaStreamSynchronize(c->sA));
     int s = ensure_quad_buffers(c);
     if (!s) s = ensure_learn_buffers(c);
-    if (!s) s = set_staging(set, c->lb.pair_cap);
+    if (!s) s = set_staging(set, (int64_t)c->lb.seg_cap * kPairSegments);
     if (s) return s;
     Params kp = c->kp;
     kp.itolsq = 1.0f / (theta * theta);

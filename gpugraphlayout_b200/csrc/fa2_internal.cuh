@@ -57,8 +57,8 @@ struct IterCounters {
     unsigned trav_done;
     unsigned disp_done;
     unsigned mom_ticket;
-    unsigned pair_count;  // (group, cell) pairs of a learned iteration's walk
     unsigned pad[1];
+    unsigned pair_count[16];  // (group, cell) pairs of a learned walk, per pair segment
     unsigned hist[8][256];  // per-pass digit histograms of the sort keys
 };
 

@@ -228,15 +228,19 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
                 lb.ggeo[2 * w + 1] = make_float4(t1 / cnt, t2 / cnt, 0.0f, 0.0f);
             }
         }
-        // LEARN: the pending cells to the pair list, one atomic per flush
+        // LEARN: the pending cells to this warp's segment of the pair list,
+        // one atomic per flush
         auto flush = [&]() {
             __syncwarp();
+            const uint32_t seg = (blockIdx.x * (kTravThreads / kWarp) + (threadIdx.x >> 5)) %
+                                 (uint32_t)kPairSegments;
             uint32_t base = 0;
-            if (lane == 0) base = atomicAdd(&ctr->pair_count, (unsigned)npend);
+            if (lane == 0) base = atomicAdd(&ctr->pair_count[seg], (unsigned)npend);
             base = __shfl_sync(kFull, base, 0);
-            if (lane < npend && base + lane < lb.pair_cap)
-                lb.pairs[base + lane] = make_uint2((uint32_t)w, my_pairs[lane]);
-            if (lane == 0 && base + (uint32_t)npend > lb.pair_cap) atomicOr(&st->err, kErrPairs);
+            if (lane < npend && base + lane < lb.seg_cap)
+                lb.pairs[(size_t)seg * lb.seg_cap + base + lane] =
+                    make_uint2((uint32_t)w, my_pairs[lane]);
+            if (lane == 0 && base + (uint32_t)npend > lb.seg_cap) atomicOr(&st->err, kErrPairs);
             __syncwarp();
             npend = 0;
         };

@@ -30,10 +30,13 @@ constexpr unsigned kFull = kFullMask;
 //   4,5 b2 / d^2           the group's complex second moment about g, turned
 //   6  |a2| / (M h^2)      how far the cell's mass sits from its centre
 //   7  log2(d^2 / dq) / 8  margin over the walk's acceptance threshold dq
-//   8  level / 32
-//   9  log2(M) / 16
+//   8  (h / d)^2
+//   9  (s / d)^2
 //   10 s / h
 //   11 bodies in the group / 32
+// Every feature is a ratio of lengths (or of moments to the matching power
+// of a length), so a model trained on one graph size serves another: the
+// tree level and the cell mass themselves are not features.
 // sig = M / d scales the outputs back, (c, s) is the turn.  Returns false
 // when the pair is not corrected: a group spread beyond kLearnMaxSpread of
 // the distance, or a degenerate cell or distance.
@@ -71,8 +74,8 @@ __device__ __forceinline__ bool pair_features(float4 cell, float2 a2, float4 g0,
     f[5] = b2i / d2;
     f[6] = sqrtf(a2.x * a2.x + a2.y * a2.y) / (M * h * h);
     f[7] = log2f(d2 / dq) * 0.125f;
-    f[8] = (float)lvl * (1.0f / 32.0f);
-    f[9] = log2f(M) * (1.0f / 16.0f);
+    f[8] = f[0] * f[0];
+    f[9] = f[1] * f[1];
     f[10] = spread / h;
     f[11] = g0.w * (1.0f / 32.0f);
     sig = M / d;
@@ -207,6 +210,59 @@ __device__ __forceinline__ void put_chunk(uint8_t *tile, int r, int chunk, int k
     *reinterpret_cast<uint4 *>(tile + operand_offset(r, chunk * 8, kchunks)) = q;
 }
 
+// Row r of the concatenated pair segments, as an index into the pair list:
+// pre[s] is the number of rows before segment s (pre[kPairSegments] all).
+__device__ __forceinline__ size_t pair_index(int64_t r, const uint32_t *pre, uint32_t seg_cap) {
+    int s = 0;
+#pragma unroll
+    for (int q = 1; q < kPairSegments; ++q) s += (r >= (int64_t)pre[q]) ? 1 : 0;
+    return (size_t)s * seg_cap + (size_t)(r - (int64_t)pre[s]);
+}
+
+// The prefix of the segments' fill (each at most seg_cap), in shared memory.
+__device__ __forceinline__ void pair_prefix(const IterCounters *ctr, uint32_t seg_cap,
+                                            uint32_t *pre) {
+    if (threadIdx.x == 0) {
+        uint32_t acc = 0;
+        for (int q = 0; q < kPairSegments; ++q) {
+            pre[q] = acc;
+            acc += min(ctr->pair_count[q], seg_cap);
+        }
+        pre[kPairSegments] = acc;
+    }
+    __syncthreads();
+}
+
+// What one row of a tile needs: a pair, its cell, the cell's second moment
+// and the group's geometry (PAIRS), or the row's features.
+struct RowInputs {
+    uint2 pair;
+    float4 cell, g0, g1;
+    float2 a2;
+    float x[kLearnIn];
+};
+
+template <bool PAIRS>
+__device__ __forceinline__ void load_row(RowInputs &r, int64_t row, int64_t rows,
+                                         const uint32_t *pre, uint32_t seg_cap,
+                                         const uint2 *__restrict pairs,
+                                         const float4 *__restrict nodes,
+                                         const float2 *__restrict quad,
+                                         const float4 *__restrict ggeo,
+                                         const float *__restrict features) {
+    if (row >= rows) return;
+    if (PAIRS) {
+        r.pair = pairs[pair_index(row, pre, seg_cap)];
+        r.cell = nodes[r.pair.y];
+        r.a2 = quad[r.pair.y];
+        r.g0 = ggeo[2 * r.pair.x];
+        r.g1 = ggeo[2 * r.pair.x + 1];
+    } else {
+#pragma unroll
+        for (int q = 0; q < kLearnIn; ++q) r.x[q] = features[row * kLearnIn + q];
+    }
+}
+
 // The MLP over rows of 12 features, 128 rows per tile and thread block (one
 // row per thread).  Layer 1 (K = 16, the 12 features padded with zeros) and
 // layer 2 (K = 64) are 128 x 64 tcgen05 MMAs with BF16 operands from shared
@@ -224,14 +280,16 @@ __device__ __forceinline__ void put_chunk(uint8_t *tile, int r, int chunk, int k
 // memory is released on every path.
 template <bool PAIRS>
 __global__ void __launch_bounds__(kMlpThreads) k_learn_mlp(
-    const uint2 *__restrict pairs, const IterCounters *ctr, uint32_t pair_cap,
+    const uint2 *__restrict pairs, const IterCounters *ctr, uint32_t seg_cap,
     const float4 *__restrict nodes, const float2 *__restrict quad, const float4 *__restrict ggeo,
     const DevState *st, Params prm, float2 *__restrict corr, const float *__restrict features,
     int64_t nrows, float2 *__restrict out, const MlpDevice *__restrict mlp, int *err) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     MlpSmem &S = *reinterpret_cast<MlpSmem *>(smem_raw);
+    __shared__ uint32_t s_pre[kPairSegments + 1];
     if (PAIRS && (st->err || st->poison)) return;
     const int t = threadIdx.x, warp = t >> 5;
+    if (PAIRS) pair_prefix(ctr, seg_cap, s_pre);
     {
         const int4 *src = reinterpret_cast<const int4 *>(mlp);
         int4 *dst = reinterpret_cast<int4 *>(&S.w);
@@ -262,35 +320,40 @@ __global__ void __launch_bounds__(kMlpThreads) k_learn_mlp(
     // this warp's 32 TMEM lanes (warp q of the block reads lanes 32q..32q+31)
     const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
     const float radius = PAIRS ? st->trav_radius : 0.0f;
-    const int64_t rows = PAIRS ? (int64_t)min(ctr->pair_count, pair_cap) : nrows;
+    const int64_t rows = PAIRS ? (int64_t)s_pre[kPairSegments] : nrows;
+    const int lane = t & 31;
     uint32_t phase = 0;
     bool bad = false;  // a wait gave up (the same for every thread)
-    for (int64_t base = (int64_t)blockIdx.x * kMlpRows; base < rows;
-         base += (int64_t)gridDim.x * kMlpRows) {
+    // The inputs of this thread's row of the next tile are loaded while the
+    // tensor cores work on the current one.
+    RowInputs next;
+    int64_t base = (int64_t)blockIdx.x * kMlpRows;
+    if (base < rows) load_row<PAIRS>(next, base + t, rows, s_pre, seg_cap, pairs, nodes, quad, ggeo, features);
+    for (; base < rows; base += (int64_t)gridDim.x * kMlpRows) {
         const int64_t row = base + t;
+        const RowInputs in = next;
         float f[kLearnInPad];
         float sig = 0.0f, c = 1.0f, s = 0.0f;
-        uint32_t grp = 0;
         bool use = false;
 #pragma unroll
         for (int q = kLearnIn; q < kLearnInPad; ++q) f[q] = 0.0f;
-        if (row < rows) {
-            if (PAIRS) {
-                const uint2 pr = pairs[row];
-                grp = pr.x;
-                float fv[kLearnIn];
-                use = pair_features(nodes[pr.y], quad[pr.y], ggeo[2 * pr.x], ggeo[2 * pr.x + 1],
-                                    radius, prm.itolsq, prm.epssq, fv, sig, c, s);
+        {
+            float fv[kLearnIn];
+            if (row < rows) {
+                if (PAIRS) {
+                    use = pair_features(in.cell, in.a2, in.g0, in.g1, radius, prm.itolsq,
+                                        prm.epssq, fv, sig, c, s);
+                } else {
 #pragma unroll
-                for (int q = 0; q < kLearnIn; ++q) f[q] = fv[q];
+                    for (int q = 0; q < kLearnIn; ++q) fv[q] = in.x[q];
+                    use = true;
+                }
             } else {
 #pragma unroll
-                for (int q = 0; q < kLearnIn; ++q) f[q] = features[row * kLearnIn + q];
-                use = true;
+                for (int q = 0; q < kLearnIn; ++q) fv[q] = 0.0f;
             }
-        } else {
 #pragma unroll
-            for (int q = 0; q < kLearnIn; ++q) f[q] = 0.0f;
+            for (int q = 0; q < kLearnIn; ++q) f[q] = fv[q];
         }
         put_chunk(S.a, t, 0, 2, f);
         put_chunk(S.a, t, 1, 2, f + 8);
@@ -301,6 +364,10 @@ __global__ void __launch_bounds__(kMlpThreads) k_learn_mlp(
             tc_fence_after();
             mma_bf16(tmem, da, dw1, kIdesc, 0);
             mma_commit(mbar);
+        }
+        {
+            const int64_t nb = base + (int64_t)gridDim.x * kMlpRows;
+            if (nb < rows) load_row<PAIRS>(next, nb + t, rows, s_pre, seg_cap, pairs, nodes, quad, ggeo, features);
         }
         bool ok = mbar_wait(mbar, phase);
         phase ^= 1u;
@@ -354,15 +421,29 @@ __global__ void __launch_bounds__(kMlpThreads) k_learn_mlp(
         }
         // the next tile's first MMA overwrites the columns just read
         tc_fence_before();
-        if (row < rows) {
-            if (PAIRS) {
-                if (use) {
-                    atomicAdd(&corr[grp].x, sig * (c * y0 - s * y1));
-                    atomicAdd(&corr[grp].y, sig * (s * y0 + c * y1));
+        if (PAIRS) {
+            // Rows of one group are adjacent (the walk writes a group's cells
+            // in runs): sum each run within the warp, one atomic per run.
+            const uint32_t grp = row < rows ? in.pair.x : 0xFFFFFFFFu;
+            float cx = use ? sig * (c * y0 - s * y1) : 0.0f;
+            float cy = use ? sig * (s * y0 + c * y1) : 0.0f;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const float ox = __shfl_down_sync(kFull, cx, o);
+                const float oy = __shfl_down_sync(kFull, cy, o);
+                const uint32_t og = __shfl_down_sync(kFull, grp, o);
+                if (lane + o < 32 && og == grp) {
+                    cx += ox;
+                    cy += oy;
                 }
-            } else {
-                out[row] = make_float2(y0, y1);
             }
+            const uint32_t prev = __shfl_up_sync(kFull, grp, 1);
+            if (grp != 0xFFFFFFFFu && (lane == 0 || prev != grp)) {
+                atomicAdd(&corr[grp].x, cx);
+                atomicAdd(&corr[grp].y, cy);
+            }
+        } else if (row < rows) {
+            out[row] = make_float2(y0, y1);
         }
     }
     if (bad) {
@@ -394,20 +475,22 @@ __global__ void __launch_bounds__(kMlpThreads) k_learn_mlp(
 // order.
 template <bool QUAD>
 __global__ void __launch_bounds__(256) k_learn_targets(
-    int n, const uint2 *__restrict pairs, const IterCounters *ctr, uint32_t pair_cap,
+    int n, const uint2 *__restrict pairs, const IterCounters *ctr, uint32_t seg_cap,
     const float4 *__restrict nodes, const float2 *__restrict quad,
     const uint32_t *__restrict owner, const uint32_t *__restrict body_node,
     const float4 *__restrict ggeo, const DevState *st, Params prm, float *__restrict features,
     float2 *__restrict targets, float *__restrict weights, uint64_t *__restrict keys,
     unsigned long long *count, uint64_t cap) {
+    __shared__ uint32_t s_pre[kPairSegments + 1];
     if (st->err || st->poison) return;
+    pair_prefix(ctr, seg_cap, s_pre);
     const int lane = threadIdx.x & 31;
-    const int64_t rows = (int64_t)min(ctr->pair_count, pair_cap);
+    const int64_t rows = (int64_t)s_pre[kPairSegments];
     const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
     const float radius = st->trav_radius;
     const double eps = (double)prm.epssq;
     for (int64_t p = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < rows; p += nw) {
-        const uint2 pr = pairs[p];
+        const uint2 pr = pairs[pair_index(p, s_pre, seg_cap)];
         const uint32_t w = pr.x, node = pr.y;
         const float4 cell = nodes[node];
         const float2 a2 = quad[node];
@@ -719,20 +802,26 @@ int mlp_blocks_per_sm() {
     static int cached = 0;
     if (cached) return cached;
     const int bytes = mlp_smem_bytes();
-    cudaFuncSetAttribute(k_learn_mlp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    cudaFuncSetAttribute(k_learn_mlp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_learn_mlp<true>, kMlpThreads, bytes);
+    if (cudaFuncSetAttribute(k_learn_mlp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             bytes) != cudaSuccess ||
+        cudaFuncSetAttribute(k_learn_mlp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             bytes) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_learn_mlp<true>, kMlpThreads,
+                                                      bytes) != cudaSuccess ||
+        nb < 1) {
+        cudaGetLastError();
+        return 1;  // not kept: the next call asks again
+    }
     // every resident block holds kMlpTmemCols of the SM's 512 TMEM columns
-    nb = nb < 1 ? 1 : (nb > (int)(512 / kMlpTmemCols) ? (int)(512 / kMlpTmemCols) : nb);
-    cached = nb;
-    return nb;
+    cached = nb > (int)(512 / kMlpTmemCols) ? (int)(512 / kMlpTmemCols) : nb;
+    return cached;
 }
 
 void launch_learn_mlp(const Buffers &b, const Params &p, const LearnBuffers &lb, int nsm,
                       cudaStream_t s) {
     k_learn_mlp<true><<<nsm * mlp_blocks_per_sm(), kMlpThreads, mlp_smem_bytes(), s>>>(
-        lb.pairs, b.ctr, lb.pair_cap, b.nodes, b.quad, lb.ggeo, b.st, p, lb.corr, nullptr, 0,
+        lb.pairs, b.ctr, lb.seg_cap, b.nodes, b.quad, lb.ggeo, b.st, p, lb.corr, nullptr, 0,
         nullptr, lb.mlp, &b.st->err);
 }
 
@@ -760,11 +849,11 @@ void launch_learn_targets(const Buffers &b, const Params &p, const LearnBuffers 
                           unsigned long long *count, uint64_t cap, int nsm, cudaStream_t s) {
     if (p.multipole >= 2)
         k_learn_targets<true><<<nsm * 8, 256, 0, s>>>(
-            b.n, lb.pairs, b.ctr, lb.pair_cap, b.nodes, b.quad, b.owner, b.body_node, lb.ggeo,
+            b.n, lb.pairs, b.ctr, lb.seg_cap, b.nodes, b.quad, b.owner, b.body_node, lb.ggeo,
             b.st, p, features, targets, weights, keys, count, cap);
     else
         k_learn_targets<false><<<nsm * 8, 256, 0, s>>>(
-            b.n, lb.pairs, b.ctr, lb.pair_cap, b.nodes, b.quad, b.owner, b.body_node, lb.ggeo,
+            b.n, lb.pairs, b.ctr, lb.seg_cap, b.nodes, b.quad, b.owner, b.body_node, lb.ggeo,
             b.st, p, features, targets, weights, keys, count, cap);
 }
 

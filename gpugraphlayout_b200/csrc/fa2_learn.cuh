@@ -51,10 +51,16 @@ __host__ __device__ constexpr uint32_t operand_offset(uint32_t r, uint32_t k, ui
     return (r >> 3) * (kchunks * 128u) + (k >> 3) * 128u + (r & 7u) * 16u + (k & 7u) * 2u;
 }
 
+// The pair list is split into kPairSegments segments of seg_cap pairs, each
+// with its own counter (IterCounters::pair_count): a warp appends to the
+// segment of its warp index, so the warps' reservations spread over 16
+// counters instead of queueing on one.
+constexpr int kPairSegments = 16;
+
 // What the walk of a learned iteration leaves for the MLP and the tail.
 struct LearnBuffers {
-    uint2 *pairs;         // (group, node) of every cell a group accepted
-    uint32_t pair_cap;
+    uint2 *pairs;         // (group, node) of every cell a group accepted, by segment
+    uint32_t seg_cap;     // pairs per segment
     float4 *ggeo;         // 2 per group: {cx, cy, trace, lanes}, {re, im, 0, 0}
     float2 *rep;          // per sorted body: the walk's repulsion (k_r m_i applied)
     float2 *corr;         // per group: sum of its pairs' corrections (per unit k_r m_i)
