@@ -30,7 +30,7 @@ EXPORTS = (
     "fa2_status_string", "fa2_version",
     "fa2_mlp_init", "fa2_set_learned_correction", "fa2_mlp_forward", "fa2_mlp_train_step",
     "fa2_learn_set_create", "fa2_learn_set_destroy", "fa2_learn_set_size", "fa2_learn_collect",
-    "fa2_learn_set_read", "fa2_learn_fit",
+    "fa2_learn_set_read", "fa2_learn_fit", "fa2_mlp_launch_shape",
 )
 
 FA2_OK = 0
@@ -64,7 +64,7 @@ class Stats(C.Structure):
                 ("speed_efficiency", C.c_float), ("radius", C.c_float),
                 ("root_x", C.c_float), ("root_y", C.c_float),
                 ("interactions", C.c_uint64), ("visits", C.c_uint64),
-                ("sort_passes", C.c_int32)]
+                ("sort_passes", C.c_int32), ("learned_pairs", C.c_uint64)]
 
 
 MLP_IN, MLP_HIDDEN, MLP_OUT = 12, 64, 2  # include/fa2b200.h
@@ -167,6 +167,7 @@ def lib():
     L.fa2_mlp_init.argtypes = [mp, C.c_uint32]
     L.fa2_set_learned_correction.argtypes = [vp, mp]
     L.fa2_mlp_forward.argtypes = [C.c_int32, mp, vp, C.c_int64, vp]
+    L.fa2_mlp_launch_shape.argtypes = [C.c_int32, vp, vp]
     L.fa2_mlp_train_step.argtypes = [C.c_int32, mp, mp, mp, C.c_int32, C.c_float, vp, vp, vp,
                                      C.c_int32, f32p]
     L.fa2_learn_set_create.restype = vp

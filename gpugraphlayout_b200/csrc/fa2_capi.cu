@@ -949,6 +949,14 @@ int fa2_get_stats(fa2_ctx *c, fa2_stats *out) {
     out->interactions = st.interactions;
     out->visits = st.visits;
     out->sort_passes = 8 - c->b.sort_first;
+    if (c->learn_on && c->n) {
+        unsigned counts[kPairSegments];
+        CK(cudaMemcpyAsync(counts, c->b.ctr->pair_count, sizeof(counts), cudaMemcpyDeviceToHost,
+                           c->sA));
+        CK(cudaStreamSynchronize(c->sA));
+        for (int q = 0; q < kPairSegments; ++q)
+            out->learned_pairs += std::min(counts[q], c->lb.seg_cap);
+    }
     return FA2_OK;
 }
 
@@ -1170,6 +1178,16 @@ int fa2_set_learned_correction(fa2_ctx *c, const fa2_mlp *mlp) {
         c->learn_on = true;
         drop_graphs(c);  // the learned walk, MLP and tail are captured anew
     }
+    return FA2_OK;
+}
+
+int fa2_mlp_launch_shape(int32_t device, int32_t *blocks_per_sm, int32_t *smem_bytes) {
+    int nsm = 0;
+    int s = use_device(device, &nsm);
+    if (s) return s;
+    const int nb = mlp_blocks_per_sm();
+    if (blocks_per_sm) *blocks_per_sm = nb;
+    if (smem_bytes) *smem_bytes = mlp_smem_bytes_host();
     return FA2_OK;
 }
 

@@ -6,6 +6,7 @@
 // point mass (src/RPBHKernels.cu:656-668), which is the term corrected here.
 #include <cuda_bf16.h>
 #include <stdint.h>
+#include <stdio.h>
 
 #include <cmath>
 
@@ -798,6 +799,8 @@ int mlp_smem_bytes() { return (int)sizeof(MlpSmem); }
 
 }  // namespace
 
+int mlp_smem_bytes_host() { return mlp_smem_bytes(); }
+
 int mlp_blocks_per_sm() {
     static int cached = 0;
     if (cached) return cached;
@@ -810,7 +813,9 @@ int mlp_blocks_per_sm() {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_learn_mlp<true>, kMlpThreads,
                                                       bytes) != cudaSuccess ||
         nb < 1) {
-        cudaGetLastError();
+        const cudaError_t e = cudaGetLastError();
+        fprintf(stderr, "fa2: MLP occupancy query failed (%s, %d blocks); 1 block per SM\n",
+                cudaGetErrorString(e), nb);
         return 1;  // not kept: the next call asks again
     }
     // every resident block holds kMlpTmemCols of the SM's 512 TMEM columns

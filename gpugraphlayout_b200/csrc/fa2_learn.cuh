@@ -112,5 +112,6 @@ void launch_learn_train_step(float *params, float *m, float *v, int step, float 
 void launch_learn_weight_sum(const float *weights, uint64_t n, double *out, cudaStream_t s);
 
 int mlp_blocks_per_sm();
+int mlp_smem_bytes_host();
 
 }  // namespace fa2

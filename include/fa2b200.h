@@ -147,6 +147,9 @@ typedef struct {
                                    after a tree no deeper than level 22, 7 after one no
                                    deeper than 26 (runs of keys equal in the sorted
                                    top bits are then ordered by a fix-up pass) */
+    uint64_t learned_pairs;     /* (group, cell) pairs the last learned iteration's walk
+                                   collected for the MLP (0 without the learned
+                                   correction; see fa2_set_learned_correction) */
 } fa2_stats;
 
 int fa2_get_stats(fa2_ctx *ctx, fa2_stats *out);
@@ -267,6 +270,11 @@ void fa2_mlp_init(fa2_mlp *mlp, uint32_t seed);
  * checks the corrected repulsion and, on a fallback, also turns the
  * correction off. */
 int fa2_set_learned_correction(fa2_ctx *ctx, const fa2_mlp *mlp);
+
+/* Launch shape of the MLP kernel on `device`: thread blocks per SM (each a
+ * 128-row tile loop holding 64 tensor-memory columns) and dynamic shared
+ * memory per block. */
+int fa2_mlp_launch_shape(int32_t device, int32_t *blocks_per_sm, int32_t *smem_bytes);
 
 /* The inference kernel alone: out[2 r], out[2 r + 1] = MLP(features[12 r ..
  * 12 r + 11]) for n rows (host arrays), on CUDA device `device`. */
