@@ -8,6 +8,7 @@
 #include <stdint.h>
 #include <stdio.h>
 
+#include <algorithm>
 #include <cmath>
 
 #include "fa2_device.cuh"
@@ -801,25 +802,36 @@ int mlp_smem_bytes() { return (int)sizeof(MlpSmem); }
 
 int mlp_smem_bytes_host() { return mlp_smem_bytes(); }
 
+// Blocks per SM of the MLP kernel, from its registers and shared memory and
+// the SM's 512 tensor-memory columns (64 per block).  The runtime's occupancy
+// query answers 1 for this kernel (it allocates tensor memory), so the limits
+// are taken from the kernel's attributes and the device's properties.
 int mlp_blocks_per_sm() {
     static int cached = 0;
     if (cached) return cached;
     const int bytes = mlp_smem_bytes();
-    int nb = 0;
+    int dev = 0;
+    cudaFuncAttributes fa;
+    cudaDeviceProp dp;
     if (cudaFuncSetAttribute(k_learn_mlp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              bytes) != cudaSuccess ||
         cudaFuncSetAttribute(k_learn_mlp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              bytes) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_learn_mlp<true>, kMlpThreads,
-                                                      bytes) != cudaSuccess ||
-        nb < 1) {
+        cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&dp, dev) != cudaSuccess ||
+        cudaFuncGetAttributes(&fa, k_learn_mlp<true>) != cudaSuccess) {
         const cudaError_t e = cudaGetLastError();
-        fprintf(stderr, "fa2: MLP occupancy query failed (%s, %d blocks); 1 block per SM\n",
-                cudaGetErrorString(e), nb);
+        fprintf(stderr, "fa2: MLP launch shape query failed (%s); 1 block per SM\n",
+                cudaGetErrorString(e));
         return 1;  // not kept: the next call asks again
     }
-    // every resident block holds kMlpTmemCols of the SM's 512 TMEM columns
-    cached = nb > (int)(512 / kMlpTmemCols) ? (int)(512 / kMlpTmemCols) : nb;
+    // per block: its shared memory plus the 1 KB the system reserves
+    const size_t per_block = (size_t)bytes + fa.sharedSizeBytes + dp.reservedSharedMemPerBlock;
+    int nb = (int)(dp.sharedMemPerMultiprocessor / per_block);
+    const int regs = fa.numRegs * kMlpThreads;
+    if (regs > 0) nb = std::min(nb, dp.regsPerMultiprocessor / regs);
+    nb = std::min(nb, dp.maxThreadsPerMultiProcessor / kMlpThreads);
+    nb = std::min(nb, (int)(512 / kMlpTmemCols));
+    cached = std::max(nb, 1);
     return cached;
 }
 
