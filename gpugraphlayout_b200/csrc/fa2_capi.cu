@@ -568,14 +568,19 @@ bool mlp_is_finite(const fa2_mlp &m) {
 void mlp_to_device(const fa2_mlp &m, MlpDevice &d) {
     memset(&d, 0, sizeof(d));
     for (int j = 0; j < kLearnHidden; ++j) {
-        for (int k = 0; k < kLearnInPad; ++k)
-            d.w1[operand_offset(j, k, kLearnInPad / 8) / 2] =
-                k < kLearnIn ? bf16_bits(m.w1[j * kLearnIn + k]) : (uint16_t)0;
+        for (int k = 0; k < kLearnInPad; ++k) {
+            uint16_t v = 0;
+            if (k < kLearnIn) v = bf16_bits(m.w1[j * kLearnIn + k]);
+            // b1 = hi + lo in BF16, against the features' two columns of ones
+            if (k == kBiasColHi) v = bf16_bits(m.b1[j]);
+            if (k == kBiasColLo) v = bf16_bits(m.b1[j] - bf16_value(m.b1[j]));
+            d.w1[operand_offset(j, k, kLearnInPad / 8) / 2] = v;
+        }
         for (int k = 0; k < kLearnHidden; ++k)
             d.w2[operand_offset(j, k, kLearnHidden / 8) / 2] = bf16_bits(m.w2[j * kLearnHidden + k]);
-        d.b1[j] = m.b1[j];
+        for (int o = 0; o < kLearnOut; ++o)
+            d.w3[operand_offset(o, j, kLearnHidden / 8) / 2] = bf16_bits(m.w3[o * kLearnHidden + j]);
         d.b2[j] = m.b2[j];
-        d.w3[j] = make_float2(bf16_value(m.w3[j]), bf16_value(m.w3[kLearnHidden + j]));
     }
     d.b3[0] = m.b3[0];
     d.b3[1] = m.b3[1];

@@ -885,8 +885,10 @@ int traverse_blocks_per_sm() {
     // the walk lives on L1 hits: give L1 the most of the SM's on-chip memory
     cudaFuncSetAttribute(k_traverse<false, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
     cudaFuncSetAttribute(k_traverse<true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-    cudaFuncSetAttribute(k_traverse<false, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-    cudaFuncSetAttribute(k_traverse<true, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+    // the learned walk keeps 4 KB of pending pairs per block: the smallest
+    // shared-memory share that holds two blocks
+    cudaFuncSetAttribute(k_traverse<false, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 8);
+    cudaFuncSetAttribute(k_traverse<true, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 8);
     int nb = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_traverse<false, false>, kTravThreads, 0);
     return nb < 1 ? 1 : nb;

@@ -60,27 +60,31 @@ __device__ __forceinline__ bool pair_features(float4 cell, float2 a2, float4 g0,
         s = 0.0f;
         return false;
     }
-    const float d = sqrtf(d2);
-    c = wx / d;
-    s = wy / d;
+    // approximate reciprocals are enough for features; training and
+    // inference compute them with this same function
+    const float inv_d = rsqrtf(d2);
+    c = wx * inv_d;
+    s = wy * inv_d;
     const float c2 = c * c - s * s, s2 = 2.0f * c * s;
     const float a2r = a2.x * c2 + a2.y * s2, a2i = a2.y * c2 - a2.x * s2;
     const float b2r = g1.x * c2 + g1.y * s2, b2i = g1.y * c2 - g1.x * s2;
-    const float md2 = M * d2;
+    const float inv_d2 = inv_d * inv_d;
+    const float inv_md2 = __fdividef(inv_d2, M);
+    const float inv_h = __fdividef(1.0f, h);
     const float dq = ldexpf(4.0f * radius * radius * itolsq, -2 * (lvl - 1)) + epssq;
-    f[0] = h / d;
-    f[1] = spread / d;
-    f[2] = a2r / md2;
-    f[3] = a2i / md2;
-    f[4] = b2r / d2;
-    f[5] = b2i / d2;
-    f[6] = sqrtf(a2.x * a2.x + a2.y * a2.y) / (M * h * h);
-    f[7] = log2f(d2 / dq) * 0.125f;
+    f[0] = h * inv_d;
+    f[1] = spread * inv_d;
+    f[2] = a2r * inv_md2;
+    f[3] = a2i * inv_md2;
+    f[4] = b2r * inv_d2;
+    f[5] = b2i * inv_d2;
+    f[6] = __fdividef(sqrtf(a2.x * a2.x + a2.y * a2.y) * inv_h * inv_h, M);
+    f[7] = __log2f(__fdividef(d2, dq)) * 0.125f;
     f[8] = f[0] * f[0];
     f[9] = f[1] * f[1];
-    f[10] = spread / h;
+    f[10] = spread * inv_h;
     f[11] = g0.w * (1.0f / 32.0f);
-    sig = M / d;
+    sig = M * inv_d;
     return true;
 }
 
@@ -179,8 +183,27 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
     return *reinterpret_cast<uint32_t *>(&p);
 }
 
-__device__ __forceinline__ float bf16_round(float x) {
-    return __bfloat162float(__float2bfloat16_rn(x));
+// max(lo, 0) and max(hi, 0) rounded to BF16 and packed, in one instruction
+__device__ __forceinline__ uint32_t pack_bf16_relu(float lo, float hi) {
+    uint32_t r;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
+
+// 16 consecutive 32-bit TMEM columns of this thread's lane (see tmem_load32).
+__device__ __forceinline__ void tmem_load16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
+        "[%16];\n\ttcgen05.wait::ld.sync.aligned;"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 // ------------------------------------------------------------ MLP kernel --
@@ -189,17 +212,24 @@ constexpr int kMlpRows = 128;  // rows per tile: one per TMEM lane and thread
 constexpr int kMlpThreads = 128;
 constexpr uint32_t kMlpTmemCols = 64;  // both layers' accumulators, in turn
 constexpr uint32_t kIdesc = instr_desc_bf16(kMlpRows, kLearnHidden);
+constexpr uint32_t kIdescOut = instr_desc_bf16(kMlpRows, kLearnOutPad);
 
 struct MlpSmem {
     uint8_t a[kMlpRows * kLearnInPad * 2];    // features, BF16, K-major operand layout
-    uint8_t h[kMlpRows * kLearnHidden * 2];   // first hidden layer, BF16
-    MlpDevice w;                              // weights (W1, W2 in operand layout)
+    uint8_t h[kMlpRows * kLearnHidden * 2];   // a hidden layer, BF16
+    MlpDevice w;                              // weights (W1, W2, W3 in operand layout)
     unsigned long long mbar;
     uint32_t tmem_base;
 };
 static_assert(sizeof(MlpDevice) % 16 == 0, "weights are copied in 16-byte pieces");
 static_assert(offsetof(MlpSmem, h) % 16 == 0 && offsetof(MlpSmem, w) % 16 == 0,
               "operand tiles start on 16-byte boundaries");
+
+// Writes 8 packed BF16 pairs' worth (16 bytes) as K chunk `chunk` of row r.
+__device__ __forceinline__ void put_packed(uint8_t *tile, int r, int chunk, int kchunks,
+                                           uint4 q) {
+    *reinterpret_cast<uint4 *>(tile + operand_offset(r, chunk * 8, kchunks)) = q;
+}
 
 // Writes the 8-element K chunk `chunk` of row r (BF16) into an operand tile.
 __device__ __forceinline__ void put_chunk(uint8_t *tile, int r, int chunk, int kchunks,
@@ -319,6 +349,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_learn_mlp(
     const uint64_t dw1 = operand_desc(smem_u32(S.w.w1), 128, 2 * 128);
     const uint64_t dh = operand_desc(smem_u32(S.h), 128, 8 * 128);
     const uint64_t dw2 = operand_desc(smem_u32(S.w.w2), 128, 8 * 128);
+    const uint64_t dw3 = operand_desc(smem_u32(S.w.w3), 128, 8 * 128);
     // this warp's 32 TMEM lanes (warp q of the block reads lanes 32q..32q+31)
     const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
     const float radius = PAIRS ? st->trav_radius : 0.0f;
@@ -357,6 +388,9 @@ __global__ void __launch_bounds__(kMlpThreads) k_learn_mlp(
 #pragma unroll
             for (int q = 0; q < kLearnIn; ++q) f[q] = fv[q];
         }
+        // the columns that meet b1's two parts in W1
+        f[kBiasColHi] = 1.0f;
+        f[kBiasColLo] = 1.0f;
         put_chunk(S.a, t, 0, 2, f);
         put_chunk(S.a, t, 1, 2, f + 8);
         fence_async_smem();
@@ -378,15 +412,19 @@ __global__ void __launch_bounds__(kMlpThreads) k_learn_mlp(
             break;
         }
         tc_fence_after();
-        // layer 1: bias, ReLU, BF16 into the second operand tile
+        // layer 1 (its bias came with the MMA): ReLU and BF16 into the
+        // hidden operand tile
 #pragma unroll
         for (int half = 0; half < 2; ++half) {
             float v[32];
             tmem_load32(taddr + half * 32, v);
 #pragma unroll
-            for (int j = 0; j < 32; ++j) v[j] = fmaxf(v[j] + S.w.b1[half * 32 + j], 0.0f);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) put_chunk(S.h, t, half * 4 + q, 8, v + 8 * q);
+            for (int q = 0; q < 4; ++q) {
+                const float *u = v + 8 * q;
+                put_packed(S.h, t, half * 4 + q, 8,
+                           make_uint4(pack_bf16_relu(u[0], u[1]), pack_bf16_relu(u[2], u[3]),
+                                      pack_bf16_relu(u[4], u[5]), pack_bf16_relu(u[6], u[7])));
+            }
         }
         fence_async_smem();
         tc_fence_before();
@@ -407,19 +445,47 @@ __global__ void __launch_bounds__(kMlpThreads) k_learn_mlp(
             break;
         }
         tc_fence_after();
-        // layer 2: bias, ReLU, BF16; output layer on the CUDA cores
-        float y0 = S.w.b3[0], y1 = S.w.b3[1];
+        // layer 2: bias, ReLU, BF16 into the hidden tile again (layer 2's
+        // MMAs have read it); then the output layer, N = 16 of which the
+        // first two columns are W3's rows
 #pragma unroll
         for (int half = 0; half < 2; ++half) {
             float v[32];
             tmem_load32(taddr + half * 32, v);
 #pragma unroll
-            for (int j = 0; j < 32; ++j) {
-                const float hv = bf16_round(fmaxf(v[j] + S.w.b2[half * 32 + j], 0.0f));
-                const float2 w3 = S.w.w3[half * 32 + j];
-                y0 = fmaf(w3.x, hv, y0);
-                y1 = fmaf(w3.y, hv, y1);
+            for (int q = 0; q < 4; ++q) {
+                float u[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) u[j] = v[8 * q + j] + S.w.b2[half * 32 + 8 * q + j];
+                put_packed(S.h, t, half * 4 + q, 8,
+                           make_uint4(pack_bf16_relu(u[0], u[1]), pack_bf16_relu(u[2], u[3]),
+                                      pack_bf16_relu(u[4], u[5]), pack_bf16_relu(u[6], u[7])));
             }
+        }
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        if (t == 0) {
+            tc_fence_after();
+#pragma unroll
+            for (int kk = 0; kk < kLearnHidden / 16; ++kk)
+                mma_bf16(tmem, dh + (uint64_t)(kk * 16), dw3 + (uint64_t)(kk * 16), kIdescOut,
+                         kk > 0 ? 1u : 0u);
+            mma_commit(mbar);
+        }
+        ok = mbar_wait(mbar, phase);
+        phase ^= 1u;
+        if (__syncthreads_or(!ok)) {
+            bad = true;
+            break;
+        }
+        tc_fence_after();
+        float y0, y1;
+        {
+            float v[16];
+            tmem_load16(taddr, v);
+            y0 = v[0] + S.w.b3[0];
+            y1 = v[1] + S.w.b3[1];
         }
         // the next tile's first MMA overwrites the columns just read
         tc_fence_before();

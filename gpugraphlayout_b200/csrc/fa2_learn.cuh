@@ -30,17 +30,20 @@ constexpr int kLearnOut = 2;
 // varies across it, which one correction per group cannot follow.
 constexpr float kLearnMaxSpread = 0.5f;
 
-// The MLP as the kernels read it: W1 and W2 in BF16, placed in the tensor
-// cores' K-major no-swizzle operand layout (8-row x 16-byte core matrices,
-// the K chunks of an 8-row group 128 bytes apart, 8-row groups one row of
-// chunks apart); biases in FP32; W3 (2 x 64, BF16 values held as floats) as
-// {W3[0][j], W3[1][j]} pairs for the CUDA-core output layer.
+// The MLP as the kernels read it: the three weight matrices in BF16, placed
+// in the tensor cores' K-major no-swizzle operand layout (8-row x 16-byte
+// core matrices, the K chunks of an 8-row group 128 bytes apart, 8-row groups
+// one row of chunks apart).  W1's 16 K columns are the 12 features, then the
+// bias b1 split into two BF16 parts (its rounding and the rest) that meet an
+// input column of ones, then zeros.  W3 is padded to 16 output rows (N = 16
+// is the smallest MMA width at M = 128).  b2 and b3 stay FP32.
+constexpr int kLearnOutPad = 16;
+constexpr int kBiasColHi = kLearnIn, kBiasColLo = kLearnIn + 1;
 struct MlpDevice {
-    uint16_t w1[kLearnHidden * kLearnInPad];   // 2 KB
-    uint16_t w2[kLearnHidden * kLearnHidden];  // 8 KB
-    float b1[kLearnHidden];
+    uint16_t w1[kLearnHidden * kLearnInPad];    // 2 KB
+    uint16_t w2[kLearnHidden * kLearnHidden];   // 8 KB
+    uint16_t w3[kLearnOutPad * kLearnHidden];   // 2 KB
     float b2[kLearnHidden];
-    float2 w3[kLearnHidden];
     float b3[kLearnOut];
     float pad[2];
 };
