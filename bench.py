@@ -260,18 +260,28 @@ def correction_report(eng, n, steps, device=0):
     # the learned correction on the same positions, samples and FP64 sums
     models, train_graph = train_learned(device)
     learned = []
+    from gpugraphlayout_b200 import Fa2Error
     for (theta, mp), (mlp, info) in models.items():
         eng.set_approximation(theta, mp)
         eng.set_learned_correction(mlp)
-        eng.set_positions(P)
-        eng.step(1)
-        tot, ga = eng.forces()
-        rep = (tot - ga)[samples].astype(np.float64)
-        err = float(np.sqrt(((rep - exact) ** 2).sum() / (exact ** 2).sum()))
-        visits = eng.stats()["visits"]
-        eng.set_positions(P)
-        ms, kms = eng.step_timed(k)
+        try:
+            eng.set_positions(P)
+            eng.step(1)
+            tot, ga = eng.forces()
+            rep = (tot - ga)[samples].astype(np.float64)
+            err = float(np.sqrt(((rep - exact) ** 2).sum() / (exact ** 2).sum()))
+            st1 = eng.stats()
+            visits, pairs = st1["visits"], st1["learned_pairs"]
+            eng.set_positions(P)
+            ms, kms = eng.step_timed(k)
+        except Fa2Error as ex:  # recorded, not fatal: the next configuration starts afresh
+            learned.append({"theta": theta, "multipole": mp, "error": str(ex),
+                            "device_error": eng.stats()["device_error"]})
+            eng.set_learned_correction(None)
+            eng.set_positions(P)
+            continue
         learned.append({"theta": theta, "multipole": mp, "rel_rmse": err, "visits": visits,
+                        "pairs": pairs,
                         "ms_per_step": ms / k,
                         "walk_ms": kms.get("traverse", 0.0) + kms.get("quadrupole", 0.0),
                         "moments_ms": kms.get("moments", 0.0),
@@ -280,9 +290,10 @@ def correction_report(eng, n, steps, device=0):
                                                              "collect_s", "fit_s")}})
         eng.set_learned_correction(None)
     eng.set_approximation(1.0, 1)
-    ok_l = [r for r in learned if r["rel_rmse"] <= base["rel_rmse"]]
+    ran = [r for r in learned if "error" not in r]
+    ok_l = [r for r in ran if r["rel_rmse"] <= base["rel_rmse"]]
     best_l = min(ok_l, key=lambda r: r["ms_per_step"]) if ok_l else None
-    fastest_l = min(learned, key=lambda r: r["ms_per_step"]) if learned else None
+    fastest_l = min(ran, key=lambda r: r["ms_per_step"]) if ran else None
     learned_guarded = None
     if best_l is not None:
         steps_g = 4 * GUARD_EVERY
