@@ -34,11 +34,14 @@ constexpr unsigned kFull = kFullMask;
 //   7  log2(d^2 / dq) / 8  margin over the walk's acceptance threshold dq
 //   8  (h / d)^2
 //   9  (s / d)^2
-//   10 s / h
+//   10 log2(1 + s / h) / 8
 //   11 bodies in the group / 32
 // Every feature is a ratio of lengths (or of moments to the matching power
 // of a length), so a model trained on one graph size serves another: the
-// tree level and the cell mass themselves are not features.
+// tree level and the cell mass themselves are not features.  Every feature
+// is bounded for an accepted cell (a cell's bodies lie within sqrt(2) h of
+// its centre of mass, the spread test bounds s / d); s / h alone is not (a
+// tiny deep cell seen from a spread-out group), hence its logarithm.
 // sig = M / d scales the outputs back, (c, s) is the turn.  Returns false
 // when the pair is not corrected: a group spread beyond kLearnMaxSpread of
 // the distance, or a degenerate cell or distance.
@@ -82,7 +85,7 @@ __device__ __forceinline__ bool pair_features(float4 cell, float2 a2, float4 g0,
     f[7] = __log2f(__fdividef(d2, dq)) * 0.125f;
     f[8] = f[0] * f[0];
     f[9] = f[1] * f[1];
-    f[10] = spread * inv_h;
+    f[10] = __log2f(1.0f + spread * inv_h) * 0.125f;
     f[11] = g0.w * (1.0f / 32.0f);
     sig = M * inv_d;
     return true;
@@ -487,6 +490,12 @@ __global__ void __launch_bounds__(kMlpThreads) k_learn_mlp(
             y0 = v[0] + S.w.b3[0];
             y1 = v[1] + S.w.b3[1];
         }
+        if (PAIRS) {
+            // a cell's correction never exceeds its own point-mass term
+            // (|y| <= 1 in units of M / d); a non-finite output adds nothing
+            y0 = isfinite(y0) ? fminf(fmaxf(y0, -kLearnMaxOut), kLearnMaxOut) : 0.0f;
+            y1 = isfinite(y1) ? fminf(fmaxf(y1, -kLearnMaxOut), kLearnMaxOut) : 0.0f;
+        }
         // the next tile's first MMA overwrites the columns just read
         tc_fence_before();
         if (PAIRS) {
@@ -622,8 +631,10 @@ __global__ void __launch_bounds__(256) k_learn_targets(
             if (idx < cap) {
 #pragma unroll
                 for (int q = 0; q < kLearnIn; ++q) features[idx * kLearnIn + q] = f[q];
-                targets[idx] = make_float2((float)((c * mx + s * my) / sig),
-                                           (float)((c * my - s * mx) / sig));
+                // within the bound the MLP's outputs are held to
+                const double lim = (double)kLearnMaxOut;
+                targets[idx] = make_float2((float)fmin(fmax((c * mx + s * my) / sig, -lim), lim),
+                                           (float)fmin(fmax((c * my - s * mx) / sig, -lim), lim));
                 weights[idx] = (float)((double)sig * sig * m2);
                 keys[idx] = (uint64_t)w << 32 | node;
             }

@@ -29,6 +29,9 @@ constexpr int kLearnOut = 2;
 // distance to the cell: a group straddling a cell boundary sees a field that
 // varies across it, which one correction per group cannot follow.
 constexpr float kLearnMaxSpread = 0.5f;
+// Largest correction of one pair, in units of the cell's point-mass term
+// M / d: the MLP's outputs (and the training targets) are clamped to it.
+constexpr float kLearnMaxOut = 1.0f;
 
 // The MLP as the kernels read it: the three weight matrices in BF16, placed
 // in the tensor cores' K-major no-swizzle operand layout (8-row x 16-byte

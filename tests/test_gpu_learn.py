@@ -190,3 +190,25 @@ def test_trained_correction_lowers_the_error_against_fp64():
         errs[name] = rel_rmse((tot - ga)[samples], exact)
     e.set_learned_correction(None)
     assert errs["learned"] < 0.8 * errs["plain"], errs
+
+
+def test_any_mlp_keeps_the_layout_finite():
+    """An untrained MLP with large weights on a graph whose trees reach deep
+    levels: each pair's correction is held to its cell's point-mass term and
+    non-finite outputs add nothing, so 30 steps leave finite positions and
+    no device error."""
+    from gpugraphlayout_b200 import Engine, FarFieldMLP, synth
+    from oracle import oracle as O
+    s, t = synth.rmat_edges(16, 1 << 20, seed=0)
+    g = O.Graph(s, t)
+    xy = O.random_positions(g.n, 2e4, 2e4, 1234)
+    mlp = FarFieldMLP(seed=4)
+    for name in ("w1", "w2", "w3", "b3"):
+        mlp[name] = mlp[name] * 40.0
+    e = Engine(g.n, g.sources, g.targets, strong_gravity=True, scale=10.0, theta=1.2)
+    e.set_positions(xy)
+    e.set_learned_correction(mlp)
+    e.step(30)
+    assert np.isfinite(e.get_positions()).all()
+    st = e.stats()
+    assert st["device_error"] == 0 and st["learned_pairs"] > 0
