@@ -171,6 +171,17 @@ class Engine:
         check(lib().fa2_set_learned_correction(self._ctx, None if mlp is None else C.byref(mlp.c)),
               "fa2_set_learned_correction")
 
+    def set_prevent_overlap(self, sizes) -> None:
+        """ForceAtlas2's prevent_overlap with one size per node (reference
+        ids), from the next step on; None turns it off."""
+        if sizes is None:
+            check(lib().fa2_set_prevent_overlap(self._ctx, None), "fa2_set_prevent_overlap")
+            return
+        sz = np.ascontiguousarray(sizes, np.float32).ravel()
+        if len(sz) != self.n:
+            raise Fa2Error(1, "set_prevent_overlap: one size per node")
+        check(lib().fa2_set_prevent_overlap(self._ctx, _ptr(sz)), "fa2_set_prevent_overlap")
+
     def set_overlap(self, enable: bool) -> None:
         """Attraction beside the tree build (default) or alone before it."""
         check(lib().fa2_set_overlap(self._ctx, 1 if enable else 0), "fa2_set_overlap")

@@ -30,7 +30,7 @@ EXPORTS = (
     "fa2_status_string", "fa2_version",
     "fa2_mlp_init", "fa2_set_learned_correction", "fa2_mlp_forward", "fa2_mlp_train_step",
     "fa2_learn_set_create", "fa2_learn_set_destroy", "fa2_learn_set_size", "fa2_learn_collect",
-    "fa2_learn_set_read", "fa2_learn_fit", "fa2_mlp_launch_shape",
+    "fa2_learn_set_read", "fa2_learn_fit", "fa2_mlp_launch_shape", "fa2_set_prevent_overlap",
 )
 
 FA2_OK = 0
@@ -168,6 +168,7 @@ def lib():
     L.fa2_set_learned_correction.argtypes = [vp, mp]
     L.fa2_mlp_forward.argtypes = [C.c_int32, mp, vp, C.c_int64, vp]
     L.fa2_mlp_launch_shape.argtypes = [C.c_int32, vp, vp]
+    L.fa2_set_prevent_overlap.argtypes = [vp, vp]
     L.fa2_mlp_train_step.argtypes = [C.c_int32, mp, mp, mp, C.c_int32, C.c_float, vp, vp, vp,
                                      C.c_int32, f32p]
     L.fa2_learn_set_create.restype = vp

@@ -326,6 +326,7 @@ void enqueue_iteration(fa2_ctx *c, bool full, bool perturb_first, bool timed) {
         launch_quad_cells(b, c->nsm, A);
         mark(S_QUAD, 1, A);
     }
+    if (c->kp.overlap) launch_sorted_sizes(b, A);
     mark(S_TRAV, 0, A);
     if (learn)
         launch_traverse_learn(b, c->kp, c->lb, c->trav_blocks, A);
@@ -1047,6 +1048,7 @@ int fa2_set_linlog(fa2_ctx *c, int32_t enable) {
     if (!c) return FA2_ERR_INVALID_ARGUMENT;
     CK(cudaSetDevice(c->device));
     if (c->kp.linlog == (enable != 0)) return FA2_OK;
+    if (enable && c->kp.overlap) return FA2_ERR_UNSUPPORTED;
     CK(cudaStreamSynchronize(c->sA));
     c->kp.linlog = enable != 0;
     c->prm.linlog = enable != 0;
@@ -1058,6 +1060,7 @@ int fa2_set_approximation(fa2_ctx *c, float theta, int32_t multipole) {
     if (!c || !(theta > 0.0f) || multipole < 1 || multipole > 2) return FA2_ERR_INVALID_ARGUMENT;
     CK(cudaSetDevice(c->device));
     const float itolsq = 1.0f / (theta * theta);  // src/RPForceAtlas2.cpp:47
+    if (multipole >= 2 && c->kp.overlap) return FA2_ERR_UNSUPPORTED;
     if (c->kp.itolsq == itolsq && c->kp.multipole == multipole) {
         c->prm.theta = theta;
         return FA2_OK;
@@ -1110,6 +1113,8 @@ const char *fa2_last_cuda_error(void) { return g_last_cuda_error; }
 
 int fa2_set_accuracy_guard(fa2_ctx *c, int32_t every, int32_t n_samples) {
     if (!c || every < 0 || (every > 0 && n_samples <= 0)) return FA2_ERR_INVALID_ARGUMENT;
+    // the guard's reference walk has no node sizes
+    if (every > 0 && c->kp.overlap) return FA2_ERR_UNSUPPORTED;
     CK(cudaSetDevice(c->device));
     c->guard_checks = c->guard_fallbacks = 0;
     c->guard_err_cur = c->guard_err_plain = 0.0;
@@ -1142,6 +1147,40 @@ int fa2_get_accuracy_guard(fa2_ctx *c, double *err_current, double *err_plain, i
     return FA2_OK;
 }
 
+int fa2_set_prevent_overlap(fa2_ctx *c, const float *sizes) {
+    if (!c) return FA2_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->sA));
+    if (!sizes) {
+        if (c->kp.overlap) {
+            c->kp.overlap = 0;
+            drop_graphs(c);
+        }
+        return FA2_OK;
+    }
+    if (c->kp.linlog || c->kp.multipole >= 2 || c->learn_on || c->guard_every > 0)
+        return FA2_ERR_UNSUPPORTED;
+    std::vector<float> internal(c->n);
+    for (uint32_t i = 0; i < c->n; ++i) {
+        const float v = sizes[c->ref_of[i]];
+        if (!(v >= 0.0f) || !std::isfinite(v)) return FA2_ERR_INVALID_ARGUMENT;
+        internal[i] = v;
+    }
+    if (c->n == 0) return FA2_OK;
+    int s = FA2_OK;
+    float *d_size = const_cast<float *>(c->b.size);
+    if (!d_size && (s = dalloc(c, &d_size, c->n))) return s;
+    if (!c->b.ssize && (s = dalloc(c, &c->b.ssize, c->n))) return s;
+    c->b.size = d_size;
+    CK(cudaMemcpyAsync(d_size, internal.data(), (size_t)c->n * 4, cudaMemcpyHostToDevice, c->sA));
+    CK(cudaStreamSynchronize(c->sA));
+    if (!c->kp.overlap) {
+        c->kp.overlap = 1;
+        drop_graphs(c);
+    }
+    return FA2_OK;
+}
+
 int fa2_set_overlap(fa2_ctx *c, int32_t enable) {
     if (!c) return FA2_ERR_INVALID_ARGUMENT;
     CK(cudaSetDevice(c->device));
@@ -1171,6 +1210,7 @@ int fa2_set_learned_correction(fa2_ctx *c, const fa2_mlp *mlp) {
         return FA2_OK;
     }
     if (!mlp_is_finite(*mlp)) return FA2_ERR_INVALID_ARGUMENT;
+    if (c->kp.overlap) return FA2_ERR_UNSUPPORTED;
     mlp_blocks_per_sm();  // the launch shape, settled outside any graph capture
     int s = ensure_quad_buffers(c);
     if (!s) s = ensure_learn_buffers(c);

@@ -37,6 +37,21 @@ __device__ __forceinline__ float sq_norm(float dx, float dy) {
     return __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
 }
 
+// prevent_overlap (the option src/RPForceAtlas2.hpp:44 declares and the
+// reference never implements, src/RPCPUForceAtlas2.cpp:201-205): the rule of
+// the ForceAtlas2 paper (Jacomy et al., PLoS ONE 2014) on the border-to-
+// border distance d' = d - s_i - s_j, with d the walk's softened distance
+// sqrt(d^2 + eps).  Repulsion k_r m_i m_j / d' while apart, 100 k_r m_i m_j
+// while overlapping, nothing at d' = 0; returned as the factor c of
+// k_r m_i c (p_i - p_j).
+__device__ __forceinline__ float overlap_factor(float d2, float si, float sj, float mj) {
+    const float ds = sqrtf(d2);
+    const float dp = ds - si - sj;
+    if (dp > 0.0f) return mj / (ds * dp);
+    if (dp < 0.0f) return 100.0f * mj / ds;
+    return 0.0f;
+}
+
 // --------------------------------------------------- shared by the kernels --
 
 // Quadrant digits of (px, py) under the root cell, computed the way

@@ -166,6 +166,8 @@ struct Buffers {
     int sort_first;           // first sort pass (0; 1 or 2 after shallow trees: k_fix_low)
     uint32_t *sort_counts;    // [8][sort tiles][256]: digit counts per tile and pass
     uint32_t *count_status;   // [count tiles]
+    const float *size;        // n: node sizes for prevent_overlap (null: off)
+    float *ssize;             // n: the same in sorted order, per iteration
 };
 
 struct Params {
@@ -174,6 +176,7 @@ struct Params {
     int linlog;     // linear-log attraction
     int multipole;  // 1: monopole cells (the reference); 2: + quadrupole term
     int nsm;
+    int overlap;    // prevent_overlap: node sizes in Buffers::size
 };
 
 constexpr int kBBoxThreads = 512;
@@ -203,6 +206,8 @@ void launch_exact_f64(const Buffers &b, const Params &p, const uint32_t *ids, in
 void launch_guard(const Buffers &b, const Params &p, int ns, double2 *exact, float2 *plain,
                   float2 *cur, cudaStream_t s);
 void launch_attract(const Buffers &b, const Params &p, const AttractPlan &plan, cudaStream_t s);
+// prevent_overlap: node sizes in sorted order (before the walk)
+void launch_sorted_sizes(const Buffers &b, cudaStream_t s);
 void launch_scatter_xy(int n, const uint32_t *ref_of, const float2 *src_ref, float2 *dst_int,
                        cudaStream_t s);
 void launch_gather_xy(int n, const uint32_t *ref_of, const float2 *src_int, float2 *dst_ref,

@@ -155,13 +155,18 @@ __global__ void __launch_bounds__(1024) k_keys(int n, int tile, int first,
 // accepted (a (group, node) pair, gathered 32 at a time in shared memory),
 // and writes each body's repulsion in sorted order instead of the tail: the
 // MLP and k_learn_tail finish the iteration.  The sums are the same.
-template <bool QUAD, bool LEARN>
+//
+// OVERLAP (prevent_overlap, with the monopole walk) repels accepted bodies by
+// the paper's anti-collision rule (overlap_factor) with the sizes of the
+// sorted bodies in ssize; a body node's sorted index is its owner's.
+template <bool QUAD, bool LEARN, bool OVERLAP = false>
 __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
     int n, const float4 *__restrict nodes, const float2 *__restrict quad,
     const uint32_t *__restrict body_node,
     const uint32_t *__restrict vals, const float2 *__restrict fag,
     const float2 *__restrict fprev, float2 *__restrict f, float2 *__restrict warp_partial,
-    DevState *st, IterCounters *ctr, Params prm, LearnBuffers lb) {
+    DevState *st, IterCounters *ctr, Params prm, LearnBuffers lb,
+    const uint32_t *__restrict owner = nullptr, const float *__restrict ssize = nullptr) {
     __shared__ float s_dq[64];
     __shared__ bool s_last;
     __shared__ float s_red[2][kTravThreads / kWarp];
@@ -200,6 +205,7 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
         // a lane without a body sits far away: it passes every test and its
         // (unused) sums never feed anything
         const float px = active ? me.x : 1e30f, py = active ? me.y : 1e30f;
+        const float my_size = OVERLAP && active ? ssize[k] : 0.0f;
         // sum of m_j d / (d^2 + eps) over the accepted nodes; the body's own
         // k_r m_i multiplies the sum once at the end
         float ax = 0.0f, ay = 0.0f;
@@ -255,7 +261,11 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
                 // written as !(d2 < dq): a NaN distance accepts, so a warp
                 // with a non-finite lane still ends its walk
                 if (__all_sync(kFull, !(d2 < s_dq[meta_level(meta)]))) {
-                    const float c = __fdividef(r.z, d2);
+                    float c;
+                    if (OVERLAP && meta_level(meta) == kBodyLevel)
+                        c = overlap_factor(d2, my_size, ssize[owner[node] >> 6], r.z);
+                    else
+                        c = __fdividef(r.z, d2);
                     ax = fmaf(dx, c, ax);
                     ay = fmaf(dy, c, ay);
                     if (LEARN && meta_level(meta) != kBodyLevel) {
@@ -758,6 +768,48 @@ __global__ void __launch_bounds__(256, (LINLOG || WEIGHTED) ? 4 : 8) k_attract(
     }
 }
 
+// Gravity plus attraction with prevent_overlap: one warp per row of the
+// padded CSR, each neighbour's pull (p_j - p_i) (d - s_i - s_j) / d while
+// apart and nothing while overlapping (the paper's rule; a padding entry is
+// the row's own id and pulls nothing), times w^delta with edge weights.
+template <bool WEIGHTED>
+__global__ void __launch_bounds__(256) k_attract_overlap(
+    int n, const float2 *__restrict pos, const float *__restrict mass,
+    const float *__restrict size, const uint32_t *__restrict off, const int *__restrict col,
+    const float *__restrict wcol, float2 *__restrict fag, Params prm) {
+    const int lane = threadIdx.x & 31;
+    const int row = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (row >= n) return;
+    const float2 p = pos[row];
+    const float si = size[row];
+    float ax = 0.0f, ay = 0.0f;
+    for (uint32_t q = off[row] + lane; q < off[row + 1]; q += 32) {
+        const int j = col[q];
+        const float2 o = pos[j];
+        const float dx = o.x - p.x, dy = o.y - p.y;
+        const float d = sqrtf(dx * dx + dy * dy);
+        const float dp = d - si - size[j];
+        float w = dp > 0.0f ? dp / d : 0.0f;
+        if (WEIGHTED) w *= wcol[q];
+        ax = fmaf(dx, w, ax);
+        ay = fmaf(dy, w, ay);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        ax += __shfl_xor_sync(kFull, ax, o);
+        ay += __shfl_xor_sync(kFull, ay, o);
+    }
+    if (lane == 0) fag[row] = with_gravity(p, mass[row], ax, ay, prm);
+}
+
+__global__ void k_sorted_sizes(int n, const float *__restrict size,
+                               const uint32_t *__restrict vals, float *__restrict ssize,
+                               const DevState *st) {
+    if (st->err || st->poison) return;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        ssize[k] = size[vals[k]];
+}
+
 // ----------------------------------------------------------- permutations --
 
 __global__ void k_scatter_xy(int n, const uint32_t *__restrict ref_of,
@@ -809,8 +861,14 @@ void launch_traverse(const Buffers &b, const Params &p, int nblocks, cudaStream_
     auto go = [&](auto kernel) {
         kernel<<<nblocks, kTravThreads, 0, s>>>(b.n, b.nodes, b.quad, b.body_node, b.vals[0],
                                                 b.fag, b.fprev, b.f, b.warp_partial, b.st, b.ctr,
-                                                p, none);
+                                                p, none, nullptr, nullptr);
     };
+    if (p.overlap) {
+        k_traverse<false, false, true><<<nblocks, kTravThreads, 0, s>>>(
+            b.n, b.nodes, b.quad, b.body_node, b.vals[0], b.fag, b.fprev, b.f, b.warp_partial,
+            b.st, b.ctr, p, none, b.owner, b.ssize);
+        return;
+    }
     if (p.multipole >= 2)
         go(k_traverse<true, false>);
     else
@@ -822,7 +880,7 @@ void launch_traverse_learn(const Buffers &b, const Params &p, const LearnBuffers
     auto go = [&](auto kernel) {
         kernel<<<nblocks, kTravThreads, 0, s>>>(b.n, b.nodes, b.quad, b.body_node, b.vals[0],
                                                 b.fag, b.fprev, b.f, b.warp_partial, b.st, b.ctr,
-                                                p, lb);
+                                                p, lb, nullptr, nullptr);
     };
     if (p.multipole >= 2)
         go(k_traverse<true, true>);
@@ -855,6 +913,18 @@ void launch_count_interactions(const Buffers &b, const Params &p, int nblocks, c
 
 void launch_attract(const Buffers &b, const Params &p, const AttractPlan &plan, cudaStream_t s) {
     if (plan.nblocks == 0) return;
+    if (p.overlap) {
+        const int blocks = (b.n + 7) / 8;
+        const int *col = reinterpret_cast<const int *>(b.csr_col4);
+        const float *w = reinterpret_cast<const float *>(b.csr_w4);
+        if (w)
+            k_attract_overlap<true><<<blocks, 256, 0, s>>>(b.n, b.pos, b.mass, b.size, b.csr_off,
+                                                           col, w, b.fag, p);
+        else
+            k_attract_overlap<false><<<blocks, 256, 0, s>>>(b.n, b.pos, b.mass, b.size,
+                                                            b.csr_off, col, w, b.fag, p);
+        return;
+    }
     const float4 *w4 = b.csr_w4;
     auto go = [&](auto kernel) {
         kernel<<<plan.nblocks, 256, 0, s>>>(plan, b.pos, b.mass, b.csr_off, b.csr_col4, w4, b.fag,
@@ -864,6 +934,11 @@ void launch_attract(const Buffers &b, const Params &p, const AttractPlan &plan, 
         p.linlog ? go(k_attract<true, true>) : go(k_attract<false, true>);
     else
         p.linlog ? go(k_attract<true, false>) : go(k_attract<false, false>);
+}
+
+void launch_sorted_sizes(const Buffers &b, cudaStream_t s) {
+    k_sorted_sizes<<<grid_for(b.n, 256, 4096), 256, 0, s>>>(b.n, b.size, b.vals[0], b.ssize,
+                                                            b.st);
 }
 
 void launch_scatter_xy(int n, const uint32_t *ref_of, const float2 *src_ref, float2 *dst_int,
@@ -885,6 +960,8 @@ int traverse_blocks_per_sm() {
     // the walk lives on L1 hits: give L1 the most of the SM's on-chip memory
     cudaFuncSetAttribute(k_traverse<false, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
     cudaFuncSetAttribute(k_traverse<true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+    cudaFuncSetAttribute(k_traverse<false, false, true>,
+                         cudaFuncAttributePreferredSharedMemoryCarveout, 0);
     // the learned walk keeps 4 KB of pending pairs per block: the smallest
     // shared-memory share that holds two blocks
     cudaFuncSetAttribute(k_traverse<false, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 8);

@@ -325,6 +325,22 @@ int fa2_learn_set_read(const fa2_learn_set *set, int64_t first, int64_t count, f
 int fa2_learn_fit(fa2_learn_set *set, fa2_mlp *mlp, int32_t steps, int32_t batch, float lr,
                   uint32_t seed, float *final_loss);
 
+/* prevent_overlap (ForceAtlas2::prevent_overlap, src/RPForceAtlas2.hpp:44),
+ * which the reference declares but never implements: its CPU displacement
+ * exits with "Not yet implemented" (src/RPCPUForceAtlas2.cpp:201-205) and its
+ * GPU path does not read the flag.  Here it is the rule of the ForceAtlas2
+ * paper (Jacomy et al., PLoS ONE 2014) on the border-to-border distance
+ * d' = d - s_i - s_j between bodies of sizes s (reference id order, one per
+ * node, finite and >= 0): repulsion k_r m_i m_j / d' while apart, 100 k_r
+ * m_i m_j while overlapping, nothing at d' = 0; attraction d' while apart,
+ * nothing while overlapping (times w^delta with edge weights).  d is the
+ * walk's softened distance sqrt(d^2 + eps) in the repulsion.  A Barnes-Hut
+ * cell has no size and repels as a point mass.  With every size 0 the forces
+ * are those of the plain rule up to float rounding (the overlap form goes
+ * through a square root).  NULL turns it off.  FA2_ERR_UNSUPPORTED with linear-log attraction,
+ * the quadrupole walk, the learned correction or the accuracy guard. */
+int fa2_set_prevent_overlap(fa2_ctx *ctx, const float *sizes);
+
 /* Measurement hook, no reference counterpart.  enable = 1 (the default) runs
  * the attraction on a second stream beside the tree build, the two sharing
  * the GPU; enable = 0 runs it alone before the tree build, so that the

@@ -562,12 +562,46 @@ void orc_tree_cells(const orc_tree *t, int32_t *level, float *mass, float *cx,
 
 #define ORC_MAXDEPTH 32 /* RPBHFA2LaunchParameters.cuh:62 */
 
+/* prevent_overlap (RPForceAtlas2.hpp:44; the reference declares it and its
+ * CPU displacement exits with "Not yet implemented", RPCPUForceAtlas2.cpp:
+ * 201-205).  The rule of the ForceAtlas2 paper (Jacomy et al., PLoS ONE
+ * 2014), with d' = d - s_i - s_j the border-to-border distance: repulsion
+ * k_r m_i m_j / d' while the nodes are apart, k_r' m_i m_j with k_r' = 100 k_r
+ * while they overlap, nothing at d' = 0; attraction d' while apart, nothing
+ * while they overlap.  Applied between bodies; a Barnes-Hut cell, which has
+ * no size, repels as a point mass.  d is the walk's softened distance
+ * sqrt(d^2 + eps).  Returns the factor c with force = k_r m_i c (p_i - p_j). */
+static float overlap_factor(float d2, float si, float sj, float mj) {
+    const float ds = sqrtf(d2);
+    const float dp = ds - si - sj;
+    if (dp > 0.0f) return mj / (ds * dp);
+    if (dp < 0.0f) return 100.0f * mj / ds;
+    return 0.0f;
+}
+
+void orc_attraction_overlap(int64_t n_edges, const int32_t *sources, const int32_t *targets,
+                            const float *sizes, const float *xy, float *fx, float *fy) {
+    for (int64_t e = 0; e < n_edges; ++e) {
+        const int32_t s = sources[e], t = targets[e];
+        const float dx = xy[2 * t] - xy[2 * s];
+        const float dy = xy[2 * t + 1] - xy[2 * s + 1];
+        const float d = sqrtf(dx * dx + dy * dy);
+        const float dp = d - sizes[s] - sizes[t];
+        const float w = dp > 0.0f ? dp / d : 0.0f;
+        const float qx = dx * w, qy = dy * w;
+        fx[s] += qx;
+        fy[s] += qy;
+        fx[t] += -qx;
+        fy[t] += -qy;
+    }
+}
+
 /* The walk of ForceCalculationKernel (restated below); with a2r/a2i set, each
  * accepted cell also adds its quadrupole term (orc_tree_repulsion_quad). */
 static int32_t tree_walk(const orc_tree *t, const float *xy, const float *mass, float k_r,
                          float itolsq, float epssq, int32_t group, const int32_t *sortd,
-                         const double *a2r, const double *a2i, float *fx, float *fy,
-                         int64_t *n_visits) {
+                         const double *a2r, const double *a2i, const float *sizes, float *fx,
+                         float *fy, int64_t *n_visits) {
     const int32_t NB = t->n;
     if (n_visits) *n_visits = 0;
     if (t->maxdepth > ORC_MAXDEPTH) return 1; /* RPBHKernels.cu:595 */
@@ -634,6 +668,13 @@ static int32_t tree_walk(const orc_tree *t, const float *xy, const float *mass, 
                         const int32_t b = lane_body[l];
                         const float dx = xy[2 * b] - nx, dy = xy[2 * b + 1] - ny;
                         const float d2 = dx * dx + dy * dy + epssq;
+                        if (sizes && n < NB) {
+                            /* prevent_overlap: border-to-border distance */
+                            const float c = overlap_factor(d2, sizes[b], sizes[n], nm);
+                            ax[l] += k_r * dx * mass[b] * c;
+                            ay[l] += k_r * dy * mass[b] * c;
+                            continue;
+                        }
                         ax[l] += k_r * dx * mass[b] * nm / d2;
                         ay[l] += k_r * dy * mass[b] * nm / d2;
                         if (a2r && n >= NB) {
@@ -672,7 +713,15 @@ int32_t orc_tree_repulsion(const orc_tree *t, const float *xy, const float *mass
                            float k_r, float itolsq, float epssq, int32_t group,
                            const int32_t *sortd, float *fx, float *fy,
                            int64_t *n_visits) {
-    return tree_walk(t, xy, mass, k_r, itolsq, epssq, group, sortd, NULL, NULL, fx, fy,
+    return tree_walk(t, xy, mass, k_r, itolsq, epssq, group, sortd, NULL, NULL, NULL, fx, fy,
+                     n_visits);
+}
+
+int32_t orc_tree_repulsion_overlap(const orc_tree *t, const float *xy, const float *mass,
+                                   const float *sizes, float k_r, float itolsq, float epssq,
+                                   int32_t group, const int32_t *sortd, float *fx, float *fy,
+                                   int64_t *n_visits) {
+    return tree_walk(t, xy, mass, k_r, itolsq, epssq, group, sortd, NULL, NULL, sizes, fx, fy,
                      n_visits);
 }
 
@@ -719,7 +768,7 @@ int32_t orc_tree_repulsion_quad(const orc_tree *t, const float *xy, const float 
         return -1;
     }
     cell_quadrupoles(t, xy, mass, 0, a2r, a2i);
-    int32_t r = tree_walk(t, xy, mass, k_r, itolsq, epssq, group, sortd, a2r, a2i, fx, fy,
+    int32_t r = tree_walk(t, xy, mass, k_r, itolsq, epssq, group, sortd, a2r, a2i, NULL, fx, fy,
                           n_visits);
     free(a2r);
     free(a2i);
@@ -786,7 +835,9 @@ int32_t orc_fa2_step(orc_fa2 *s) {
     const int32_t n = s->n;
     /* fx, fy are zero here: the previous displacement cleared them. */
     orc_gravity(n, s->xy, s->mass, s->k_g, s->strong_gravity, s->fx, s->fy);
-    if (s->linlog)
+    if (s->sizes)
+        orc_attraction_overlap(s->m, s->sources, s->targets, s->sizes, s->xy, s->fx, s->fy);
+    else if (s->linlog)
         orc_attraction_linlog(s->m, s->sources, s->targets, s->xy, s->fx, s->fy);
     else
         orc_attraction(s->m, s->sources, s->targets, s->xy, s->fx, s->fy);
@@ -805,8 +856,8 @@ int32_t orc_fa2_step(orc_fa2 *s) {
     if (t->maxdepth > s->maxdepth) s->maxdepth = t->maxdepth;
     s->depth_overflow = s->maxdepth > ORC_MAXDEPTH;
     if (!s->depth_overflow)
-        orc_tree_repulsion(t, s->xy, s->mass, s->k_r, s->itolsq, s->epssq, s->group, sortd,
-                           s->fx, s->fy, NULL);
+        tree_walk(t, s->xy, s->mass, s->k_r, s->itolsq, s->epssq, s->group, sortd, NULL, NULL,
+                  s->sizes, s->fx, s->fy, NULL);
     if (!s->sortd_out) free(sortd);
     orc_tree_free(t);
     if (s->f_tot_out)

@@ -148,6 +148,21 @@ int32_t orc_tree_repulsion_quad(const orc_tree *t, const float *xy, const float 
                                 float k_r, float itolsq, float epssq, int32_t group,
                                 const int32_t *sortd, float *fx, float *fy, int64_t *n_visits);
 
+/* orc_tree_repulsion with prevent_overlap between bodies (sizes per node):
+ * the ForceAtlas2 paper's anti-collision repulsion on the border-to-border
+ * distance; cells repel as point masses.  No reference implementation: the
+ * reference declares prevent_overlap (RPForceAtlas2.hpp:44) and exits on it
+ * (RPCPUForceAtlas2.cpp:201-205). */
+int32_t orc_tree_repulsion_overlap(const orc_tree *t, const float *xy, const float *mass,
+                                   const float *sizes, float k_r, float itolsq, float epssq,
+                                   int32_t group, const int32_t *sortd, float *fx, float *fy,
+                                   int64_t *n_visits);
+
+/* Attraction with prevent_overlap: per edge (p_t - p_s) (d - s_s - s_t) / d
+ * while the nodes are apart, nothing while they overlap. */
+void orc_attraction_overlap(int64_t n_edges, const int32_t *sources, const int32_t *targets,
+                            const float *sizes, const float *xy, float *fx, float *fy);
+
 /* Exact pairwise repulsion in double precision for the listed nodes:
  * F_i = sum_{j != i} k_r m_i m_j (p_i - p_j) / (|p_i - p_j|^2 + eps),
  * the force of src/RPCPUForceAtlas2.cpp:92-101 with the GPU softening eps
@@ -180,6 +195,7 @@ typedef struct {
     int32_t maxdepth, n_perturbed, depth_overflow;
     float swg_sum, etra_sum;
     int32_t linlog;                     /* 1: linear-log attraction */
+    const float *sizes;                 /* n node sizes: prevent_overlap; NULL: off */
 } orc_fa2;
 
 /* One CUDAForceAtlas2::doStep (src/RPGPUForceAtlas2.cu:206-248) in its kernel

@@ -66,6 +66,11 @@ def lib():
         L.orc_tree_repulsion.argtypes = walk_args
         L.orc_tree_repulsion_quad.restype = C.c_int32
         L.orc_tree_repulsion_quad.argtypes = walk_args
+        L.orc_tree_repulsion_overlap.restype = C.c_int32
+        L.orc_tree_repulsion_overlap.argtypes = [C.c_void_p, _f32p, _f32p, _f32p, C.c_float,
+                                                 C.c_float, C.c_float, C.c_int32, _i32p, _f32p,
+                                                 _f32p, C.POINTER(C.c_int64)]
+        L.orc_attraction_overlap.argtypes = [C.c_int64, _i32p, _i32p, _f32p, _f32p, _f32p, _f32p]
         L.orc_exact_repulsion_f64.argtypes = [C.c_int32, _f32p, _f32p, C.c_double, C.c_double,
                                               C.c_int32, _i32p, _f64p, _f64p]
         L.orc_fa2_step.restype = C.c_int32
@@ -122,15 +127,19 @@ def edge_weight_powers(weights, delta: float) -> np.ndarray:
 
 
 def gravity_attraction(g: Graph, xy: np.ndarray, k_g: float, strong: bool, linlog: bool = False,
-                       weights=None, delta: float = 0.0):
+                       weights=None, delta: float = 0.0, sizes=None):
     """Gravity plus attraction per node; with weights and delta != 0, each edge's
-    attraction times w**delta (orc_attraction_weighted)."""
+    attraction times w**delta (orc_attraction_weighted); with sizes, the
+    prevent_overlap attraction (orc_attraction_overlap)."""
     n = g.n
     fx = np.zeros(n, np.float32)
     fy = np.zeros(n, np.float32)
     p = np.ascontiguousarray(xy, np.float32).reshape(-1)
     lib().orc_gravity(n, p, g.mass, k_g, int(strong), fx, fy)
-    if weights is not None and delta != 0.0:
+    if sizes is not None:
+        lib().orc_attraction_overlap(g.m, g.sources, g.targets,
+                                     np.ascontiguousarray(sizes, np.float32), p, fx, fy)
+    elif weights is not None and delta != 0.0:
         wd = edge_weight_powers(weights, delta)
         lib().orc_attraction_weighted(g.m, g.sources, g.targets, wd, int(linlog), p, fx, fy)
     else:
@@ -190,10 +199,16 @@ class Tree:
         return dict(level=level, mass=mass, cx=cx, cy=cy, count=count)
 
     def repulsion(self, k_r: float, itolsq: float = 1.0, epssq: float = 0.05 * 0.05,
-                  group: int = 32, multipole: int = 1):
+                  group: int = 32, multipole: int = 1, sizes=None):
         fx = np.zeros(self.n, np.float32)
         fy = np.zeros(self.n, np.float32)
         visits = C.c_int64(0)
+        if sizes is not None:
+            sz = np.ascontiguousarray(sizes, np.float32)
+            ovf = lib().orc_tree_repulsion_overlap(self._t, self.xy, self.mass, sz, k_r, itolsq,
+                                                   np.float32(epssq), group, self.sort(), fx,
+                                                   fy, C.byref(visits))
+            return np.stack([fx, fy], 1), bool(ovf), visits.value
         walk = lib().orc_tree_repulsion_quad if multipole >= 2 else lib().orc_tree_repulsion
         ovf = walk(self._t, self.xy, self.mass, k_r, itolsq, np.float32(epssq),
                    group, self.sort(), fx, fy, C.byref(visits))
@@ -227,6 +242,7 @@ class _OrcFa2(C.Structure):
         ("sortd_out", C.c_void_p), ("f_ga_out", C.c_void_p), ("f_tot_out", C.c_void_p),
         ("maxdepth", C.c_int32), ("n_perturbed", C.c_int32), ("depth_overflow", C.c_int32),
         ("swg_sum", C.c_float), ("etra_sum", C.c_float), ("linlog", C.c_int32),
+        ("sizes", C.c_void_p),
     ]
 
 
@@ -234,7 +250,7 @@ class FA2:
     """The reference GPU path's iteration (CUDAForceAtlas2::doStep) restated on the CPU."""
 
     def __init__(self, g: Graph, xy: np.ndarray, k_r: float, k_g: float, strong_gravity: bool,
-                 linlog: bool = False):
+                 linlog: bool = False, sizes=None):
         self.g = g
         n = g.n
         self.xy = np.ascontiguousarray(xy, np.float32).reshape(-1).copy()
@@ -259,6 +275,9 @@ class FA2:
         s.f_tot_out = self.f_tot.ctypes.data
         s.maxdepth = 1
         s.linlog = int(linlog)
+        # prevent_overlap with these node sizes (None: off)
+        self._sizes = None if sizes is None else np.ascontiguousarray(sizes, np.float32)
+        s.sizes = None if self._sizes is None else self._sizes.ctypes.data
         self.s = s
 
     def step(self, iters: int = 1):
