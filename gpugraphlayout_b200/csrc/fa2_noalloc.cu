@@ -152,7 +152,7 @@ int run(const float *d_xy, const float *d_mass, uint32_t n, const fa2_params *pr
     b.count_status = b.sort_counts + sort_counts;
     const size_t zero_bytes = sizeof(IterCounters) + 4 * (sort_counts + count_tiles((int)n));
 
-    Params kp;
+    Params kp{};  // every field: the kernels read all of them
     kp.k_r = prm->scale;
     kp.k_g = 0.0f;
     kp.itolsq = 1.0f / (prm->theta * prm->theta);  // src/RPForceAtlas2.cpp:47
@@ -161,6 +161,7 @@ int run(const float *d_xy, const float *d_mass, uint32_t n, const fa2_params *pr
     kp.linlog = 0;
     kp.multipole = 1;
     kp.nsm = d.nsm;
+    kp.overlap = 0;
 
     // Must start at zero on every call: the counters, histograms, per-tile
     // digit counts and look-back flags; the device scalars (error and
