@@ -166,8 +166,11 @@ def run_reference(args, world, rank):
     }))
 
 
-def workload_config(n, m, theta=1.0, multipole=1, workload="rmat20"):
+def workload_config(n, m, theta=1.0, multipole=1, workload="rmat20", learned=False):
     walk = ("plain Barnes-Hut" if multipole == 1 else "Barnes-Hut with the quadrupole term")
+    if learned:
+        walk += (" with the learned far-field correction (MLP trained on R-MAT scale 16 "
+                 "layouts, FP64 targets)")
     scale, draws, width = RMAT[workload]
     return {"workload": f"R-MAT scale {scale} ({draws:,} draws, a=.57 b=.19 c=.19, seed 0), "
                         f"N={n:,} E={m:,}; positions U[-{width / 2:g},{width / 2:g}]^2; "
@@ -209,8 +212,8 @@ LEARNED = ((1.2, 1), (1.5, 1), (2.0, 1), (2.0, 2))
 EQUAL_RMSE_TARGET = 1.5  # the speed-up at equal or lower error the design aims at
 
 
-def train_learned(eng_device):
-    """One MLP per (theta, multipole) of LEARNED, trained on the engine's
+def train_learned(eng_device, combos=LEARNED):
+    """One MLP per (theta, multipole) of `combos`, trained on the engine's
     own layouts of the scale-16 R-MAT graph (gpugraphlayout_b200.learn)."""
     from gpugraphlayout_b200 import UGraph, synth
     from gpugraphlayout_b200.learn import train_correction
@@ -218,7 +221,7 @@ def train_learned(eng_device):
     g = UGraph.from_pairs(s_raw, t_raw)
     s, t = g.edges()
     out = {}
-    for theta, mp in LEARNED:
+    for theta, mp in combos:
         out[(theta, mp)] = train_correction(g.num_nodes(), s, t, theta=theta, multipole=mp,
                                             strong_gravity=STRONG, gravity=K_G, scale=K_R,
                                             width=WIDTH, device=eng_device)
@@ -396,8 +399,17 @@ def run_ours(args, world, rank, local, fp64_n=FP64_CHECKS, correction=True):
     xy0 = random_positions(n, width, width, 1234)
     eng = Engine(n, s, t, strong_gravity=STRONG, gravity=K_G, scale=K_R, device=local,
                  theta=args.theta, multipole=args.multipole)
-    plain = args.theta == 1.0 and args.multipole == 1
+    learned = getattr(args, "learned", None)
+    plain = args.theta == 1.0 and args.multipole == 1 and learned is None
     eng.set_positions(xy0)
+    train_info = None
+    if learned is not None:
+        # the workload with the learned correction at theta `learned`,
+        # trained first (outside the timed region) on the scale-16 graph
+        models, _ = train_learned(local, ((learned, args.multipole),))
+        mlp, train_info = models[(learned, args.multipole)]
+        eng.set_approximation(learned, args.multipole)
+        eng.set_learned_correction(mlp)
 
     import torch
     torch.cuda.set_device(local)
@@ -444,7 +456,7 @@ def run_ours(args, world, rank, local, fp64_n=FP64_CHECKS, correction=True):
     # the correction report compares against the plain walk, so it runs only
     # when the plain walk is the workload
     correction = (correction_report(eng, n, args.steps, local)
-                  if correction and plain and not large else None)
+                  if correction and plain and not large and not args.no_correction else None)
     fp64 = fp64_checks(eng, n, fp64_n) if large else None
     names = kernel_names()
     pk, pk_kind = peaks()
@@ -491,10 +503,14 @@ def run_ours(args, world, rank, local, fp64_n=FP64_CHECKS, correction=True):
         "warmup": max(args.warmup, 3), "ms_per_step": ms_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": workload_config(n, m, args.theta, args.multipole, args.workload),
+        "config": workload_config(n, m, args.theta if learned is None else learned,
+                                  args.multipole, args.workload, learned is not None),
         "clocks": clocks_summary(clk_path),
+        # + moment scan and per-cell a2 (quadrupole walk or learned
+        # correction), + MLP and tail (learned correction)
         "gpu_launches": (KERNELS_PER_ITER + st["sort_passes"] + (st["sort_passes"] < 8)
-                         + (2 if args.multipole == 2 else 0)) * args.steps,
+                         + (2 if args.multipole == 2 or learned is not None else 0)
+                         + (2 if learned is not None else 0)) * args.steps,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * n,
                 "d2h_bytes_per_step": 8 * n},
         "roofline": roofline,
@@ -506,6 +522,10 @@ def run_ours(args, world, rank, local, fp64_n=FP64_CHECKS, correction=True):
     }
     if fp64 is not None:
         out["fp64_checks"] = fp64
+    if train_info is not None:
+        out["learned_training"] = {k: train_info[k] for k in ("samples", "snapshots", "final_loss",
+                                                               "collect_s", "fit_s")}
+        out["learned_pairs"] = st["learned_pairs"]
     if large:
         # ncu's DRAM count above was taken at scale 20
         out["roofline"]["traffic"] = None
@@ -753,6 +773,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-correction", action="store_true",
+                    help="leave out the far-field correction report (theta sweep, learned rows)")
+    ap.add_argument("--learned", type=float, default=None,
+                    help="rmat20: time the workload with the learned correction at this theta "
+                         "(trained first on R-MAT scale 16)")
     ap.add_argument("--no-extras", action="store_true",
                     help="rmat20 at N=1 only: leave out the batched and rmat23 sub-records")
     ap.add_argument("--theta", type=float, default=1.0,
