@@ -408,7 +408,9 @@ __global__ void __launch_bounds__(kMlpThreads) k_learn_mlp(
             const int64_t nb = base + (int64_t)gridDim.x * kMlpRows;
             if (nb < rows) load_row<PAIRS>(next, nb + t, rows, s_pre, seg_cap, pairs, nodes, quad, ggeo, features);
         }
-        bool ok = mbar_wait(mbar, phase);
+        // one thread waits for the tensor cores; the others wait at the
+        // barrier and take no issue slots from the blocks beside them
+        bool ok = t == 0 ? mbar_wait(mbar, phase) : true;
         phase ^= 1u;
         if (__syncthreads_or(!ok)) {
             bad = true;
@@ -441,7 +443,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_learn_mlp(
                          kk > 0 ? 1u : 0u);
             mma_commit(mbar);
         }
-        ok = mbar_wait(mbar, phase);
+        ok = t == 0 ? mbar_wait(mbar, phase) : true;
         phase ^= 1u;
         if (__syncthreads_or(!ok)) {
             bad = true;
@@ -457,9 +459,11 @@ __global__ void __launch_bounds__(kMlpThreads) k_learn_mlp(
             tmem_load32(taddr + half * 32, v);
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                float u[8];
-#pragma unroll
-                for (int j = 0; j < 8; ++j) u[j] = v[8 * q + j] + S.w.b2[half * 32 + 8 * q + j];
+                const float4 ba = *reinterpret_cast<const float4 *>(&S.w.b2[half * 32 + 8 * q]);
+                const float4 bb = *reinterpret_cast<const float4 *>(&S.w.b2[half * 32 + 8 * q + 4]);
+                const float u[8] = {v[8 * q] + ba.x,     v[8 * q + 1] + ba.y, v[8 * q + 2] + ba.z,
+                                    v[8 * q + 3] + ba.w, v[8 * q + 4] + bb.x, v[8 * q + 5] + bb.y,
+                                    v[8 * q + 6] + bb.z, v[8 * q + 7] + bb.w};
                 put_packed(S.h, t, half * 4 + q, 8,
                            make_uint4(pack_bf16_relu(u[0], u[1]), pack_bf16_relu(u[2], u[3]),
                                       pack_bf16_relu(u[4], u[5]), pack_bf16_relu(u[6], u[7])));
@@ -476,7 +480,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_learn_mlp(
                          kk > 0 ? 1u : 0u);
             mma_commit(mbar);
         }
-        ok = mbar_wait(mbar, phase);
+        ok = t == 0 ? mbar_wait(mbar, phase) : true;
         phase ^= 1u;
         if (__syncthreads_or(!ok)) {
             bad = true;
@@ -523,8 +527,8 @@ __global__ void __launch_bounds__(kMlpThreads) k_learn_mlp(
             out[row] = make_float2(y0, y1);
         }
     }
-    if (bad) {
-        if (t == 0) atomicOr(err, kErrMlpWait);
+    if (bad && t == 0) {
+        atomicOr(err, kErrMlpWait);
         mbar_wait(mbar, phase ^ 1u);  // the MMAs in flight, bounded again
     }
     tc_fence_before();
