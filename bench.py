@@ -53,8 +53,8 @@ KERNELS_PER_ITER = 6
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_attract
 # launch at this workload, from an ncu capture of
 #   ncu --set full --clock-control none -k regex:k_attract -s 4 -c 1 \
-#       python bench.py --steps 3 --warmup 3 --no-cpu-baseline
-ATTRACT_TRAFFIC_BYTES = 146_956_800
+#       python bench.py --steps 5 --warmup 3 --no-cpu-baseline --no-extras --no-correction
+ATTRACT_TRAFFIC_BYTES = 144_444_160
 
 
 def clocks_sampler(device: int, path: str):
