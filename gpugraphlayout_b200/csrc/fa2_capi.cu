@@ -275,9 +275,8 @@ void enqueue_iteration(fa2_ctx *c, bool full, bool perturb_first, bool timed) {
             cudaEventRecordWithFlags(c->slot_events[slot * 2 + end], s, cudaEventRecordExternal);
     };
     const bool learn = c->learn_on;
-    // the moment scan and per-cell second moments: the quadrupole walk and
-    // the learned correction's features use them
-    const bool quad = c->kp.multipole >= 2 || learn;
+    // the moment scan and per-cell second moments of the quadrupole walk
+    const bool quad = c->kp.multipole >= 2;
     const bool side = full && c->overlap;  // stream B carries the attraction
     cudaMemsetAsync(c->scratch, 0, c->scratch_bytes, A);
     if (learn) cudaMemsetAsync(c->lb.corr, 0, ((size_t)c->n + 31) / 32 * sizeof(float2), A);
@@ -1212,8 +1211,7 @@ int fa2_set_learned_correction(fa2_ctx *c, const fa2_mlp *mlp) {
     if (!mlp_is_finite(*mlp)) return FA2_ERR_INVALID_ARGUMENT;
     if (c->kp.overlap) return FA2_ERR_UNSUPPORTED;
     mlp_blocks_per_sm();  // the launch shape, settled outside any graph capture
-    int s = ensure_quad_buffers(c);
-    if (!s) s = ensure_learn_buffers(c);
+    int s = ensure_learn_buffers(c);
     if (s) return s;
     MlpDevice host;
     mlp_to_device(*mlp, host);
@@ -1354,7 +1352,7 @@ int fa2_learn_collect(fa2_learn_set *set, fa2_ctx *c, float theta, int32_t multi
     CK(cudaSetDevice(c->device));
     if (c->n == 0) return FA2_OK;
     CK(cudaStreamSynchronize(c->sA));
-    int s = ensure_quad_buffers(c);
+    int s = multipole >= 2 ? ensure_quad_buffers(c) : FA2_OK;
     if (!s) s = ensure_learn_buffers(c);
     if (!s) s = set_staging(set, (int64_t)c->lb.seg_cap * kPairSegments);
     if (s) return s;
@@ -1368,10 +1366,10 @@ int fa2_learn_collect(fa2_learn_set *set, fa2_ctx *c, float theta, int32_t multi
     CK(cudaMemsetAsync(set->st_count, 0, sizeof(unsigned long long), A));
     launch_keys(b, c->nsm, A);
     launch_sort(b, A);
-    launch_tree_count(b, true, A);
-    launch_moments(b, A);
+    launch_tree_count(b, multipole >= 2, A);
+    if (multipole >= 2) launch_moments(b, A);
     launch_emit(b, c->nsm, A);
-    launch_quad_cells(b, c->nsm, A);
+    if (multipole >= 2) launch_quad_cells(b, c->nsm, A);
     launch_traverse_learn(b, kp, c->lb, c->trav_blocks, A);
     launch_learn_targets(b, kp, c->lb, set->st_feat, set->st_tgt, set->st_w, set->st_key,
                          set->st_count, (uint64_t)set->st_cap, c->nsm, A);

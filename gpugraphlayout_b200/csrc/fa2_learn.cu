@@ -22,13 +22,35 @@ constexpr unsigned kFull = kFullMask;
 
 // ------------------------------------------------------------- features --
 
+// The complex second moment of a cell about its centre of mass Z as its
+// children (at most four, in preorder after the cell; the first four bodies
+// of a run of coincident keys) give it: sum_c m_c (z_c - Z)^2.  It leaves out
+// each child's own second moment, so it is a feature, not the quadrupole
+// term; it needs no moment scan, only the tree.
+__device__ __forceinline__ float2 children_a2(const float4 *__restrict nodes, uint32_t g,
+                                              float4 cell) {
+    const uint32_t end = meta_next(__float_as_int(cell.w));
+    uint32_t c = g + 1;
+    float ar = 0.0f, ai = 0.0f;
+#pragma unroll 1
+    for (int q = 0; q < 4 && c < end; ++q) {
+        const float4 ch = nodes[c];
+        const float dx = ch.x - cell.x, dy = ch.y - cell.y;
+        ar = fmaf(ch.z, dx * dx - dy * dy, ar);
+        ai = fmaf(ch.z, 2.0f * dx * dy, ai);
+        c = meta_next(__float_as_int(ch.w));  // the node after the child's subtree
+    }
+    return make_float2(ar, ai);
+}
+
 // The 12 features of a (group, cell) pair, in the frame turned so that the
 // direction from the cell's centre of mass Z to the group's centroid g is the
 // first axis, lengths over d = |g - Z|:
 //   0  h / d               cell width h = 2 radius / 2^level
 //   1  s / d               group spread s (root of the mean squared distance
 //                          of its bodies from g)
-//   2,3 a2 / (M d^2)       the cell's complex second moment about Z, turned
+//   2,3 a2 / (M d^2)       the cell's complex second moment about Z as its
+//                          children give it (children_a2), turned
 //   4,5 b2 / d^2           the group's complex second moment about g, turned
 //   6  |a2| / (M h^2)      how far the cell's mass sits from its centre
 //   7  log2(d^2 / dq) / 8  margin over the walk's acceptance threshold dq
@@ -289,7 +311,7 @@ __device__ __forceinline__ void load_row(RowInputs &r, int64_t row, int64_t rows
     if (PAIRS) {
         r.pair = pairs[pair_index(row, pre, seg_cap)];
         r.cell = nodes[r.pair.y];
-        r.a2 = quad[r.pair.y];
+        r.a2 = children_a2(nodes, r.pair.y, r.cell);
         r.g0 = ggeo[2 * r.pair.x];
         r.g1 = ggeo[2 * r.pair.x + 1];
     } else {
@@ -574,7 +596,7 @@ __global__ void __launch_bounds__(256) k_learn_targets(
         const uint2 pr = pairs[pair_index(p, s_pre, seg_cap)];
         const uint32_t w = pr.x, node = pr.y;
         const float4 cell = nodes[node];
-        const float2 a2 = quad[node];
+        const float2 a2 = children_a2(nodes, node, cell);
         float f[kLearnIn], sig, c, s;
         if (!pair_features(cell, a2, ggeo[2 * w], ggeo[2 * w + 1], radius, prm.itolsq,
                            prm.epssq, f, sig, c, s))
@@ -613,8 +635,9 @@ __global__ void __launch_bounds__(256) k_learn_targets(
             const float xx = ux * ux, yy = uy * uy;
             const float ur = ux * fmaf(-3.0f, yy, xx);
             const float ui = uy * fmaf(-3.0f, xx, yy);
-            bx = fmaf(a2.x, ur, fmaf(-a2.y, ui, bx));
-            by = fmaf(-a2.x, ui, fmaf(-a2.y, ur, by));
+            const float2 q = quad[node];  // the walk's own (exact) a2
+            bx = fmaf(q.x, ur, fmaf(-q.y, ui, bx));
+            by = fmaf(-q.x, ui, fmaf(-q.y, ur, by));
         } else {
             const float cm = __fdividef(cell.z, d2f);
             bx = dxf * cm;
