@@ -61,6 +61,7 @@ struct fa2_ctx {
     int bbox_blocks = 0, trav_blocks = 0;
     cudaStream_t sA = nullptr, sB = nullptr;
     cudaEvent_t evFork = nullptr, evJoin = nullptr, evCounted = nullptr;
+    cudaEvent_t evEmitted = nullptr, evA2 = nullptr;  // the learned cells' a2 pass on stream B
     // graphs
     cudaGraphExec_t exec = nullptr;
     cudaGraphExec_t exec_timed = nullptr;
@@ -133,7 +134,8 @@ int ensure_quad_buffers(fa2_ctx *c) {
 
 // Buffers of the learned correction, allocated when it is first used: the
 // pair list (up to 32 pairs per body), the groups' geometry and corrections,
-// the sorted bodies' repulsion and the MLP's weights.
+// the sorted bodies' repulsion, the cells' second moments and the MLP's
+// weights.
 int ensure_learn_buffers(fa2_ctx *c) {
     LearnBuffers &lb = c->lb;
     const size_t groups = ((size_t)c->n + 31) / 32;
@@ -146,6 +148,7 @@ int ensure_learn_buffers(fa2_ctx *c) {
         (!lb.ggeo && (s = dalloc(c, &lb.ggeo, 2 * groups))) ||
         (!lb.rep && (s = dalloc(c, &lb.rep, (size_t)c->n))) ||
         (!lb.corr && (s = dalloc(c, &lb.corr, groups))) ||
+        (!lb.a2 && (s = dalloc(c, &lb.a2, c->b.capacity))) ||
         (!c->d_mlp && (s = dalloc(c, &c->d_mlp, 1))))
         return s;
     lb.seg_cap = (uint32_t)seg;
@@ -164,6 +167,8 @@ void free_all(fa2_ctx *c) {
     if (c->evFork) cudaEventDestroy(c->evFork);
     if (c->evJoin) cudaEventDestroy(c->evJoin);
     if (c->evCounted) cudaEventDestroy(c->evCounted);
+    if (c->evEmitted) cudaEventDestroy(c->evEmitted);
+    if (c->evA2) cudaEventDestroy(c->evA2);
     if (c->sA) cudaStreamDestroy(c->sA);
     if (c->sB) cudaStreamDestroy(c->sB);
 }
@@ -319,6 +324,20 @@ void enqueue_iteration(fa2_ctx *c, bool full, bool perturb_first, bool timed) {
     mark(S_EMIT, 0, A);
     launch_emit(b, c->nsm, A);
     mark(S_EMIT, 1, A);
+    if (learn) {
+        // the cells' second moments (a feature of the pairs), beside the walk
+        // on stream B when it is in use; the MLP waits for them
+        cudaStream_t M = side ? B : A;
+        if (side) {
+            cudaEventRecord(c->evEmitted, A);
+            cudaStreamWaitEvent(B, c->evEmitted, 0);
+        }
+        // timed in the moments slot, which the monopole walk leaves free
+        if (!quad) mark(S_MOM, 0, M);
+        launch_cell_a2(b, c->lb, c->nsm, M);
+        if (!quad) mark(S_MOM, 1, M);
+        if (side) cudaEventRecord(c->evA2, B);
+    }
     if (side) cudaStreamWaitEvent(A, c->evJoin, 0);
     if (quad) {
         mark(S_QUAD, 0, A);
@@ -333,6 +352,7 @@ void enqueue_iteration(fa2_ctx *c, bool full, bool perturb_first, bool timed) {
         launch_traverse(b, c->kp, c->trav_blocks, A);
     mark(S_TRAV, 1, A);
     if (learn) {
+        if (side) cudaStreamWaitEvent(A, c->evA2, 0);
         mark(S_LEARN, 0, A);
         launch_learn_mlp(b, c->kp, c->lb, c->nsm, A);
         launch_learn_tail(b, c->kp, c->lb, c->nsm, A);
@@ -562,9 +582,9 @@ bool mlp_is_finite(const fa2_mlp &m) {
     return true;
 }
 
-// The FP32 parameters as the kernels read them (MlpDevice): W1 and W2 in BF16
-// in the tensor cores' operand layout (W1's K padded from 12 to 16 with
-// zeros), W3 as BF16 values in {W3[0][j], W3[1][j]} pairs, biases as given.
+// The FP32 parameters as the kernels read them (MlpDevice): W1, W2 and W3 in
+// BF16 in the tensor cores' operand layout, b1 and b2 as BF16 pairs (value and
+// rest) in W1's and W2's extra K columns, W3 padded to 16 rows, b3 as given.
 void mlp_to_device(const fa2_mlp &m, MlpDevice &d) {
     memset(&d, 0, sizeof(d));
     for (int j = 0; j < kLearnHidden; ++j) {
@@ -576,11 +596,16 @@ void mlp_to_device(const fa2_mlp &m, MlpDevice &d) {
             if (k == kBiasColLo) v = bf16_bits(m.b1[j] - bf16_value(m.b1[j]));
             d.w1[operand_offset(j, k, kLearnInPad / 8) / 2] = v;
         }
-        for (int k = 0; k < kLearnHidden; ++k)
-            d.w2[operand_offset(j, k, kLearnHidden / 8) / 2] = bf16_bits(m.w2[j * kLearnHidden + k]);
+        for (int k = 0; k < kLearnHidPad; ++k) {
+            uint16_t v = 0;
+            if (k < kLearnHidden) v = bf16_bits(m.w2[j * kLearnHidden + k]);
+            // b2 = hi + lo against the hidden tile's two columns of ones
+            if (k == kBias2ColHi) v = bf16_bits(m.b2[j]);
+            if (k == kBias2ColLo) v = bf16_bits(m.b2[j] - bf16_value(m.b2[j]));
+            d.w2[operand_offset(j, k, kLearnHidPad / 8) / 2] = v;
+        }
         for (int o = 0; o < kLearnOut; ++o)
             d.w3[operand_offset(o, j, kLearnHidden / 8) / 2] = bf16_bits(m.w3[o * kLearnHidden + j]);
-        d.b2[j] = m.b2[j];
     }
     d.b3[0] = m.b3[0];
     d.b3[1] = m.b3[1];
@@ -826,7 +851,9 @@ fa2_ctx *fa2_create(const fa2_graph_desc *g, const fa2_params *prm, int *status)
         cudaStreamCreateWithPriority(&c->sB, cudaStreamNonBlocking, prio_low) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->evFork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->evJoin, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->evCounted, cudaEventDisableTiming) != cudaSuccess)
+        cudaEventCreateWithFlags(&c->evCounted, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->evEmitted, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->evA2, cudaEventDisableTiming) != cudaSuccess)
         return fail(FA2_ERR_CUDA);
     c->slot_events.resize(kNumSlots * 2);
     for (auto &e : c->slot_events)
@@ -1370,6 +1397,7 @@ int fa2_learn_collect(fa2_learn_set *set, fa2_ctx *c, float theta, int32_t multi
     if (multipole >= 2) launch_moments(b, A);
     launch_emit(b, c->nsm, A);
     if (multipole >= 2) launch_quad_cells(b, c->nsm, A);
+    launch_cell_a2(b, c->lb, c->nsm, A);
     launch_traverse_learn(b, kp, c->lb, c->trav_blocks, A);
     launch_learn_targets(b, kp, c->lb, set->st_feat, set->st_tgt, set->st_w, set->st_key,
                          set->st_count, (uint64_t)set->st_cap, c->nsm, A);

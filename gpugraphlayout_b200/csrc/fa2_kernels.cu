@@ -170,9 +170,7 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
     __shared__ float s_dq[64];
     __shared__ bool s_last;
     __shared__ float s_red[2][kTravThreads / kWarp];
-    __shared__ uint32_t s_pair[LEARN ? kTravThreads : 1];
     if (st->err || st->poison) return;
-    uint32_t *my_pairs = s_pair + (LEARN ? (threadIdx.x & ~31u) : 0u);
     if (threadIdx.x == 0) {
         // src/RPBHKernels.cu:579-592: dq for the children of the root is
         // (2 radius)^2 / theta^2 + eps, quartering per level.
@@ -210,7 +208,10 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
         // k_r m_i multiplies the sum once at the end
         float ax = 0.0f, ay = 0.0f;
         uint32_t node = 1;
-        int npend = 0;  // LEARN: accepted cells waiting in my_pairs
+        // LEARN: the warp's accepted cells not yet written out; lane j holds
+        // the j-th of them
+        int npend = 0;
+        uint32_t my_cell = 0;
         if (LEARN) {
             // the group's centroid and second moments about it
             const float cnt = (float)__popc(__ballot_sync(kFull, active));
@@ -237,7 +238,6 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
         // LEARN: the pending cells to this warp's segment of the pair list,
         // one atomic per flush
         auto flush = [&]() {
-            __syncwarp();
             const uint32_t seg = (blockIdx.x * (kTravThreads / kWarp) + (threadIdx.x >> 5)) %
                                  (uint32_t)kPairSegments;
             uint32_t base = 0;
@@ -245,9 +245,8 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
             base = __shfl_sync(kFull, base, 0);
             if (lane < npend && base + lane < lb.seg_cap)
                 lb.pairs[(size_t)seg * lb.seg_cap + base + lane] =
-                    make_uint2((uint32_t)w, my_pairs[lane]);
+                    make_uint2((uint32_t)w, my_cell);
             if (lane == 0 && base + (uint32_t)npend > lb.seg_cap) atomicOr(&st->err, kErrPairs);
-            __syncwarp();
             npend = 0;
         };
         // An opened cell's first child is node + 1 and always exists, so only
@@ -269,7 +268,7 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
                     ax = fmaf(dx, c, ax);
                     ay = fmaf(dy, c, ay);
                     if (LEARN && meta_level(meta) != kBodyLevel) {
-                        if (lane == 0) my_pairs[npend] = node;
+                        if (lane == npend) my_cell = node;
                         if (++npend == 32) flush();
                     }
                     node = meta_next(meta);
@@ -310,7 +309,7 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
                         ax = fmaf(q.x, ur, fmaf(-q.y, ui, ax));
                         ay = fmaf(-q.x, ui, fmaf(-q.y, ur, ay));
                         if (LEARN) {
-                            if (lane == 0) my_pairs[npend] = node;
+                            if (lane == npend) my_cell = node;
                             if (++npend == 32) flush();
                         }
                     }
@@ -962,10 +961,9 @@ int traverse_blocks_per_sm() {
     cudaFuncSetAttribute(k_traverse<true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
     cudaFuncSetAttribute(k_traverse<false, false, true>,
                          cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-    // the learned walk keeps 4 KB of pending pairs per block: the smallest
-    // shared-memory share that holds two blocks
-    cudaFuncSetAttribute(k_traverse<false, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 8);
-    cudaFuncSetAttribute(k_traverse<true, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 8);
+    // the learned walk keeps its pending pairs in registers, one per lane
+    cudaFuncSetAttribute(k_traverse<false, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+    cudaFuncSetAttribute(k_traverse<true, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
     int nb = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_traverse<false, false>, kTravThreads, 0);
     return nb < 1 ? 1 : nb;

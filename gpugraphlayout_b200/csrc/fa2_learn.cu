@@ -43,6 +43,19 @@ __device__ __forceinline__ float2 children_a2(const float4 *__restrict nodes, ui
     return make_float2(ar, ai);
 }
 
+// children_a2 of every cell of the tree, one thread per node; bodies are
+// skipped (no pair has one).
+__global__ void __launch_bounds__(256) k_cell_a2(const float4 *__restrict nodes,
+                                                 const DevState *st, float2 *__restrict a2) {
+    if (st->err || st->poison) return;
+    const uint32_t end = st->tree_nodes;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x + 1; i < end;
+         i += gridDim.x * blockDim.x) {
+        const float4 cell = nodes[i];
+        if (meta_level(__float_as_int(cell.w)) != kBodyLevel) a2[i] = children_a2(nodes, i, cell);
+    }
+}
+
 // The 12 features of a (group, cell) pair, in the frame turned so that the
 // direction from the cell's centre of mass Z to the group's centroid g is the
 // first axis, lengths over d = |g - Z|:
@@ -238,10 +251,16 @@ constexpr int kMlpThreads = 128;
 constexpr uint32_t kMlpTmemCols = 64;  // both layers' accumulators, in turn
 constexpr uint32_t kIdesc = instr_desc_bf16(kMlpRows, kLearnHidden);
 constexpr uint32_t kIdescOut = instr_desc_bf16(kMlpRows, kLearnOutPad);
+constexpr int kTileChunks = kLearnHidPad / 8;  // 16-byte K chunks per row of the tile
 
+// The tile is the A operand of all three layers, one row per thread, K-major
+// with kTileChunks chunks a row: the features (chunks 0-1) for layer 1, the
+// first hidden layer (chunks 0-7) and two columns of ones for b2 (chunk 8,
+// written once; chunk 9 zeros) for layer 2, the second hidden layer (chunks
+// 0-7) for the output layer.  Each is written after the MMAs that read the
+// previous one have completed.
 struct MlpSmem {
-    uint8_t a[kMlpRows * kLearnInPad * 2];    // features, BF16, K-major operand layout
-    uint8_t h[kMlpRows * kLearnHidden * 2];   // a hidden layer, BF16
+    uint8_t h[kMlpRows * kLearnHidPad * 2];   // BF16 operand tile
     MlpDevice w;                              // weights (W1, W2, W3 in operand layout)
     unsigned long long mbar;
     uint32_t tmem_base;
@@ -249,6 +268,9 @@ struct MlpSmem {
 static_assert(sizeof(MlpDevice) % 16 == 0, "weights are copied in 16-byte pieces");
 static_assert(offsetof(MlpSmem, h) % 16 == 0 && offsetof(MlpSmem, w) % 16 == 0,
               "operand tiles start on 16-byte boundaries");
+static_assert(kLearnHidPad % 16 == 0 && kBias2ColLo < kLearnHidPad && kBias2ColHi / 8 == 8 &&
+                  kBias2ColLo / 8 == 8,
+              "b2's columns of ones fill the start of chunk 8");
 
 // Writes 8 packed BF16 pairs' worth (16 bytes) as K chunk `chunk` of row r.
 __device__ __forceinline__ void put_packed(uint8_t *tile, int r, int chunk, int kchunks,
@@ -304,14 +326,14 @@ __device__ __forceinline__ void load_row(RowInputs &r, int64_t row, int64_t rows
                                          const uint32_t *pre, uint32_t seg_cap,
                                          const uint2 *__restrict pairs,
                                          const float4 *__restrict nodes,
-                                         const float2 *__restrict quad,
+                                         const float2 *__restrict cell_a2,
                                          const float4 *__restrict ggeo,
                                          const float *__restrict features) {
     if (row >= rows) return;
     if (PAIRS) {
         r.pair = pairs[pair_index(row, pre, seg_cap)];
         r.cell = nodes[r.pair.y];
-        r.a2 = children_a2(nodes, r.pair.y, r.cell);
+        r.a2 = cell_a2[r.pair.y];
         r.g0 = ggeo[2 * r.pair.x];
         r.g1 = ggeo[2 * r.pair.x + 1];
     } else {
@@ -321,11 +343,13 @@ __device__ __forceinline__ void load_row(RowInputs &r, int64_t row, int64_t rows
 }
 
 // The MLP over rows of 12 features, 128 rows per tile and thread block (one
-// row per thread).  Layer 1 (K = 16, the 12 features padded with zeros) and
-// layer 2 (K = 64) are 128 x 64 tcgen05 MMAs with BF16 operands from shared
-// memory and FP32 accumulators in tensor memory; each thread reads its row
-// back with tcgen05.ld, adds the bias, applies ReLU and rounds to BF16.  The
-// 64 -> 2 output layer runs on the CUDA cores in FP32 over the BF16 values.
+// row per thread).  Layer 1 (K = 16: the 12 features, two columns of ones
+// against b1's two BF16 parts, zeros) and layer 2 (K = 80: the 64 hidden
+// units, two columns of ones against b2's parts, zeros) are 128 x 64 tcgen05
+// MMAs with BF16 operands from shared memory and FP32 accumulators in tensor
+// memory; each thread reads its row back with tcgen05.ld, applies ReLU and
+// rounds to BF16 in one instruction per pair.  The output layer is a
+// 128 x 16 MMA (W3's two rows and zeros) plus b3 in FP32.
 //
 // PAIRS: rows are the pairs of a learned iteration; the features come from
 // the tree, the group geometry and the cell moments, and each output, turned
@@ -338,8 +362,9 @@ __device__ __forceinline__ void load_row(RowInputs &r, int64_t row, int64_t rows
 template <bool PAIRS>
 __global__ void __launch_bounds__(kMlpThreads) k_learn_mlp(
     const uint2 *__restrict pairs, const IterCounters *ctr, uint32_t seg_cap,
-    const float4 *__restrict nodes, const float2 *__restrict quad, const float4 *__restrict ggeo,
-    const DevState *st, Params prm, float2 *__restrict corr, const float *__restrict features,
+    const float4 *__restrict nodes, const float2 *__restrict cell_a2,
+    const float4 *__restrict ggeo, const DevState *st, Params prm, float2 *__restrict corr,
+    const float *__restrict features,
     int64_t nrows, float2 *__restrict out, const MlpDevice *__restrict mlp, int *err) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     MlpSmem &S = *reinterpret_cast<MlpSmem *>(smem_raw);
@@ -352,6 +377,10 @@ __global__ void __launch_bounds__(kMlpThreads) k_learn_mlp(
         int4 *dst = reinterpret_cast<int4 *>(&S.w);
         for (int i = t; i < (int)(sizeof(MlpDevice) / 16); i += kMlpThreads) dst[i] = src[i];
     }
+    // this row's columns of ones against b2 (chunk 8) and the zeros after
+    // them (chunk 9); the epilogues and the features never write these chunks
+    put_packed(S.h, t, kBias2ColHi / 8, kTileChunks, make_uint4(0x3F803F80u, 0u, 0u, 0u));
+    put_packed(S.h, t, kBias2ColHi / 8 + 1, kTileChunks, make_uint4(0u, 0u, 0u, 0u));
     const uint32_t mbar = smem_u32(&S.mbar);
     if (t == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
@@ -370,11 +399,10 @@ __global__ void __launch_bounds__(kMlpThreads) k_learn_mlp(
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = S.tmem_base;
-    const uint64_t da = operand_desc(smem_u32(S.a), 128, 2 * 128);
-    const uint64_t dw1 = operand_desc(smem_u32(S.w.w1), 128, 2 * 128);
-    const uint64_t dh = operand_desc(smem_u32(S.h), 128, 8 * 128);
-    const uint64_t dw2 = operand_desc(smem_u32(S.w.w2), 128, 8 * 128);
-    const uint64_t dw3 = operand_desc(smem_u32(S.w.w3), 128, 8 * 128);
+    const uint64_t dh = operand_desc(smem_u32(S.h), 128, kTileChunks * 128);
+    const uint64_t dw1 = operand_desc(smem_u32(S.w.w1), 128, (kLearnInPad / 8) * 128);
+    const uint64_t dw2 = operand_desc(smem_u32(S.w.w2), 128, kTileChunks * 128);
+    const uint64_t dw3 = operand_desc(smem_u32(S.w.w3), 128, (kLearnHidden / 8) * 128);
     // this warp's 32 TMEM lanes (warp q of the block reads lanes 32q..32q+31)
     const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
     const float radius = PAIRS ? st->trav_radius : 0.0f;
@@ -386,7 +414,8 @@ __global__ void __launch_bounds__(kMlpThreads) k_learn_mlp(
     // tensor cores work on the current one.
     RowInputs next;
     int64_t base = (int64_t)blockIdx.x * kMlpRows;
-    if (base < rows) load_row<PAIRS>(next, base + t, rows, s_pre, seg_cap, pairs, nodes, quad, ggeo, features);
+    if (base < rows) load_row<PAIRS>(next, base + t, rows, s_pre, seg_cap, pairs, nodes, cell_a2, ggeo,
+                                     features);
     for (; base < rows; base += (int64_t)gridDim.x * kMlpRows) {
         const int64_t row = base + t;
         const RowInputs in = next;
@@ -416,19 +445,20 @@ __global__ void __launch_bounds__(kMlpThreads) k_learn_mlp(
         // the columns that meet b1's two parts in W1
         f[kBiasColHi] = 1.0f;
         f[kBiasColLo] = 1.0f;
-        put_chunk(S.a, t, 0, 2, f);
-        put_chunk(S.a, t, 1, 2, f + 8);
+        put_chunk(S.h, t, 0, kTileChunks, f);
+        put_chunk(S.h, t, 1, kTileChunks, f + 8);
         fence_async_smem();
         tc_fence_before();
         __syncthreads();
         if (t == 0) {
             tc_fence_after();
-            mma_bf16(tmem, da, dw1, kIdesc, 0);
+            mma_bf16(tmem, dh, dw1, kIdesc, 0);
             mma_commit(mbar);
         }
         {
             const int64_t nb = base + (int64_t)gridDim.x * kMlpRows;
-            if (nb < rows) load_row<PAIRS>(next, nb + t, rows, s_pre, seg_cap, pairs, nodes, quad, ggeo, features);
+            if (nb < rows) load_row<PAIRS>(next, nb + t, rows, s_pre, seg_cap, pairs, nodes, cell_a2, ggeo,
+                                        features);
         }
         // one thread waits for the tensor cores; the others wait at the
         // barrier and take no issue slots from the blocks beside them
@@ -440,7 +470,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_learn_mlp(
         }
         tc_fence_after();
         // layer 1 (its bias came with the MMA): ReLU and BF16 into the
-        // hidden operand tile
+        // operand tile
 #pragma unroll
         for (int half = 0; half < 2; ++half) {
             float v[32];
@@ -448,7 +478,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_learn_mlp(
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 const float *u = v + 8 * q;
-                put_packed(S.h, t, half * 4 + q, 8,
+                put_packed(S.h, t, half * 4 + q, kTileChunks,
                            make_uint4(pack_bf16_relu(u[0], u[1]), pack_bf16_relu(u[2], u[3]),
                                       pack_bf16_relu(u[4], u[5]), pack_bf16_relu(u[6], u[7])));
             }
@@ -458,9 +488,9 @@ __global__ void __launch_bounds__(kMlpThreads) k_learn_mlp(
         __syncthreads();
         if (t == 0) {
             tc_fence_after();
-            // K = 64 in four steps of 16: the next two K chunks, 256 bytes on
+            // K = 80 in five steps of 16: the next two K chunks, 256 bytes on
 #pragma unroll
-            for (int kk = 0; kk < kLearnHidden / 16; ++kk)
+            for (int kk = 0; kk < kLearnHidPad / 16; ++kk)
                 mma_bf16(tmem, dh + (uint64_t)(kk * 16), dw2 + (uint64_t)(kk * 16), kIdesc,
                          kk > 0 ? 1u : 0u);
             mma_commit(mbar);
@@ -472,21 +502,17 @@ __global__ void __launch_bounds__(kMlpThreads) k_learn_mlp(
             break;
         }
         tc_fence_after();
-        // layer 2: bias, ReLU, BF16 into the hidden tile again (layer 2's
-        // MMAs have read it); then the output layer, N = 16 of which the
-        // first two columns are W3's rows
+        // layer 2 (its bias came with the MMA): ReLU and BF16 into the
+        // operand tile again (layer 2's MMAs have read it); then the output
+        // layer, N = 16 of which the first two columns are W3's rows
 #pragma unroll
         for (int half = 0; half < 2; ++half) {
             float v[32];
             tmem_load32(taddr + half * 32, v);
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                const float4 ba = *reinterpret_cast<const float4 *>(&S.w.b2[half * 32 + 8 * q]);
-                const float4 bb = *reinterpret_cast<const float4 *>(&S.w.b2[half * 32 + 8 * q + 4]);
-                const float u[8] = {v[8 * q] + ba.x,     v[8 * q + 1] + ba.y, v[8 * q + 2] + ba.z,
-                                    v[8 * q + 3] + ba.w, v[8 * q + 4] + bb.x, v[8 * q + 5] + bb.y,
-                                    v[8 * q + 6] + bb.z, v[8 * q + 7] + bb.w};
-                put_packed(S.h, t, half * 4 + q, 8,
+                const float *u = v + 8 * q;
+                put_packed(S.h, t, half * 4 + q, kTileChunks,
                            make_uint4(pack_bf16_relu(u[0], u[1]), pack_bf16_relu(u[2], u[3]),
                                       pack_bf16_relu(u[4], u[5]), pack_bf16_relu(u[6], u[7])));
             }
@@ -580,7 +606,8 @@ template <bool QUAD>
 __global__ void __launch_bounds__(256) k_learn_targets(
     int n, const uint2 *__restrict pairs, const IterCounters *ctr, uint32_t seg_cap,
     const float4 *__restrict nodes, const float2 *__restrict quad,
-    const uint32_t *__restrict owner, const uint32_t *__restrict body_node,
+    const float2 *__restrict cell_a2, const uint32_t *__restrict owner,
+    const uint32_t *__restrict body_node,
     const float4 *__restrict ggeo, const DevState *st, Params prm, float *__restrict features,
     float2 *__restrict targets, float *__restrict weights, uint64_t *__restrict keys,
     unsigned long long *count, uint64_t cap) {
@@ -596,7 +623,7 @@ __global__ void __launch_bounds__(256) k_learn_targets(
         const uint2 pr = pairs[pair_index(p, s_pre, seg_cap)];
         const uint32_t w = pr.x, node = pr.y;
         const float4 cell = nodes[node];
-        const float2 a2 = children_a2(nodes, node, cell);
+        const float2 a2 = cell_a2[node];
         float f[kLearnIn], sig, c, s;
         if (!pair_features(cell, a2, ggeo[2 * w], ggeo[2 * w + 1], radius, prm.itolsq,
                            prm.epssq, f, sig, c, s))
@@ -942,7 +969,7 @@ int mlp_blocks_per_sm() {
 void launch_learn_mlp(const Buffers &b, const Params &p, const LearnBuffers &lb, int nsm,
                       cudaStream_t s) {
     k_learn_mlp<true><<<nsm * mlp_blocks_per_sm(), kMlpThreads, mlp_smem_bytes(), s>>>(
-        lb.pairs, b.ctr, lb.seg_cap, b.nodes, b.quad, lb.ggeo, b.st, p, lb.corr, nullptr, 0,
+        lb.pairs, b.ctr, lb.seg_cap, b.nodes, lb.a2, lb.ggeo, b.st, p, lb.corr, nullptr, 0,
         nullptr, lb.mlp, &b.st->err);
 }
 
@@ -958,6 +985,10 @@ void launch_mlp_rows(const MlpDevice *mlp, const float *features, int64_t n, flo
         mlp, err);
 }
 
+void launch_cell_a2(const Buffers &b, const LearnBuffers &lb, int nsm, cudaStream_t s) {
+    k_cell_a2<<<nsm * 8, 256, 0, s>>>(b.nodes, b.st, lb.a2);
+}
+
 void launch_learn_tail(const Buffers &b, const Params &p, const LearnBuffers &lb, int nsm,
                        cudaStream_t s) {
     k_learn_tail<<<nsm * (2048 / kTravThreads), kTravThreads, 0, s>>>(
@@ -970,11 +1001,13 @@ void launch_learn_targets(const Buffers &b, const Params &p, const LearnBuffers 
                           unsigned long long *count, uint64_t cap, int nsm, cudaStream_t s) {
     if (p.multipole >= 2)
         k_learn_targets<true><<<nsm * 8, 256, 0, s>>>(
-            b.n, lb.pairs, b.ctr, lb.seg_cap, b.nodes, b.quad, b.owner, b.body_node, lb.ggeo,
+            b.n, lb.pairs, b.ctr, lb.seg_cap, b.nodes, b.quad, lb.a2, b.owner, b.body_node,
+            lb.ggeo,
             b.st, p, features, targets, weights, keys, count, cap);
     else
         k_learn_targets<false><<<nsm * 8, 256, 0, s>>>(
-            b.n, lb.pairs, b.ctr, lb.seg_cap, b.nodes, b.quad, b.owner, b.body_node, lb.ggeo,
+            b.n, lb.pairs, b.ctr, lb.seg_cap, b.nodes, b.quad, lb.a2, b.owner, b.body_node,
+            lb.ggeo,
             b.st, p, features, targets, weights, keys, count, cap);
 }
 

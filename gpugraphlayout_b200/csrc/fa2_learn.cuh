@@ -38,15 +38,18 @@ constexpr float kLearnMaxOut = 1.0f;
 // core matrices, the K chunks of an 8-row group 128 bytes apart, 8-row groups
 // one row of chunks apart).  W1's 16 K columns are the 12 features, then the
 // bias b1 split into two BF16 parts (its rounding and the rest) that meet an
-// input column of ones, then zeros.  W3 is padded to 16 output rows (N = 16
-// is the smallest MMA width at M = 128).  b2 and b3 stay FP32.
+// input column of ones, then zeros.  W2's 80 K columns are the 64 hidden
+// units, then b2 split the same way against two more columns of ones, then
+// zeros.  W3 is padded to 16 output rows (N = 16 is the smallest MMA width
+// at M = 128).  b3 stays FP32.
 constexpr int kLearnOutPad = 16;
+constexpr int kLearnHidPad = 80;  // the second layer's K: hidden units, b2's columns
 constexpr int kBiasColHi = kLearnIn, kBiasColLo = kLearnIn + 1;
+constexpr int kBias2ColHi = kLearnHidden, kBias2ColLo = kLearnHidden + 1;
 struct MlpDevice {
     uint16_t w1[kLearnHidden * kLearnInPad];    // 2 KB
-    uint16_t w2[kLearnHidden * kLearnHidden];   // 8 KB
+    uint16_t w2[kLearnHidden * kLearnHidPad];   // 10 KB
     uint16_t w3[kLearnOutPad * kLearnHidden];   // 2 KB
-    float b2[kLearnHidden];
     float b3[kLearnOut];
     float pad[2];
 };
@@ -70,6 +73,7 @@ struct LearnBuffers {
     float4 *ggeo;         // 2 per group: {cx, cy, trace, lanes}, {re, im, 0, 0}
     float2 *rep;          // per sorted body: the walk's repulsion (k_r m_i applied)
     float2 *corr;         // per group: sum of its pairs' corrections (per unit k_r m_i)
+    float2 *a2;           // per node: a cell's second moment as its children give it
     const MlpDevice *mlp;
 };
 
@@ -80,6 +84,9 @@ constexpr int kErrMlpWait = 64;
 
 // ------------------------------------------------------------- launchers --
 
+// Every cell's second moment from its children (LearnBuffers::a2), a feature
+// of the pairs; after the emit, before the MLP and the training targets.
+void launch_cell_a2(const Buffers &b, const LearnBuffers &lb, int nsm, cudaStream_t s);
 // The MLP over every pair the walk collected: corrections summed per group.
 void launch_learn_mlp(const Buffers &b, const Params &p, const LearnBuffers &lb, int nsm,
                       cudaStream_t s);
