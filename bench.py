@@ -229,24 +229,47 @@ def train_learned(eng_device, combos=LEARNED):
                  "nodes": g.num_nodes(), "edges": g.num_edges()}
 
 
-def timed_from(eng, P, k):
-    """k timed steps from positions P, the timed graph captured beforehand
-    (one untimed step, then the positions again)."""
+def snapshot(eng):
+    """The layout state a step starts from: positions, global speed, speed
+    efficiency and the previous forces."""
+    return eng.get_positions(), eng.speed_state()
+
+
+def restore(eng, S):
+    """Back to a snapshot.  Positions alone are not enough: a step repeated
+    from the same positions sees no swing, so the speed rule raises the
+    global speed as far as it may, and the layout that follows is shaken
+    for tens of iterations (its walk up to 40 % slower)."""
+    P, (gs, se, fp) = S
     eng.set_positions(P)
+    eng.set_speed_state(gs, se, fp)
+
+
+def timed_from(eng, S, k):
+    """k steps from snapshot S, timed twice: the step time without per-kernel
+    events, then the kernels' times with them.  Both iteration graphs are
+    captured beforehand (one untimed step each, then the snapshot again)."""
+    restore(eng, S)
+    eng.step(1)
+    restore(eng, S)
     eng.step_timed(1)
-    eng.set_positions(P)
-    return eng.step_timed(k)
+    restore(eng, S)
+    ms, _ = eng.step_timed(k, kernels=False)
+    restore(eng, S)
+    _, kms = eng.step_timed(k)
+    return ms, kms
 
 
 def correction_report(eng, n, steps, device=0):
     """Far-field accuracy against cost at the current layout: the reference's
     monopole walk at theta 1 beside the quadrupole walk at larger theta.  Each
-    configuration computes one step's repulsion from the same positions P; the
-    error is the relative RMSE against the exact FP64 all-pairs sum over
-    CORRECTION_SAMPLES sampled nodes, and the cost is the mean step and walk
-    (traverse + quadrupole sums) time over a few steps from P.  Outside the
+    configuration computes one step's repulsion from the same state S
+    (positions and speed state); the error is the relative RMSE against the
+    exact FP64 all-pairs sum over CORRECTION_SAMPLES sampled nodes, and the
+    cost is the mean step and walk (traverse + quadrupole sums) time over a
+    few steps from S.  Outside the
     timed region; the engine is left at theta 1, multipole 1."""
-    P = eng.get_positions()
+    S = snapshot(eng)
     rng = np.random.default_rng(3)
     samples = np.sort(rng.choice(n, min(CORRECTION_SAMPLES, n), replace=False)).astype(np.uint32)
     exact = eng.exact_repulsion(samples)
@@ -254,13 +277,13 @@ def correction_report(eng, n, steps, device=0):
     rows = []
     for theta, mp in [(1.0, 1)] + [(t, 2) for t in CORRECTION_THETAS]:
         eng.set_approximation(theta, mp)
-        eng.set_positions(P)
+        restore(eng, S)
         eng.step(1)
         tot, ga = eng.forces()
         rep = (tot - ga)[samples].astype(np.float64)
         err = float(np.sqrt(((rep - exact) ** 2).sum() / (exact ** 2).sum()))
         visits = eng.stats()["visits"]
-        ms, kms = timed_from(eng, P, k)
+        ms, kms = timed_from(eng, S, k)
         rows.append({"theta": theta, "multipole": mp, "rel_rmse": err, "visits": visits,
                      "ms_per_step": ms / k,
                      "walk_ms": kms.get("traverse", 0.0) + kms.get("quadrupole", 0.0),
@@ -276,19 +299,19 @@ def correction_report(eng, n, steps, device=0):
         eng.set_approximation(theta, mp)
         eng.set_learned_correction(mlp)
         try:
-            eng.set_positions(P)
+            restore(eng, S)
             eng.step(1)
             tot, ga = eng.forces()
             rep = (tot - ga)[samples].astype(np.float64)
             err = float(np.sqrt(((rep - exact) ** 2).sum() / (exact ** 2).sum()))
             st1 = eng.stats()
             visits, pairs = st1["visits"], st1["learned_pairs"]
-            ms, kms = timed_from(eng, P, k)
+            ms, kms = timed_from(eng, S, k)
         except Fa2Error as ex:  # recorded, not fatal: the next configuration starts afresh
             learned.append({"theta": theta, "multipole": mp, "error": str(ex),
                             "device_error": eng.stats()["device_error"]})
             eng.set_learned_correction(None)
-            eng.set_positions(P)
+            restore(eng, S)
             continue
         learned.append({"theta": theta, "multipole": mp, "rel_rmse": err, "visits": visits,
                         "pairs": pairs,
@@ -307,11 +330,11 @@ def correction_report(eng, n, steps, device=0):
     learned_guarded = None
     if best_l is not None:
         steps_g = 4 * GUARD_EVERY
-        ms_plain, _ = timed_from(eng, P, steps_g)
+        ms_plain, _ = timed_from(eng, S, steps_g)
         eng.set_approximation(best_l["theta"], best_l["multipole"])
         eng.set_learned_correction(models[(best_l["theta"], best_l["multipole"])][0])
         eng.set_accuracy_guard(GUARD_EVERY, GUARD_SAMPLES)
-        ms, _ = timed_from(eng, P, steps_g)
+        ms, _ = timed_from(eng, S, steps_g)
         gd = eng.accuracy_guard()
         eng.set_accuracy_guard(0, 0)
         eng.set_learned_correction(None)
@@ -347,10 +370,10 @@ def correction_report(eng, n, steps, device=0):
         # checking it against the FP64 sum every GUARD_EVERY steps
         steps_g = 4 * GUARD_EVERY
         eng.set_approximation(1.0, 1)
-        ms_plain, _ = timed_from(eng, P, steps_g)
+        ms_plain, _ = timed_from(eng, S, steps_g)
         eng.set_approximation(best["theta"], 2)
         eng.set_accuracy_guard(GUARD_EVERY, GUARD_SAMPLES)
-        ms, _ = timed_from(eng, P, steps_g)
+        ms, _ = timed_from(eng, S, steps_g)
         gd = eng.accuracy_guard()
         eng.set_accuracy_guard(0, 0)
         # the same steps from the same positions with the plain walk
@@ -359,7 +382,7 @@ def correction_report(eng, n, steps, device=0):
                    "plain_ms_per_step": ms_plain / steps_g,
                    "speedup_vs_plain": ms_plain / ms, **gd}
     eng.set_approximation(1.0, 1)
-    eng.set_positions(P)
+    restore(eng, S)
     return {
         "samples": len(samples), "exact": "fp64 all-pairs on the GPU",
         "configs": rows,
@@ -426,15 +449,19 @@ def run_ours(args, world, rank, local, fp64_n=FP64_CHECKS, correction=True):
     time.sleep(0.3)
     barrier(world)
     torch.cuda.synchronize()
-    ms, kms = eng.step_timed(args.steps)
+    ms, _ = eng.step_timed(args.steps, kernels=False)
     torch.cuda.synchronize()
     barrier(world)
     if sampler:
         sampler.terminate()
         sampler.wait()
-    st = eng.stats()
     ms_max = barrier_max(world, ms)
     value = world * args.steps / (ms_max / 1000.0)
+    # per-kernel times inside the iteration graph, from a copy of it with an
+    # event around every kernel (those events cost time of their own, so the
+    # timed steps above run without them)
+    _, kms = eng.step_timed(min(args.steps, 20))
+    st = eng.stats()
 
     # per-kernel times with every kernel running alone (the attraction is
     # otherwise spread over the tree build's gaps): the roofline denominators
@@ -709,7 +736,7 @@ def config1_record(local, no_cpu_baseline):
     eng.step_timed(5)  # from the same state
     eng.set_positions(xy0)
     eng.set_speed_state(1.0, 1.0)
-    ms, _ = eng.step_timed(CONFIG1_ITERS)
+    ms, _ = eng.step_timed(CONFIG1_ITERS, kernels=False)
     ours_xy = eng.get_positions()
     eng.set_speed_state(1.0, 1.0)
     t0 = time.perf_counter()

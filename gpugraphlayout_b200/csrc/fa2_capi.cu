@@ -935,8 +935,10 @@ int fa2_step_timed(fa2_ctx *c, int32_t n_iters, float *ms_total, float *kernel_m
     CK(cudaEventCreate(&t1));
     std::vector<double> sum(kNumSlots, 0.0);
     std::vector<int> cnt(kNumSlots, 0);
+    const bool per_kernel = kernel_ms && n_kernels > 0;
     cudaEventRecord(t0, c->sA);
-    int s = run_steps(c, n_iters, true, &sum, &cnt);
+    int s = per_kernel ? run_steps(c, n_iters, true, &sum, &cnt)
+                       : run_steps(c, n_iters, false, nullptr, nullptr);
     cudaEventRecord(t1, c->sA);
     cudaEventSynchronize(t1);
     float ms = 0.0f;
@@ -944,7 +946,7 @@ int fa2_step_timed(fa2_ctx *c, int32_t n_iters, float *ms_total, float *kernel_m
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     *ms_total = ms;
-    if (kernel_ms)
+    if (per_kernel)
         for (int q = 0; q < n_kernels && q < kNumSlots; ++q)
             kernel_ms[q] = cnt[q] ? (float)(sum[q] / cnt[q]) : 0.0f;
     return s;

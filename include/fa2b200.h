@@ -114,10 +114,13 @@ int fa2_get_positions(fa2_ctx *ctx, float *xy);
 int fa2_step(fa2_ctx *ctx, int32_t n_iters);
 
 /* fa2_step with device timing: *ms_total receives the CUDA-event time of
- * the whole call on the engine's stream; kernel_ms (may be NULL) receives,
- * for each kernel listed by fa2_kernel_name, its mean duration per launch in
- * ms over the call.  n_kernels is the size of kernel_ms.  No reference
- * counterpart: it serves measurement. */
+ * the whole call on the engine's stream.  With kernel_ms (n_kernels > 0) the
+ * iterations run a copy of the iteration graph with an event before and
+ * after each kernel, and kernel_ms receives, for each kernel listed by
+ * fa2_kernel_name, its mean duration per launch in ms over the call; those
+ * events cost time of their own, most on small graphs.  With kernel_ms NULL
+ * (or n_kernels 0) the iterations run fa2_step's graph, with events only
+ * around the call.  No reference counterpart: it serves measurement. */
 int fa2_step_timed(fa2_ctx *ctx, int32_t n_iters, float *ms_total, float *kernel_ms,
                    int32_t n_kernels);
 

@@ -127,6 +127,23 @@ def test_set_force_params_and_speed_state(ba3k):
     assert np.array_equal(e.get_positions(), after)
 
 
+def test_timed_steps_take_the_same_steps(ba3k):
+    """fa2_step_timed, with per-kernel events or without, runs the iterations
+    fa2_step runs: the same positions bit for bit, and a positive time."""
+    from oracle import oracle as O
+    xy = O.random_positions(ba3k.n, 2000, 2000, 8)
+    ref = _engine(ba3k, xy, k_r=10.0)
+    ref.step(6)
+    for kernels in (False, True):
+        e = _engine(ba3k, xy, k_r=10.0)
+        ms, kms = e.step_timed(6, kernels=kernels)
+        assert ms > 0.0
+        assert bool(kms) == kernels
+        if kernels:
+            assert kms["traverse"] > 0.0 and kms["attract"] > 0.0
+        assert np.array_equal(e.get_positions(), ref.get_positions())
+
+
 def test_deterministic_repeat(ba3k):
     from oracle import oracle as O
     xy = O.random_positions(ba3k.n, 2000, 2000, 5)
