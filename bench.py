@@ -14,7 +14,8 @@ events on the engine's stream around K iterations, max over ranks, summed
 over ranks: with N > 1 every rank lays out its own replica of the graph, the
 single-graph path does not shard).  `e2e` is the same metric through the
 public C ABI with host buffers: per step, the positions are copied in from
-pinned host memory, one iteration runs and the positions are copied back.
+pinned host memory, one iteration runs and the positions are copied back
+(fa2_step_host: the three in one call, one host synchronisation).
 `--impl reference` times the reference's own CPU ForceAtlas2
 (CPUForceAtlas2::doStep, built from its sources into oracle/_ref) on the same
 graph and positions, one iteration per step.
@@ -480,9 +481,8 @@ def run_ours(args, world, rank, local, fp64_n=FP64_CHECKS, correction=True):
     barrier(world)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        eng.set_positions_ptr(ptr)
-        eng.step(1)
-        eng.get_positions_ptr(ptr)
+        # positions in from pinned memory, one iteration, positions out
+        eng.step_host(ptr, 1, ptr)
     e2e_s = barrier_max(world, time.perf_counter() - t0)
     e2e = world * args.steps / e2e_s
 
@@ -542,11 +542,11 @@ def run_ours(args, world, rank, local, fp64_n=FP64_CHECKS, correction=True):
         "config": workload_config(n, m, args.theta if learned is None else learned,
                                   args.multipole, args.workload, learned is not None),
         "clocks": clocks_summary(clk_path),
-        # + moment scan and per-cell a2 (quadrupole walk or learned
-        # correction), + MLP and tail (learned correction)
+        # + moment scan and per-cell a2 (quadrupole walk), + the cells'
+        # children moments, MLP and tail (learned correction)
         "gpu_launches": (KERNELS_PER_ITER + st["sort_passes"] + (st["sort_passes"] < 8)
-                         + (2 if args.multipole == 2 or learned is not None else 0)
-                         + (2 if learned is not None else 0)) * args.steps,
+                         + (2 if args.multipole == 2 else 0)
+                         + (3 if learned is not None else 0)) * args.steps,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * n,
                 "d2h_bytes_per_step": 8 * n},
         "roofline": roofline,

@@ -117,6 +117,21 @@ class Engine:
     def step(self, iters: int = 1) -> None:
         check(lib().fa2_step(self._ctx, iters), "fa2_step")
 
+    def step_host(self, xy_in, iters: int, xy_out) -> None:
+        """Positions in, iters steps, positions out, with one synchronisation
+        (fa2_step_host).  xy_in and xy_out are float32 (n, 2) arrays (or None),
+        or raw host pointers as ints (e.g. pinned memory)."""
+        def arg(a, writable):
+            if a is None or isinstance(a, int):
+                return None if a is None else C.c_void_p(a)
+            if not (isinstance(a, np.ndarray) and a.dtype == np.float32 and
+                    a.flags["C_CONTIGUOUS"] and a.size == 2 * self.n and
+                    (a.flags["WRITEABLE"] or not writable)):
+                raise ValueError("positions: a C-contiguous float32 array of n x 2")
+            return C.c_void_p(a.ctypes.data)
+        check(lib().fa2_step_host(self._ctx, arg(xy_in, False), int(iters), arg(xy_out, True)),
+              "fa2_step_host")
+
     def step_timed(self, iters: int, kernels: bool = True):
         """Runs iters steps; returns (device ms of the call, {kernel: mean ms per
         launch}).  kernels=False runs the steps without the per-kernel events

@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(HERE, "libfa2b200.so")
 # Exported names declared in include/fa2b200.h.
 EXPORTS = (
     "fa2_default_params", "fa2_create", "fa2_destroy", "fa2_set_positions",
-    "fa2_get_positions", "fa2_step", "fa2_step_timed", "fa2_kernel_name",
+    "fa2_get_positions", "fa2_step", "fa2_step_host", "fa2_step_timed", "fa2_kernel_name",
     "fa2_get_stats", "fa2_get_forces", "fa2_get_sort_order", "fa2_set_speed_state",
     "fa2_get_speed_state", "fa2_set_force_params", "fa2_set_linlog", "fa2_set_overlap",
     "fa2_set_approximation", "fa2_exact_repulsion", "fa2_last_cuda_error",
@@ -112,6 +112,7 @@ def lib():
     L.fa2_get_positions.argtypes = [vp, vp]
     L.fa2_step.argtypes = [vp, C.c_int32]
     L.fa2_step_timed.argtypes = [vp, C.c_int32, f32p, f32p, C.c_int32]
+    L.fa2_step_host.argtypes = [vp, vp, C.c_int32, vp]
     L.fa2_kernel_name.restype = C.c_char_p
     L.fa2_kernel_name.argtypes = [C.c_int32]
     L.fa2_get_stats.argtypes = [vp, C.POINTER(Stats)]

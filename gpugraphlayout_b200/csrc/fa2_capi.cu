@@ -57,6 +57,8 @@ struct fa2_ctx {
     void *scratch = nullptr;
     size_t scratch_bytes = 0;
     float2 *stage_xy = nullptr;    // n, reference order
+    DevState *h_state = nullptr;   // pinned: the state after fa2_step_host's iterations
+    int *h_iters = nullptr;        // pinned: iterations done before them
     uint32_t *stage_ids = nullptr; // n
     int bbox_blocks = 0, trav_blocks = 0;
     cudaStream_t sA = nullptr, sB = nullptr;
@@ -171,6 +173,8 @@ void free_all(fa2_ctx *c) {
     if (c->evA2) cudaEventDestroy(c->evA2);
     if (c->sA) cudaStreamDestroy(c->sA);
     if (c->sB) cudaStreamDestroy(c->sB);
+    if (c->h_state) cudaFreeHost(c->h_state);
+    if (c->h_iters) cudaFreeHost(c->h_iters);
 }
 
 // Nodes in degree-descending order (ties by reference id), a symmetric CSR
@@ -853,7 +857,9 @@ fa2_ctx *fa2_create(const fa2_graph_desc *g, const fa2_params *prm, int *status)
         cudaEventCreateWithFlags(&c->evJoin, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->evCounted, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->evEmitted, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->evA2, cudaEventDisableTiming) != cudaSuccess)
+        cudaEventCreateWithFlags(&c->evA2, cudaEventDisableTiming) != cudaSuccess ||
+        cudaMallocHost(&c->h_state, sizeof(DevState)) != cudaSuccess ||
+        cudaMallocHost(&c->h_iters, sizeof(int)) != cudaSuccess)
         return fail(FA2_ERR_CUDA);
     c->slot_events.resize(kNumSlots * 2);
     for (auto &e : c->slot_events)
@@ -924,6 +930,57 @@ int fa2_step(fa2_ctx *c, int32_t n_iters) {
     if (!c || n_iters < 0) return FA2_ERR_INVALID_ARGUMENT;
     CK(cudaSetDevice(c->device));
     return run_steps(c, n_iters, false, nullptr, nullptr);
+}
+
+int fa2_step_host(fa2_ctx *c, const float *xy_in, int32_t n_iters, float *xy_out) {
+    if (!c || n_iters < 0) return FA2_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(c->device));
+    if (c->n == 0) return FA2_OK;
+    int s = FA2_OK;
+    if (guard_active(c)) {
+        // the guard's checks sit between iterations: the separate calls
+        if (xy_in && (s = fa2_set_positions(c, xy_in))) return s;
+        if ((s = run_steps(c, n_iters, false, nullptr, nullptr))) return s;
+        return xy_out ? fa2_get_positions(c, xy_out) : FA2_OK;
+    }
+    if (n_iters > 0 && !c->exec && (s = capture(c, false, &c->exec))) return s;
+    cudaStream_t A = c->sA;
+    const size_t bytes = (size_t)c->n * 8;
+    if (xy_in) {
+        // fa2_set_positions without its synchronisation
+        CK(cudaMemcpyAsync(c->stage_xy, xy_in, bytes, cudaMemcpyHostToDevice, A));
+        launch_scatter_xy((int)c->n, c->b.ref_of, c->stage_xy, c->b.pos, A);
+        CK(cudaMemsetAsync(c->scratch, 0, c->scratch_bytes, A));
+        CK(cudaMemsetAsync(&c->b.st->err, 0, sizeof(int), A));
+        launch_bbox(c->b, c->bbox_blocks, A);
+    }
+    CK(cudaMemcpyAsync(c->h_iters, &c->b.st->iters_done, sizeof(int), cudaMemcpyDeviceToHost, A));
+    c->last_perturb_rounds = 0;
+    for (int it = 0; it < n_iters; ++it) CK(cudaGraphLaunch(c->exec, A));
+    CK(cudaMemcpyAsync(c->h_state, c->b.st, sizeof(DevState), cudaMemcpyDeviceToHost, A));
+    if (xy_out) {
+        launch_gather_xy((int)c->n, c->b.ref_of, c->b.pos, c->stage_xy, A);
+        CK(cudaMemcpyAsync(xy_out, c->stage_xy, bytes, cudaMemcpyDeviceToHost, A));
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(A));
+    DevState st = *c->h_state;
+    if (st.err) return FA2_ERR_DEVICE_LIMIT;
+    int completed = st.iters_done - *c->h_iters;
+    if (completed == n_iters && !st.poison) {
+        choose_sort_passes(c, st);
+        return FA2_OK;
+    }
+    // An iteration was replayed (coincident bodies, or a sort that needs all
+    // its digits): the iterations after it did nothing.  The rest as
+    // fa2_step does it, then the positions again.
+    if (st.poison) {
+        if ((s = resolve_poison(c, &st))) return s;
+        completed += 1;
+    }
+    if (completed < n_iters && (s = run_steps(c, n_iters - completed, false, nullptr, nullptr)))
+        return s;
+    return xy_out ? fa2_get_positions(c, xy_out) : FA2_OK;
 }
 
 int fa2_step_timed(fa2_ctx *c, int32_t n_iters, float *ms_total, float *kernel_ms,

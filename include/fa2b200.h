@@ -113,6 +113,18 @@ int fa2_get_positions(fa2_ctx *ctx, float *xy);
  * cudaDeviceSynchronize (:246). */
 int fa2_step(fa2_ctx *ctx, int32_t n_iters);
 
+/* fa2_set_positions(xy_in), fa2_step(n_iters) and fa2_get_positions(xy_out)
+ * in one call, with one synchronisation of the host instead of three: the
+ * copies, the iterations and the state read that follows them are queued
+ * together.  xy_in and xy_out (2 floats per node, reference order) may each
+ * be NULL, and may be the same buffer; from pinned memory the copies run at
+ * the link's rate.  The positions and forces are those of the three calls,
+ * bit for bit.  An iteration that must be replayed (coincident bodies) and
+ * an active accuracy guard take the path of the three calls.  No reference
+ * counterpart: a host loop that owns the positions (graph_viewer writes
+ * them out between runs of iterations) calls this once per round trip. */
+int fa2_step_host(fa2_ctx *ctx, const float *xy_in, int32_t n_iters, float *xy_out);
+
 /* fa2_step with device timing: *ms_total receives the CUDA-event time of
  * the whole call on the engine's stream.  With kernel_ms (n_kernels > 0) the
  * iterations run a copy of the iteration graph with an event before and

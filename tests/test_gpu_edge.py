@@ -144,6 +144,58 @@ def test_timed_steps_take_the_same_steps(ba3k):
         assert np.array_equal(e.get_positions(), ref.get_positions())
 
 
+@pytest.mark.parametrize("iters", [1, 5])
+def test_step_host_equals_the_three_calls(ba3k, iters):
+    """fa2_step_host (positions in, iterations, positions out, one host
+    synchronisation) against fa2_set_positions + fa2_step + fa2_get_positions:
+    the same positions and forces bit for bit, for several round trips in a
+    row, with the input and output in one buffer, and with either side left
+    out."""
+    from oracle import oracle as O
+    xy = O.random_positions(ba3k.n, 2000, 2000, 21)
+    a = _engine(ba3k, xy, k_r=10.0)
+    b = _engine(ba3k, xy, k_r=10.0)
+    host = xy.copy()
+    for _ in range(3):
+        a.set_positions(host)
+        a.step(iters)
+        want = a.get_positions()
+        b.step_host(host, iters, host)  # in and out in the same buffer
+        assert np.array_equal(host, want)
+        assert np.array_equal(b.forces()[0], a.forces()[0])
+    # no input: from the device's positions; no output: positions stay there
+    a.step(iters)
+    b.step_host(None, iters, None)
+    assert np.array_equal(b.get_positions(), a.get_positions())
+    out = np.zeros_like(host)
+    b.step_host(None, 0, out)
+    assert np.array_equal(out, a.get_positions())
+    with pytest.raises(ValueError):
+        b.step_host(np.zeros((3, 2), np.float32), 1, None)
+
+
+def test_step_host_replays_coincident_bodies():
+    """A round trip whose first iteration must be replayed (coincident
+    bodies) gives what the three calls give."""
+    from gpugraphlayout_b200 import synth
+    from oracle import oracle as O
+    s, t = synth.ba_edges(400, 2, seed=2)
+    g = O.Graph(s, t)
+    xy = O.random_positions(g.n, 500, 500, 4)
+    xy[7] = xy[3]
+    xy[11] = xy[3]
+    xy[20] = xy[19]
+    a = _engine(g, xy)
+    a.step(3)
+    assert a.stats()["perturb_rounds"] >= 1  # the first of the 3 was replayed
+    want = a.get_positions()
+    b = _engine(g, xy)
+    out = np.zeros_like(xy)
+    b.step_host(xy, 3, out)
+    assert np.array_equal(out, want)
+    assert np.array_equal(b.sort_order(), a.sort_order())
+
+
 def test_deterministic_repeat(ba3k):
     from oracle import oracle as O
     xy = O.random_positions(ba3k.n, 2000, 2000, 5)
