@@ -98,6 +98,14 @@ __global__ void __launch_bounds__(kBBoxThreads) k_bbox(int n, const float2 *__re
     bbox_finish<kBBoxThreads>(a, bad, partial, &ctr->bbox_done, st);
 }
 
+// Whether a learned walk keeps an accepted cell as a pair: its size h is at
+// least kLearnMinRatio theta of its distance (wx, wy) from the group's
+// centroid.  With the cell's threshold dq = (2h)^2 / theta^2 + eps,
+// h / d >= c theta  <=>  dq - eps >= 4 c^2 d^2: no theta needed.
+__device__ __forceinline__ bool learn_keep(float dq, float wx, float wy, float eps) {
+    return dq - eps >= 4.0f * kLearnMinRatio * kLearnMinRatio * (wx * wx + wy * wy);
+}
+
 // ------------------------------------------------------------------- keys --
 
 // One block per sort tile: the tile's keys, the tile's counts of the digit
@@ -151,10 +159,12 @@ __global__ void __launch_bounds__(1024) k_keys(int n, int tile, int first,
 // reference counterpart: it is the option fa2_set_approximation selects.
 //
 // LEARN (the learned correction, fa2_learn.cuh) also records, per group, the
-// centroid and second moments of its bodies and every cell the whole group
-// accepted (a (group, node) pair, gathered 32 at a time in shared memory),
-// and writes each body's repulsion in sorted order instead of the tail: the
-// MLP and k_learn_tail finish the iteration.  The sums are the same.
+// centroid and second moments of its bodies and the cells the whole group
+// accepted that are not small for their distance (a (group, node) pair,
+// gathered 32 at a time in registers, one per lane, and tested with
+// learn_keep when the 32 are written out), and
+// writes each body's repulsion in sorted order instead of the tail: the MLP
+// and k_learn_tail finish the iteration.  The sums are the same.
 //
 // OVERLAP (prevent_overlap, with the monopole walk) repels accepted bodies by
 // the paper's anti-collision rule (overlap_factor) with the sizes of the
@@ -235,18 +245,29 @@ __global__ void __launch_bounds__(kTravThreads, 2048 / kTravThreads) k_traverse(
                 lb.ggeo[2 * w + 1] = make_float4(t1 / cnt, t2 / cnt, 0.0f, 0.0f);
             }
         }
-        // LEARN: the pending cells to this warp's segment of the pair list,
-        // one atomic per flush
+        // LEARN: the pending cells the group sees at a size ratio h / d of at
+        // least kLearnMinRatio theta (d from the group's centroid) to this
+        // warp's segment of the pair list, one atomic per flush
         auto flush = [&]() {
+            __syncwarp();  // lane 0's store of the centroid is seen by all lanes
+            bool keep = false;
+            if (lane < npend) {
+                const float4 cell = __ldg(&nodes[my_cell]);
+                const float4 g0 = lb.ggeo[2 * w];
+                keep = learn_keep(s_dq[meta_level(__float_as_int(cell.w))], g0.x - cell.x,
+                                  g0.y - cell.y, prm.epssq);
+            }
+            const unsigned km = __ballot_sync(kFull, keep);
+            const unsigned nk = (unsigned)__popc(km);
             const uint32_t seg = (blockIdx.x * (kTravThreads / kWarp) + (threadIdx.x >> 5)) %
                                  (uint32_t)kPairSegments;
             uint32_t base = 0;
-            if (lane == 0) base = atomicAdd(&ctr->pair_count[seg], (unsigned)npend);
+            if (lane == 0 && nk) base = atomicAdd(&ctr->pair_count[seg], nk);
             base = __shfl_sync(kFull, base, 0);
-            if (lane < npend && base + lane < lb.seg_cap)
-                lb.pairs[(size_t)seg * lb.seg_cap + base + lane] =
-                    make_uint2((uint32_t)w, my_cell);
-            if (lane == 0 && base + (uint32_t)npend > lb.seg_cap) atomicOr(&st->err, kErrPairs);
+            const uint32_t idx = base + (uint32_t)__popc(km & ((1u << lane) - 1u));
+            if (keep && idx < lb.seg_cap)
+                lb.pairs[(size_t)seg * lb.seg_cap + idx] = make_uint2((uint32_t)w, my_cell);
+            if (lane == 0 && base + nk > lb.seg_cap) atomicOr(&st->err, kErrPairs);
             npend = 0;
         };
         // An opened cell's first child is node + 1 and always exists, so only

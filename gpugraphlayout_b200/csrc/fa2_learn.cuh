@@ -29,6 +29,14 @@ constexpr int kLearnOut = 2;
 // distance to the cell: a group straddling a cell boundary sees a field that
 // varies across it, which one correction per group cannot follow.
 constexpr float kLearnMaxSpread = 0.5f;
+// A pair is collected only when the cell's size h is at least
+// kLearnMinRatio theta of its distance d from the group's centroid (feature
+// 0; the walk tests the cells it accepted 32 at a time, when it writes them
+// out).  The smaller cells left out carry little of the correctable error: on
+// R-MAT scale 20 at theta 1.5 the pairs with h / d > 0.4 are 45 % of all and
+// carry 98.6 % of the squared group-mean error, weighted as in training (0.5
+// and 41 % / 98.6 % at theta 2, 0.3 and 54 % / 99.3 % at theta 1.2).
+constexpr float kLearnMinRatio = 0.25f;
 // Largest correction of one pair, in units of the cell's point-mass term
 // M / d: the MLP's outputs (and the training targets) are clamped to it.
 constexpr float kLearnMaxOut = 1.0f;
