@@ -209,7 +209,7 @@ CORRECTION_THETAS = (1.2, 1.4, 1.5, 1.6, 1.7, 1.8, 2.0)
 # 200 layout snapshots of a plain run, evaluated on the workload at these
 # (theta, multipole) walks against the plain walk at theta 1.
 TRAIN_SCALE, TRAIN_DRAWS = 16, 1 << 20
-LEARNED = ((1.2, 1), (1.5, 1), (1.7, 1), (2.0, 1), (2.0, 2))
+LEARNED = ((1.2, 1), (1.5, 1), (1.6, 1), (1.7, 1), (2.0, 1), (2.0, 2))
 EQUAL_RMSE_TARGET = 1.5  # the speed-up at equal or lower error the design aims at
 
 
