@@ -490,9 +490,11 @@ def run_ours(args, world, rank, local, fp64_n=FP64_CHECKS, correction=True):
         eng.close()
         return None
     # the correction report compares against the plain walk, so it runs only
-    # when the plain walk is the workload
+    # when the plain walk is the workload, and only at N = 1 (with N > 1 the
+    # other ranks have left; their GPUs are not held for it)
     correction = (correction_report(eng, n, args.steps, local)
-                  if correction and plain and not large and not args.no_correction else None)
+                  if (correction and plain and not large and not args.no_correction
+                      and world == 1) else None)
     fp64 = fp64_checks(eng, n, fp64_n) if large else None
     names = kernel_names()
     pk, pk_kind = peaks()
