@@ -33,6 +33,9 @@ namespace {
 // result is the same for each (stable sort, exact integer sums, per-warp
 // walks, fixed-order speed sums); only the speed differs.
 constexpr int kBRounds = 4;                       // keys per thread in a sort chunk
+// A sort that skips low digits leaves runs of keys equal in the digits it
+// sorted; a run longer than this sends the graph back to a sort on every digit.
+constexpr int kBMaxRun = 128;
 constexpr uint32_t kBatchMaxNodes = FA2_BATCH_MAX_NODES;  // nodes per graph
 constexpr int kErrPoisonRounds = 1 << 9;          // coincident bodies kept reappearing
 
@@ -111,6 +114,8 @@ struct BatchSmem {
     int ticket;
     int graph;
     int err, poison;
+    int maxlev;   // deepest cell level of the last tree (phase_count)
+    int resort;   // a run of the partial sort was too long: sort on every digit
     float gs, se;
 };
 
@@ -337,12 +342,18 @@ __device__ void sort_pass(int pass, uint32_t n, const uint64_t *kin, const uint3
     }
 }
 
-// Keys from the positions, the 8 sort passes (ending in keys0/vals0) and the
+// Keys from the positions, the sort passes (ending in keys0/vals0) and the
 // ordering of equal-key runs; returns with S.poison set if exactly
 // coincident bodies were found (perturb = 0) or after scaling them (1).
+// With first = 2 or 4 the sort skips its lowest 2 or 4 digits (after a tree
+// no deeper than level 22 or 14, so the digits it sorts reach two levels
+// deeper), and each run of keys equal in the digits it sorted is then
+// ordered by the full key, stably: exactly the order of the full sort (the
+// rule of the single-graph engine's k_fix_low).  A run longer than kBMaxRun
+// sorts the graph again on every digit.
 template <int T>
 __device__ void phase_keys_sort(const BatchArgs &A, uint32_t base, uint32_t n, char *slot,
-                                BatchSmem<T> &S, int perturb) {
+                                BatchSmem<T> &S, int perturb, int first = 0) {
     uint64_t *k0 = slot_ptr<uint64_t>(slot, A.L.keys0), *k1 = slot_ptr<uint64_t>(slot, A.L.keys1);
     uint32_t *v0 = slot_ptr<uint32_t>(slot, A.L.vals0), *v1 = slot_ptr<uint32_t>(slot, A.L.vals1);
     const float rx = S.rx, ry = S.ry, rr = S.radius;
@@ -351,10 +362,46 @@ __device__ void phase_keys_sort(const BatchArgs &A, uint32_t base, uint32_t n, c
         k0[i] = morton_key(p.x, p.y, rx, ry, rr);
         v0[i] = i;
     }
+    if (threadIdx.x == 0) S.resort = 0;
     __syncthreads();
-    for (int pass = 0; pass < 8; pass += 2) {
+    for (int pass = first; pass < 8; pass += 2) {
         sort_pass(pass, n, k0, v0, k1, v1, S);
         sort_pass(pass + 1, n, k1, v1, k0, v0, S);
+    }
+    if (first > 0) {
+        const int low = 8 * first;
+        for (uint32_t k = threadIdx.x; k + 1 < n; k += T) {
+            const uint64_t hk = k0[k] >> low;
+            if ((k0[k + 1] >> low) != hk || (k > 0 && (k0[k - 1] >> low) == hk)) continue;
+            uint32_t len = 2;
+            while (k + len < n && (k0[k + len] >> low) == hk && len <= (uint32_t)kBMaxRun) ++len;
+            if (len > (uint32_t)kBMaxRun) {
+                S.resort = 1;
+                continue;
+            }
+            uint64_t *kr = k0 + k;
+            uint32_t *vr = v0 + k;
+            for (uint32_t a = 1; a < len; ++a) {  // insertion sort, stable
+                const uint64_t ka = kr[a];
+                const uint32_t va = vr[a];
+                int j = (int)a - 1;
+                while (j >= 0 && kr[j] > ka) {
+                    kr[j + 1] = kr[j];
+                    vr[j + 1] = vr[j];
+                    --j;
+                }
+                kr[j + 1] = ka;
+                vr[j + 1] = va;
+            }
+        }
+        __syncthreads();
+        // every digit, from the order the partial sort left: equal keys keep
+        // their input order through both, so this is the full sort's order
+        if (S.resort)
+            for (int pass = 0; pass < 8; pass += 2) {
+                sort_pass(pass, n, k0, v0, k1, v1, S);
+                sort_pass(pass + 1, n, k1, v1, k0, v0, S);
+            }
     }
     for (uint32_t k = threadIdx.x; k + 1 < n; k += T) {
         if (k0[k + 1] != k0[k] || (k > 0 && k0[k - 1] == k0[k])) continue;
@@ -379,6 +426,8 @@ __device__ void phase_count(const BatchArgs &A, uint32_t base, uint32_t n, char 
     const float rx = S.rx, ry = S.ry;
     const uint32_t cap = A.L.cap;
     NodeSums carry{0, 0, 0, 0};
+    int lmax = 0;  // this thread's deepest shared-digit count: the tree's depth
+    if (threadIdx.x == 0) S.maxlev = 0;
     for (uint32_t c0 = 0; c0 < n; c0 += T) {
         const uint32_t k = c0 + threadIdx.x;
         NodeSums v{0, 0, 0, 0};
@@ -386,6 +435,7 @@ __device__ void phase_count(const BatchArgs &A, uint32_t base, uint32_t n, char 
         int c = 0;
         if (k < n) {
             const int Lk = lcp_at(keys, (int)n, (int)k), Lkm1 = lcp_at(keys, (int)n, (int)k - 1);
+            lmax = Lk > lmax ? Lk : lmax;
             lcp[k] = (int8_t)Lk;
             c = cells_at((int)k, Lk, Lkm1);
             const uint32_t i = vals[k];
@@ -413,6 +463,7 @@ __device__ void phase_count(const BatchArgs &A, uint32_t base, uint32_t n, char 
         }
         sums_add(carry, total);
     }
+    atomicMax(&S.maxlev, lmax);
     if (threadIdx.x == 0) {
         pm[n] = carry.m;
         pxy[2 * (size_t)n] = carry.x;
@@ -610,12 +661,13 @@ __global__ void __launch_bounds__(T, 2048 / T) k_batch(BatchArgs A) {
         }
         __syncthreads();
         int rounds = 0;
+        int first = 0;  // low digits the next sort skips, from the last tree's depth
         for (int it = 0; it < A.iters && n > 0; ++it) {
             if (S.err) break;
             phase_attract<T, LINLOG>(A, base, n, fa);
             phase_bbox(A, base, n, S);
             if (S.err) break;
-            phase_keys_sort(A, base, n, slot, S, 0);
+            phase_keys_sort(A, base, n, slot, S, 0, first);
             // Exactly coincident bodies: scale the later ones by .99 (the
             // reference's re-insertion, src/RPBHKernels.cu:271-278) and build
             // again, keeping gravity, attraction and the box of before.
@@ -634,6 +686,7 @@ __global__ void __launch_bounds__(T, 2048 / T) k_batch(BatchArgs A) {
             if (S.err) break;
             phase_count(A, base, n, slot, S);
             if (S.err) break;
+            first = S.maxlev <= kLevels - 18 ? 4 : (S.maxlev <= kLevels - 10 ? 2 : 0);
             phase_emit(A, base, n, slot, S);
             phase_traverse(A, base, n, slot, S);
             phase_displace(A, base, n, slot, S);
