@@ -178,10 +178,19 @@ __device__ void phase_attract(const BatchArgs &A, uint32_t base, uint32_t n, flo
         if (valid) {
             p = A.pos[base + row];
             const uint32_t e1 = A.off[base + row + 1];
-            for (uint32_t e = A.off[base + row] + (uint32_t)l8; e < e1; e += 8) {
-                const float2 q = pull<LINLOG>(A.pos[A.col[e]], p);
-                ax += q.x;
-                ay += q.y;
+            // two of the lane's edges in flight at a time, added in order
+            for (uint32_t e = A.off[base + row] + (uint32_t)l8; e < e1; e += 16) {
+                const bool two = e + 8 < e1;
+                const uint32_t c0 = A.col[e], c1 = two ? A.col[e + 8] : c0;
+                const float2 p0 = A.pos[c0], p1 = A.pos[c1];
+                const float2 q0 = pull<LINLOG>(p0, p);
+                ax += q0.x;
+                ay += q0.y;
+                if (two) {
+                    const float2 q1 = pull<LINLOG>(p1, p);
+                    ax += q1.x;
+                    ay += q1.y;
+                }
             }
         }
 #pragma unroll
