@@ -77,7 +77,7 @@ struct fa2_ctx {
     int guard_every = 0, guard_samples = 0, guard_cap = 0, guard_left = 0;
     int guard_checks = 0, guard_fallbacks = 0;
     double guard_err_cur = 0.0, guard_err_plain = 0.0;
-    double2 *guard_exact = nullptr;
+    double2 *guard_exact = nullptr, *guard_part = nullptr;
     float2 *guard_plain = nullptr, *guard_cur = nullptr;
     // learned correction (fa2_set_learned_correction)
     bool learn_on = false;
@@ -407,7 +407,8 @@ bool guard_active(const fa2_ctx *c) {
 // the sampled bodies; the plain walk takes over when it is the more accurate.
 int guard_check(fa2_ctx *c) {
     const int ns = c->guard_samples;
-    launch_guard(c->b, c->kp, ns, c->guard_exact, c->guard_plain, c->guard_cur, c->sA);
+    launch_guard(c->b, c->kp, ns, c->guard_exact, c->guard_plain, c->guard_cur, c->guard_part,
+                 c->sA);
     CK(cudaGetLastError());
     std::vector<double2> ex((size_t)ns);
     std::vector<float2> pl((size_t)ns), cu((size_t)ns);
@@ -1211,6 +1212,7 @@ int fa2_set_accuracy_guard(fa2_ctx *c, int32_t every, int32_t n_samples) {
     if (ns > c->guard_cap) {
         int s = FA2_OK;
         if ((s = dalloc(c, &c->guard_exact, (size_t)ns)) ||
+            (s = dalloc(c, &c->guard_part, guard_part_count(ns))) ||
             (s = dalloc(c, &c->guard_plain, (size_t)ns)) ||
             (s = dalloc(c, &c->guard_cur, (size_t)ns)))
             return s;

@@ -203,8 +203,12 @@ void launch_displace(const Buffers &b, int nsm, cudaStream_t s);
 void launch_count_interactions(const Buffers &b, const Params &p, int nblocks, cudaStream_t s);
 void launch_exact_f64(const Buffers &b, const Params &p, const uint32_t *ids, int n_ids,
                       double2 *out, cudaStream_t s);
+// The accuracy guard's sums for ns samples: exact (FP64), the reference walk's
+// (plain) and the applied repulsion (cur); part holds guard_part_count(ns)
+// partial sums.
+size_t guard_part_count(int ns);
 void launch_guard(const Buffers &b, const Params &p, int ns, double2 *exact, float2 *plain,
-                  float2 *cur, cudaStream_t s);
+                  float2 *cur, double2 *part, cudaStream_t s);
 void launch_attract(const Buffers &b, const Params &p, const AttractPlan &plan, cudaStream_t s);
 // prevent_overlap: node sizes in sorted order (before the walk)
 void launch_sorted_sizes(const Buffers &b, cudaStream_t s);

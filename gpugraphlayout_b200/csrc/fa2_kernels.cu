@@ -490,16 +490,22 @@ __device__ __forceinline__ int guard_sample(int s, int ns, int n) {
     return (int)(((long long)(2 * s + 1) * n) / (2ll * ns));
 }
 
+// The exact sums are split over kGuardSplit blocks per sample (blockIdx.y
+// takes a slice of the sorted bodies), so that the few hundred samples of a
+// check fill the GPU; k_guard_finish adds the slices in a fixed order.
+constexpr int kGuardSplit = 16;
+
 __global__ void __launch_bounds__(kExactThreads) k_guard_exact(
     int n, int ns, const float4 *__restrict nodes, const uint32_t *__restrict body_node,
-    const uint32_t *__restrict vals, const float2 *__restrict f, const float2 *__restrict fag,
-    Params prm, double2 *__restrict exact, float2 *__restrict cur) {
+    Params prm, double2 *__restrict part) {
     __shared__ double s_x[kExactThreads], s_y[kExactThreads];
     const int k = guard_sample(blockIdx.x, ns, n);
     const float4 me = nodes[body_node[k]];
     const double px = me.x, py = me.y;
+    const int per = (n + kGuardSplit - 1) / kGuardSplit;
+    const int j0 = (int)blockIdx.y * per, j1 = min(n, j0 + per);
     double ax = 0.0, ay = 0.0;
-    for (int j = threadIdx.x; j < n; j += kExactThreads) {
+    for (int j = j0 + threadIdx.x; j < j1; j += kExactThreads) {
         if (j == k) continue;
         const float4 o = nodes[body_node[j]];
         const double dx = px - o.x, dy = py - o.y;
@@ -517,12 +523,30 @@ __global__ void __launch_bounds__(kExactThreads) k_guard_exact(
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) {
-        const double kmi = (double)prm.k_r * me.z;
-        exact[blockIdx.x] = make_double2(kmi * s_x[0], kmi * s_y[0]);
-        const uint32_t i = vals[k];
-        cur[blockIdx.x] = make_float2(f[i].x - fag[i].x, f[i].y - fag[i].y);
+    if (threadIdx.x == 0)
+        part[(size_t)blockIdx.x * kGuardSplit + blockIdx.y] = make_double2(s_x[0], s_y[0]);
+}
+
+// One thread per sample: its slices' sums in order, times k_r m_i, and the
+// repulsion the iteration applied to it.
+__global__ void __launch_bounds__(256) k_guard_finish(
+    int n, int ns, const float4 *__restrict nodes, const uint32_t *__restrict body_node,
+    const uint32_t *__restrict vals, const float2 *__restrict f, const float2 *__restrict fag,
+    Params prm, const double2 *__restrict part, double2 *__restrict exact,
+    float2 *__restrict cur) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= ns) return;
+    const int k = guard_sample(s, ns, n);
+    double sx = 0.0, sy = 0.0;
+    for (int c = 0; c < kGuardSplit; ++c) {
+        const double2 v = part[(size_t)s * kGuardSplit + c];
+        sx += v.x;
+        sy += v.y;
     }
+    const double kmi = (double)prm.k_r * nodes[body_node[k]].z;
+    exact[s] = make_double2(kmi * sx, kmi * sy);
+    const uint32_t i = vals[k];
+    cur[s] = make_float2(f[i].x - fag[i].x, f[i].y - fag[i].y);
 }
 
 // One warp per sample: the plain walk of the sample's group (the k_traverse
@@ -908,11 +932,15 @@ void launch_traverse_learn(const Buffers &b, const Params &p, const LearnBuffers
         go(k_traverse<false, true>);
 }
 
+size_t guard_part_count(int ns) { return (size_t)ns * kGuardSplit; }
+
 void launch_guard(const Buffers &b, const Params &p, int ns, double2 *exact, float2 *plain,
-                  float2 *cur, cudaStream_t s) {
+                  float2 *cur, double2 *part, cudaStream_t s) {
     if (ns <= 0 || b.n <= 0) return;
-    k_guard_exact<<<ns, kExactThreads, 0, s>>>(b.n, ns, b.nodes, b.body_node, b.vals[0], b.f,
-                                               b.fag, p, exact, cur);
+    k_guard_exact<<<dim3(ns, kGuardSplit), kExactThreads, 0, s>>>(b.n, ns, b.nodes, b.body_node,
+                                                                   p, part);
+    k_guard_finish<<<(ns + 255) / 256, 256, 0, s>>>(b.n, ns, b.nodes, b.body_node, b.vals[0], b.f,
+                                                    b.fag, p, part, exact, cur);
     k_guard_plain<<<(ns + 7) / 8, 256, 0, s>>>(b.n, ns, b.nodes, b.body_node, b.st, p, plain);
 }
 
