@@ -5,7 +5,8 @@
 //
 // The correction works on (group, cell) pairs: a group is the 32 sorted
 // bodies one warp walks together, and the pair is a cell the whole group
-// accepted.  For each pair, 12 features of the cell's multipole statistics as
+// accepted that is not small for its distance (kLearnMinRatio).  For each
+// pair, 12 features of the cell's multipole statistics as
 // seen from the group go through a 12 -> 64 -> 64 -> 2 MLP (BF16 weights and
 // activations, FP32 accumulation).  Its two outputs are the mean, over the
 // group's bodies, of the error the point-mass (or quadrupole) term makes for
